@@ -1,0 +1,278 @@
+/*
+ * storm_fvt.h -- C-ABI of the B200 finite-volume (FVT) time step for SToRM.
+ *
+ * This library replaces one call of the SToRM Fortran program:
+ *
+ *     CALL solverFVT(iter,ttime,rmax,fn,title)      Source_xsy-64bit/solver.f90:57
+ *
+ * whose body is Source_xsy-64bit/solverFVT.f90:129-478 (the SSP-RK loop and the
+ * ~45 routines it calls).  The Fortran host keeps mesh/option input, boundary
+ * set-up (read_data, dataprepFVT) and output; at the call site it passes the
+ * module arrays it already holds (geometry, dep_vars, options, vbc_arrays) through
+ * the StormFvtMesh struct below, then steps the solution on the GPU.
+ *
+ * Conventions (identical to the Fortran module arrays, so a BIND(C) shim can pass
+ * them unchanged):
+ *   - node, element and edge ids are 1-based INTEGER(4);
+ *   - 2-D arrays are column-major with the leading dimension stated per field;
+ *   - LOGICAL(4) arrays are int32 (0 = .FALSE., non-zero = .TRUE.);
+ *   - every real is REAL(KIND=8).
+ *
+ * Every entry point returns 0 on success or a negative STORM_ERR_* code; the
+ * message of the most recent failure on the calling thread is returned by
+ * storm_fvt_last_error().  Device-side checks (non-finite depth, a bounded wait
+ * that ran out) are reported by the next call on the handle.
+ *
+ * Threading: one handle may be used by one host thread at a time; each handle owns
+ * one CUDA stream on the device named in StormFvtOptions.device.
+ */
+#ifndef STORM_FVT_H
+#define STORM_FVT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STORM_FVT_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+  STORM_OK = 0,
+  STORM_ERR_ARG = -1,         /* invalid argument or option value              */
+  STORM_ERR_MESH = -2,        /* mesh/boundary data inconsistent (byebye cases)*/
+  STORM_ERR_CUDA = -3,        /* CUDA runtime error                            */
+  STORM_ERR_NOMEM = -4,       /* host or device allocation failed              */
+  STORM_ERR_DEVICE = -5,      /* device-side check tripped (see message)       */
+  STORM_ERR_UNSUPPORTED = -6  /* option not implemented by this library         */
+};
+
+/* ---- choices ------------------------------------------------------------ */
+enum { STORM_FLUX_ROE = 0, STORM_FLUX_HLL = 1, STORM_FLUX_RUSANOV = 2 };
+enum { STORM_PREC_FP64 = 0, STORM_PREC_MIXED = 1 };
+
+/*
+ * Solver options: the fields of MODULE options (Source_xsy-64bit/options.f90) that
+ * solverFVT reads, with the defaults of initialize_options.f90:23-141 listed.
+ * `flux` and `precision` have no counterpart in the reference (it hard-wires Roe,
+ * invisc_fluxes.f90:137, and FP64).
+ */
+typedef struct StormFvtOptions {
+  double h_dry;        /* dry threshold, default 0.001            (options.f90:39) */
+  double h_wet;        /* wet threshold = coef*h_dry, default h_dry                */
+  double cfl;          /* CFL number; with steady=0 and dt_op=0 it is dt in s     */
+  double vceiling;     /* velocity clip ceiling, default 35                       */
+  double rstop;        /* steady stop threshold on rmax                            */
+  double visc;         /* kinematic viscosity (opt_friction 3), viscosity(18 C)   */
+  int32_t steady;      /* 1 = local-time-step pseudo-time march (default 1)       */
+  int32_t dt_op;       /* unsteady: 0 = fixed dt (=cfl), 1 = CFL dt reduction     */
+  int32_t rkorder;     /* 1, 2 or 3 (SSP-RK), default 2                           */
+  int32_t opt_limiter; /* 0 = zero gradients, 1 = LSQ, 2 = LSQ + Barth-Jespersen   */
+  int32_t btype;       /* walls: 0 = no-slip (wenslp3), 1 = slip (weslp2)          */
+  int32_t hvalve;      /* numerical valve at stage boundaries, default 1           */
+  int32_t vclip;       /* velocity clipping, default 0                             */
+  int32_t opt_friction;/* 0 Manning, 1 Chezy, 2 drag, 3 Colebrook, 4 Strickler     */
+  int32_t stop_cr;     /* steady stop criterion: 0 max|phi|, 1 RMS relative dh     */
+  int32_t flux;        /* interior-edge flux: STORM_FLUX_ROE|HLL|RUSANOV           */
+  int32_t precision;   /* STORM_PREC_FP64 (only value accepted by this version)    */
+  int32_t device;      /* CUDA device ordinal                                      */
+  int32_t reserved[6]; /* must be zero                                             */
+} StormFvtOptions;
+
+/* Fill `opt` with the defaults of initialize_options.f90:23-141 (+ ROE, FP64). */
+void storm_fvt_default_options(StormFvtOptions* opt);
+
+/*
+ * One boundary-condition node string (ioflow.f90 / read_cgns.f90:433-552 input):
+ *   inflow  strings: type = vtype (1 = Q by depth, 4 = stage, 5 = Q by depth on wet
+ *                    cells only); value = qin (m^3/s) or inflow stage (vtype 4);
+ *   outflow strings: type = htype (0 = free, 1 = stage, 2 = critical); value = hbc.
+ * A time series (n_series > 0) replaces `value` through get_time_bcs
+ * (get_time_bcs.f90:31-77).
+ */
+typedef struct StormFvtBoundary {
+  int32_t type;
+  int32_t n_nodes;
+  const int32_t* nodes;      /* [n_nodes], 1-based, consecutive nodes share an edge */
+  double value;
+  int32_t n_series;
+  const double* series_t;    /* [n_series] times (s), increasing                  */
+  const double* series_v;    /* [n_series] values                                  */
+} StormFvtBoundary;
+
+/*
+ * Raw problem description, the input of read_data (mesh, bed, roughness, BC
+ * strings).  storm_fvt_mesh_build() turns it into the prepared StormFvtMesh the
+ * way find_edges / t_areas / walls / ibc_arrays / node_db / elemnt_db and
+ * dataprepFVT do.  Callers that already hold the Fortran module arrays skip it.
+ */
+typedef struct StormFvtProblem {
+  int32_t n_pts, n_elems;
+  const double* x;           /* [n_pts] node coordinates                           */
+  const double* y;
+  const int32_t* tri;        /* [3*n_elems] 1-based vertices, counter-clockwise   */
+  int32_t n_edges;           /* 0: edges are derived (find_edges.f90:41-54);       */
+  const int32_t* edge_p;     /*  else Triangle .edge endpoints [2*n_edges]         */
+  const int32_t* edge_e;     /*  and .v.edge elements [2*n_edges] (-1 = ray)       */
+  const double* zb;          /* bed elevation                                      */
+  int32_t zb_at_vertices;    /*  1: zb is [n_pts] (datav(3)); 0: [n_elems]         */
+  const double* cd;          /* roughness coefficient                              */
+  int32_t cd_at_vertices;    /*  1: cd is [n_pts] (datav(7)); 0: [n_elems]         */
+  int32_t n_inflow;
+  const StormFvtBoundary* inflow;
+  int32_t n_outflow;
+  const StormFvtBoundary* outflow;
+} StormFvtProblem;
+
+/*
+ * Prepared mesh: the module state at the solverFVT call site (after dataprepFVT).
+ * Field names follow the Fortran arrays; array shapes are given as Fortran
+ * declarations, stored column-major.
+ */
+typedef struct StormFvtMesh {
+  int32_t n_pts, n_elems, n_edges;
+  /* geometry.f90 */
+  const double* node_x;          /* nodes(:)%x                 [n_pts]             */
+  const double* node_y;          /* nodes(:)%y                 [n_pts]             */
+  const int32_t* tri_vertex;     /* grid(:)%vertex             (3,n_elems)         */
+  const int32_t* tri_edge;       /* grid(:)%edge, signed       (3,n_elems)         */
+  const double* tri_area;        /* grid(:)%area               [n_elems]           */
+  const double* tri_perim;       /* grid(:)%perim              [n_elems]           */
+  const double* tri_xc;          /* grid(:)%xc                 [n_elems]           */
+  const double* tri_yc;          /* grid(:)%yc                 [n_elems]           */
+  const int32_t* edge_p;         /* edges(:)%p                 (2,n_edges)         */
+  const int32_t* edge_e;         /* edges(:)%e (<1: no element)(2,n_edges)         */
+  const double* edge_normal;     /* edges(:)%normal, unit      (2,n_edges)         */
+  const double* edge_tang;       /* edges(:)%tang, unit        (2,n_edges)         */
+  const double* edge_length;     /* edges(:)%length            [n_edges]           */
+  const double* rc_x;            /* rc(:,:)%x                  (n_elems,3)         */
+  const double* rc_y;            /* rc(:,:)%y                  (n_elems,3)         */
+  int32_t t2t_ncol;              /* SIZE(t2t,2) = maxdim                            */
+  const int32_t* t2t;            /* t2t                        (n_elems,t2t_ncol)  */
+  const double* lsq_dx;          /* dx                         (n_elems,t2t_ncol-1)*/
+  const double* lsq_dy;          /* dy                         (n_elems,t2t_ncol-1)*/
+  const double* lsq_w;           /* lsqweight                  (n_elems,t2t_ncol-1)*/
+  const double* lsq_a;           /* ai  [n_elems] */
+  const double* lsq_b;           /* bi  [n_elems] */
+  const double* lsq_c;           /* ci  [n_elems] */
+  const double* lsq_det;         /* det [n_elems] */
+  const int32_t* t2t3;           /* t2t3                       (3,n_elems)         */
+  int32_t n2t_ncol;              /* SIZE(n2t,2)                                     */
+  const int32_t* n2t;            /* n2t                        (n_pts,n2t_ncol)    */
+  int32_t c2v_ncol;              /* SIZE(c2v_weights_id,2) (>= n2t_ncol-1)          */
+  const double* c2v_w;           /* c2v_weights_id             (n_pts,c2v_ncol)    */
+  const int32_t* csortedz;       /* csortedz(:)%p              (3,n_elems)         */
+  int32_t flow_edges1;           /* interior edges                                  */
+  const int32_t* flowedg1;       /* [flow_edges1]                                   */
+  int32_t wall_edges1;           /* wall edges with a flux (walls.f90:132-136)      */
+  const int32_t* walledg1;       /* [wall_edges1]                                   */
+  int32_t n_bcedges;
+  const int32_t* bcedges;        /* [n_bcedges]                                     */
+  const int32_t* hbar;           /* LOGICAL [n_bcedges]: stage-boundary edge        */
+  /* dep_vars.f90 */
+  const double* z;               /* cell bed elevation         [n_elems]           */
+  const double* zvtx;            /* vertex bed elevation       [n_pts]             */
+  const double* cd;              /* roughness                  [n_elems]           */
+  /* vbc_arrays.f90 / dep_vars.f90: inflow boundaries */
+  int32_t n_inflowbdr;
+  const int32_t* vtype;          /* [n_inflowbdr]                                   */
+  const double* qin;             /* [n_inflowbdr]                                   */
+  int32_t bcin_ld;               /* SIZE(bcedgesinflow,1) = d1+1                    */
+  const int32_t* bcedgesinflow;  /* (0:d1,n_inflowbdr); row 0 holds the count       */
+  int32_t tsq_ld;                /* SIZE(timelocq,1)                                */
+  const int32_t* n_timeserq;     /* [n_inflowbdr]                                   */
+  const double* timelocq;        /* (tsq_ld,n_inflowbdr)                            */
+  const double* timeserq;        /* (tsq_ld,n_inflowbdr)                            */
+  /* outflow boundaries */
+  int32_t n_outflowbdr;
+  const int32_t* htype;          /* [n_outflowbdr]                                  */
+  const double* hbc;             /* [n_outflowbdr]                                  */
+  int32_t bcout_ld;              /* SIZE(bcedgesoutflow,1) = d1+1                   */
+  const int32_t* bcedgesoutflow; /* (0:d1,n_outflowbdr)                             */
+  int32_t hbc_ld;                /* SIZE(hbc_nodes,1)                               */
+  const int32_t* n_hbc;          /* [n_outflowbdr]                                  */
+  const int32_t* hbc_nodes;      /* (hbc_ld,n_outflowbdr)                           */
+  int32_t tsh_ld;                /* SIZE(timeloch,1)                                */
+  const int32_t* n_timeserh;     /* [n_outflowbdr]                                  */
+  const double* timeloch;        /* (tsh_ld,n_outflowbdr)                           */
+  const double* timeserh;        /* (tsh_ld,n_outflowbdr)                           */
+  double bch_max;                /* dataprepFVT.f90:278-286                         */
+} StormFvtMesh;
+
+/* Per-call statistics, the scalars solverFVT prints per iteration
+ * (solverFVT.f90:407-449).  cqin3/cqout3 are those of the last RK stage. */
+#define STORM_MAX_BDR 16
+typedef struct StormFvtStepStats {
+  int32_t iter;        /* iterations done so far on this handle                    */
+  int32_t converged;   /* steady: rmax < rstop was reached (solverFVT.f90:431)     */
+  double ttime;        /* sum of delt (solverFVT.f90:155)                          */
+  double stime;        /* simulated time (unsteady) or iter (steady)               */
+  double delt;         /* last dt (steady: local dt of the last cell, as the ref.) */
+  double rmax;         /* stopping quantity (steady) / max|phi| (unsteady)         */
+  double rms_dh;       /* SQRT(sumtop/sumbot)                                      */
+  double tmass;        /* SUM(h*area)                                              */
+  double cqin3[STORM_MAX_BDR];
+  double cqout3[STORM_MAX_BDR];
+  int32_t device_status; /* 0, or the device-side check code                      */
+  int32_t reserved[7];
+} StormFvtStepStats;
+
+typedef struct StormFvtHandle StormFvtHandle;
+
+/* Message of the last failure on this thread ("" if none). */
+const char* storm_fvt_last_error(void);
+
+/*
+ * Build the prepared mesh from a raw problem: the C++ restatement of read_data's
+ * topology builders and of dataprepFVT (find_edges.f90, edge_normals.f90,
+ * t_areas.f90, walls.f90, ibc_arrays.f90, node_db.f90:60-68, elemnt_db.f90:50-233,
+ * cde_t2t.f90, dataprepFVT.f90:69-306, c2v_setup.f90:98-119, lsq_setup.f90:92-145).
+ * The result is owned by the library and freed by storm_fvt_mesh_free().
+ */
+int storm_fvt_mesh_build(const StormFvtProblem* prob, StormFvtMesh** out);
+void storm_fvt_mesh_free(StormFvtMesh* mesh);
+
+/*
+ * Create a solver on the device: copies the prepared mesh to HBM in the library's
+ * reordered structure-of-arrays layout.  Replaces the state set-up part of
+ * solverFVT.f90:53-126.  The mesh arrays are not retained.
+ */
+int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt,
+                     StormFvtHandle** out);
+
+/* Set the cell state h, u, v [n_elems] (dep_vars.f90 arrays, element order) and
+ * reset the iteration counters; rk*(:,rkorder) = h, h*u, h*v (solverFVT.f90:122-126). */
+int storm_fvt_set_state(StormFvtHandle* hd, const double* h, const double* u,
+                        const double* v);
+
+/*
+ * Advance up to `nsteps` iterations of the main loop (solverFVT.f90:129-478).  In
+ * steady mode the loop stops early once rmax < rstop, like the EXIT at :431.
+ * `stats` (may be NULL) receives the scalars after the last iteration done.
+ */
+int storm_fvt_step(StormFvtHandle* hd, int32_t nsteps, StormFvtStepStats* stats);
+
+/* Copy the state back to host arrays in element/node order.  Any pointer may be
+ * NULL.  rk* receive level rkorder; hvtx the vertex depth of the last stage. */
+int storm_fvt_get_state(StormFvtHandle* hd, double* h, double* u, double* v,
+                        double* rkh, double* rku, double* rkv, double* hvtx);
+
+/* Dry-cell flags of the first RK stage of the next iteration, as find_dry_cells
+ * (find_dry_cells.f90:25-42) sets them, element order, int32 0/1. */
+int storm_fvt_get_drycell(StormFvtHandle* hd, int32_t* drycell);
+
+/* Number of this library's kernel launches since create (launch accounting). */
+int64_t storm_fvt_kernel_launches(const StormFvtHandle* hd);
+
+/* Device time (ms, CUDA events on the handle's stream) of the last storm_fvt_step
+ * call, and the summed time of its flux kernel launches. */
+int storm_fvt_last_timing(const StormFvtHandle* hd, double* step_ms,
+                          double* flux_kernel_ms, int64_t* flux_kernel_launches);
+
+int storm_fvt_destroy(StormFvtHandle* hd);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STORM_FVT_H */
