@@ -1,0 +1,300 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FVT time step (SToRM solverFVT) -- one JSON line.
+
+Workload: the 2,000,000-triangle transient meander (seeded jittered-lattice Delaunay
+mesh, sloped bed + Gaussian random field, Manning n ~ U[0.02,0.06], ~30% dry cells,
+Q = 200 m^3/s, Roe flux, LSQ + Barth-Jespersen, SSP-RK3 with the CFL dt reduction),
+FP64.  One "step" is one iteration of solverFVT's main loop: three RK stages over the
+whole mesh plus friction and the stop/mass reductions.  The metric is cell-stage
+updates/s = n_cells * rkorder * steps / time.
+
+Arms:
+  --impl ours       (default) the CUDA library; `value` is device time of the K timed
+                    iterations (graph replays, state resident in HBM, CUDA events on
+                    the library's stream, max over ranks); `e2e` goes through the C-ABI
+                    with host buffers: set_state (H2D), K x storm_fvt_step(1) each
+                    returning its scalars (D2H), get_state (D2H), host wall clock.
+  --impl reference  the reference algorithm on the host CPU cores: the FP64 oracle
+                    port (the Fortran reference has no compiler on these machines),
+                    all host threads, same mesh and metric.
+
+Multi-GPU (torchrun, one rank per GPU): every rank advances its own copy of the
+scenario (independent units, no collective on the data path): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from storm_b200 import scenarios  # noqa: E402
+
+METRIC = "cell-stage updates/s (FVT time step, 2M-triangle meander)"
+UNIT = "cell-stage updates/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        d["source"] = "measured"
+        return d
+    return dict(PEAKS_FALLBACK)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        try:
+            self.f.flush()
+            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        except OSError:
+            rows = []
+        finally:
+            try:
+                os.unlink(self.f.name)
+            except OSError:
+                pass
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(args):
+    if args.config == "meander":
+        sc = scenarios.meander(n_target=args.cells)
+    elif args.config == "dambreak":
+        sc = scenarios.dambreak(n_target=args.cells)
+    else:
+        sc = scenarios.channel()
+    return sc
+
+
+def mesh_ratios(sc):
+    from storm_b200 import fvt
+    pm = fvt.build_mesh(sc.problem)
+    m = pm.mesh
+    return pm, m.n_elems, m.n_edges, m.n_pts
+
+
+def run_cpu(sc, steps, threads, warmup=0):
+    """The reference algorithm (oracle port) on the host; returns (updates/s, seconds)."""
+    from oracle.oracle import Oracle
+    o = Oracle(sc.problem, sc.options, threads=threads)
+    o.set_state(sc.h0, sc.u0, sc.v0)
+    if warmup:
+        o.step(warmup)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return sc.n_elems * sc.options.rkorder * steps / dt, dt
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["meander", "dambreak", "channel"], default="meander")
+    ap.add_argument("--cells", type=int, default=2_000_000)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="oracle iterations timed for cpu_baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        sc = build_workload(args)
+        from oracle import oracle as _o
+        _o.build()
+        # each timed step is one full iteration of the workload on all host threads
+        val, secs = run_cpu(sc, args.steps, threads, warmup=min(args.warmup, 1))
+        out = {
+            "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"{args.config}-{sc.n_elems}", "cells": sc.n_elems,
+                       "rkorder": sc.options.rkorder, "parallelism": "host threads"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full iterations of the {sc.n_elems}-cell workload"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(out))
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    from storm_b200 import build, fvt
+    build.build()
+    sc = build_workload(args)
+    sc.options.device = local
+    pm, T, E, N = mesh_ratios(sc)
+    K_rk = sc.options.rkorder
+    solver = fvt.Solver(pm, sc.options, keep=pm)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timed region ----
+    solver.set_state(sc.h0, sc.u0, sc.v0)
+    solver.step(args.warmup)
+    barrier()
+    launches0 = solver.kernel_launches()
+    with ClockSampler(local) as clk:
+        barrier()
+        stats = solver.step(args.steps)
+        barrier()
+    ms = solver.last_timing()["step_ms"]
+    gpu_launches = solver.kernel_launches() - launches0
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * T * K_rk * args.steps / (ms_max / 1e3)
+
+    # ---- end-to-end through the C-ABI with host buffers ----
+    e2e_steps = max(1, min(args.steps, 200))
+    barrier()
+    t0 = time.perf_counter()
+    solver.set_state(sc.h0, sc.u0, sc.v0)
+    for _ in range(e2e_steps):
+        solver.step(1)
+    st = solver.state()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = world * T * K_rk * e2e_steps / e2e_s
+    h2d = 3 * 8 * T / e2e_steps
+    d2h = 224 + (6 * 8 * T + 8 * N) / e2e_steps  # StepStats per call + the final state
+
+    # ---- per-kernel timing pass (roofline of the RK-stage kernel chain) ----
+    solver.set_state(sc.h0, sc.u0, sc.v0)
+    solver.set_kernel_timing(True)
+    kt_steps = 5
+    solver.step(kt_steps)
+    kt = solver.kernel_times()
+    solver.set_kernel_timing(False)
+    stage_ms = sum(kt[k][0] for k in ("node", "grad", "bc", "flux"))
+    B = scenarios.algorithmic_bytes_per_cell_stage(T, E, N)
+    pk = peaks()
+    achieved = B * T * K_rk * kt_steps / (stage_ms / 1e3) / 1e9
+    iter_ms = sum(v[0] for v in kt.values())
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
+        "frac": achieved / pk["hbm_gbs"], "traffic": None,
+        "kernel": "one RK stage: k_node + k_grad + k_bc + k_flux",
+        "bytes_per_cell_stage": B, "peak_source": pk["source"],
+        "kernel_ms_share": {k: round(v[0] / iter_ms, 4) for k, v in kt.items()},
+        "flux_kernel_avg_ms": kt["flux"][0] / max(1, kt["flux"][1]),
+    }
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator; no public dataset exists for this path)",
+        "config": {"workload": f"{args.config}-{T}", "cells": T, "edges": E, "nodes": N, "rkorder": K_rk,
+                   "flux": int(sc.options.flux), "precision": "fp64", "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2 (inputs larger than the 126 MB L2)",
+                   "dry_fraction": sc.info.get("dry_fraction")},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "gpu_launches": gpu_launches,
+        "roofline": roofline,
+        "clocks": clk.summary(),
+        "final": {"iter": stats["iter"], "tmass": stats["tmass"], "status": stats["device_status"]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cv, secs = run_cpu(sc, args.cpu_steps, threads)
+        out["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"{args.cpu_steps} iterations of the same {T}-cell workload "
+                                         f"({secs:.1f} s on {threads} threads)"}
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

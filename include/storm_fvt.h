@@ -37,6 +37,12 @@ extern "C" {
 
 #define STORM_FVT_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define STORM_FVT_API __attribute__((visibility("default")))
+#else
+#define STORM_FVT_API
+#endif
+
 /* ---- status codes ------------------------------------------------------- */
 enum {
   STORM_OK = 0,
@@ -81,7 +87,7 @@ typedef struct StormFvtOptions {
 } StormFvtOptions;
 
 /* Fill `opt` with the defaults of initialize_options.f90:23-141 (+ ROE, FP64). */
-void storm_fvt_default_options(StormFvtOptions* opt);
+STORM_FVT_API void storm_fvt_default_options(StormFvtOptions* opt);
 
 /*
  * One boundary-condition node string (ioflow.f90 / read_cgns.f90:433-552 input):
@@ -221,7 +227,7 @@ typedef struct StormFvtStepStats {
 typedef struct StormFvtHandle StormFvtHandle;
 
 /* Message of the last failure on this thread ("" if none). */
-const char* storm_fvt_last_error(void);
+STORM_FVT_API const char* storm_fvt_last_error(void);
 
 /*
  * Build the prepared mesh from a raw problem: the C++ restatement of read_data's
@@ -230,20 +236,20 @@ const char* storm_fvt_last_error(void);
  * cde_t2t.f90, dataprepFVT.f90:69-306, c2v_setup.f90:98-119, lsq_setup.f90:92-145).
  * The result is owned by the library and freed by storm_fvt_mesh_free().
  */
-int storm_fvt_mesh_build(const StormFvtProblem* prob, StormFvtMesh** out);
-void storm_fvt_mesh_free(StormFvtMesh* mesh);
+STORM_FVT_API int storm_fvt_mesh_build(const StormFvtProblem* prob, StormFvtMesh** out);
+STORM_FVT_API void storm_fvt_mesh_free(StormFvtMesh* mesh);
 
 /*
  * Create a solver on the device: copies the prepared mesh to HBM in the library's
  * reordered structure-of-arrays layout.  Replaces the state set-up part of
  * solverFVT.f90:53-126.  The mesh arrays are not retained.
  */
-int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt,
+STORM_FVT_API int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt,
                      StormFvtHandle** out);
 
 /* Set the cell state h, u, v [n_elems] (dep_vars.f90 arrays, element order) and
  * reset the iteration counters; rk*(:,rkorder) = h, h*u, h*v (solverFVT.f90:122-126). */
-int storm_fvt_set_state(StormFvtHandle* hd, const double* h, const double* u,
+STORM_FVT_API int storm_fvt_set_state(StormFvtHandle* hd, const double* h, const double* u,
                         const double* v);
 
 /*
@@ -251,26 +257,37 @@ int storm_fvt_set_state(StormFvtHandle* hd, const double* h, const double* u,
  * steady mode the loop stops early once rmax < rstop, like the EXIT at :431.
  * `stats` (may be NULL) receives the scalars after the last iteration done.
  */
-int storm_fvt_step(StormFvtHandle* hd, int32_t nsteps, StormFvtStepStats* stats);
+STORM_FVT_API int storm_fvt_step(StormFvtHandle* hd, int32_t nsteps, StormFvtStepStats* stats);
 
 /* Copy the state back to host arrays in element/node order.  Any pointer may be
  * NULL.  rk* receive level rkorder; hvtx the vertex depth of the last stage. */
-int storm_fvt_get_state(StormFvtHandle* hd, double* h, double* u, double* v,
+STORM_FVT_API int storm_fvt_get_state(StormFvtHandle* hd, double* h, double* u, double* v,
                         double* rkh, double* rku, double* rkv, double* hvtx);
 
 /* Dry-cell flags of the first RK stage of the next iteration, as find_dry_cells
  * (find_dry_cells.f90:25-42) sets them, element order, int32 0/1. */
-int storm_fvt_get_drycell(StormFvtHandle* hd, int32_t* drycell);
+STORM_FVT_API int storm_fvt_get_drycell(StormFvtHandle* hd, int32_t* drycell);
 
 /* Number of this library's kernel launches since create (launch accounting). */
-int64_t storm_fvt_kernel_launches(const StormFvtHandle* hd);
+STORM_FVT_API int64_t storm_fvt_kernel_launches(const StormFvtHandle* hd);
+
+/* Kernel timing mode (off by default).  When on, storm_fvt_step launches the
+ * kernels of each iteration one by one (no CUDA graph) with a CUDA event pair
+ * around every flux-kernel launch, for per-kernel roofline figures. */
+STORM_FVT_API int storm_fvt_set_kernel_timing(StormFvtHandle* hd, int32_t on);
 
 /* Device time (ms, CUDA events on the handle's stream) of the last storm_fvt_step
- * call, and the summed time of its flux kernel launches. */
-int storm_fvt_last_timing(const StormFvtHandle* hd, double* step_ms,
+ * call; in kernel timing mode also the summed time of its flux-kernel launches. */
+STORM_FVT_API int storm_fvt_last_timing(const StormFvtHandle* hd, double* step_ms,
                           double* flux_kernel_ms, int64_t* flux_kernel_launches);
 
-int storm_fvt_destroy(StormFvtHandle* hd);
+/* Per-kernel device time (ms) and launch counts of the last storm_fvt_step call in
+ * kernel timing mode, indexed 0 node (vertex depth), 1 grad (gradients/limiter),
+ * 2 bc (open boundaries), 3 flux (fluxes + sources + RK update), 4 fric (friction
+ * and reduction partials), 5 final (iteration scalars); 6-7 are zero. */
+STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, int64_t* launches);
+
+STORM_FVT_API int storm_fvt_destroy(StormFvtHandle* hd);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,571 @@
+// api.cu -- the C-ABI entry points of include/storm_fvt.h (handle, state, stepping).
+//
+// storm_fvt_create copies the prepared mesh to HBM in the reordered SoA layout and
+// captures one full iteration (all RK stages, friction, reductions) as a CUDA graph;
+// storm_fvt_step replays the graph `nsteps` times on the handle's stream, polling
+// the device-side stop flag every few iterations in steady mode, so the host never
+// synchronises inside an iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "fvt_device.cuh"
+#include "storm_internal.h"
+
+namespace storm {
+
+__global__ void k_init(Dev d);
+__global__ void k_init_final(Dev d, int nblk);
+__global__ void k_node(Dev d, const double* hs, const uint8_t* dry);
+__global__ void k_grad(Dev d, const double* hs, const uint8_t* dry, double* rku_prev, double* rkv_prev);
+__global__ void k_bc(Dev d, const double* hs, const uint8_t* dry);
+__global__ void k_flux(Dev d, int s, const double* hs, const uint8_t* dry, uint8_t* dry_next);
+__global__ void k_fric(Dev d);
+__global__ void k_final(Dev d, int nblk);
+
+static thread_local std::string g_err;
+
+int set_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+void clear_error() { g_err.clear(); }
+
+}  // namespace storm
+
+using namespace storm;
+
+struct StormFvtHandle {
+  StormFvtOptions opt{};
+  HostLayout L;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  void* arena = nullptr;
+  Dev d{};
+  Scalars* sc_host = nullptr;  // pinned
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int kernels_per_step = 0;
+  int64_t launches = 0;
+  size_t bc_smem = 0;
+  bool have_state = false;
+  bool timing = false;
+  double last_step_ms = 0.0, last_flux_ms = 0.0;
+  int64_t last_flux_launches = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> fev;  // event pairs of the timing mode
+  std::vector<int> fev_class;    // kernel class of each pair
+  double kt_ms[8] = {0};         // per-class totals of the last timed call
+  int64_t kt_n[8] = {0};
+};
+
+namespace {
+
+constexpr int kCellThreads = 256;
+constexpr int kFluxThreads = 128;
+constexpr int kNodeThreads = 256;
+constexpr int kRed = 256;
+
+#define CK(call)                                                                                     \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return set_error(STORM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+int check_options(const StormFvtOptions& o) {
+  if (o.rkorder < 1 || o.rkorder > 3) return set_error(STORM_ERR_ARG, "Incorrect Runge-Kutta order (1, 2 or 3)");
+  if (o.opt_limiter < 0 || o.opt_limiter > 2) return set_error(STORM_ERR_ARG, "opt_limiter must be 0, 1 or 2");
+  if (o.btype != 0 && o.btype != 1) return set_error(STORM_ERR_ARG, "btype must be 0 or 1");
+  if (o.opt_friction < 0 || o.opt_friction > 4)
+    return set_error(STORM_ERR_UNSUPPORTED, "opt_friction must be 0..4 (5, the vegetation model, is not built)");
+  if (o.flux < 0 || o.flux > 2) return set_error(STORM_ERR_ARG, "flux must be ROE, HLL or RUSANOV");
+  if (o.stop_cr != 0 && o.stop_cr != 1) return set_error(STORM_ERR_ARG, "stop_cr must be 0 or 1");
+  if (o.precision != STORM_PREC_FP64)
+    return set_error(STORM_ERR_UNSUPPORTED, "only STORM_PREC_FP64 is available in this version");
+  if (!(o.h_dry > 0.0) || !(o.h_wet >= o.h_dry)) return set_error(STORM_ERR_ARG, "need 0 < h_dry <= h_wet");
+  if (!(o.cfl > 0.0)) return set_error(STORM_ERR_ARG, "cfl must be positive");
+  for (int i = 0; i < 6; i++)
+    if (o.reserved[i]) return set_error(STORM_ERR_ARG, "reserved option fields must be zero");
+  return 0;
+}
+
+// Device arena: every buffer 256-byte aligned inside one allocation.
+struct Arena {
+  size_t off = 0;
+  std::vector<std::pair<size_t, size_t>> items;
+  size_t take(size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  }
+};
+
+template <class T>
+T* at(void* base, size_t off) {
+  return reinterpret_cast<T*>(static_cast<char*>(base) + off);
+}
+
+// Kernel classes of the per-kernel timing mode.
+enum { KT_NODE = 0, KT_GRAD, KT_BC, KT_FLUX, KT_FRIC, KT_FINAL, KT_COUNT };
+
+int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
+  const Dev& d = h->d;
+  const int T = d.T, N = d.N, K = d.K;
+  const int gT = (T + kCellThreads - 1) / kCellThreads;
+  const int gF = (T + kFluxThreads - 1) / kFluxThreads;
+  const int gN = (N + kNodeThreads - 1) / kNodeThreads;
+  // in timing mode every launch is bracketed by an event pair tagged with its class
+  auto mark = [&](int cls) -> int {
+    if (!timing) return 0;
+    CK(cudaEventRecord(h->fev[*fev_used], h->stream));
+    h->fev_class[*fev_used / 2] = cls;
+    (*fev_used)++;
+    return 0;
+  };
+  auto done = [&]() -> int {
+    if (!timing) return 0;
+    CK(cudaEventRecord(h->fev[(*fev_used)++], h->stream));
+    return 0;
+  };
+  for (int s = 1; s <= K; s++) {
+    const double* hs = d.rkh + (size_t)(s - 1) * T;
+    uint8_t* dry = (s & 1) ? d.dry_a : d.dry_b;
+    uint8_t* dry_next = (s & 1) ? d.dry_b : d.dry_a;
+    if (mark(KT_NODE)) return STORM_ERR_CUDA;
+    k_node<<<gN, kNodeThreads, 0, h->stream>>>(d, hs, dry);
+    if (done() || mark(KT_GRAD)) return STORM_ERR_CUDA;
+    k_grad<<<gT, kCellThreads, 0, h->stream>>>(d, hs, dry, d.rku + (size_t)(s - 1) * T, d.rkv + (size_t)(s - 1) * T);
+    if (done()) return STORM_ERR_CUDA;
+    if (d.nbdr > 0) {
+      if (mark(KT_BC)) return STORM_ERR_CUDA;
+      k_bc<<<d.nbdr, 128, h->bc_smem, h->stream>>>(d, hs, dry);
+      if (done()) return STORM_ERR_CUDA;
+    }
+    if (mark(KT_FLUX)) return STORM_ERR_CUDA;
+    k_flux<<<gF, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
+    if (done()) return STORM_ERR_CUDA;
+  }
+  if (mark(KT_FRIC)) return STORM_ERR_CUDA;
+  k_fric<<<d.nblk_red, kRed, 0, h->stream>>>(d);
+  if (done() || mark(KT_FINAL)) return STORM_ERR_CUDA;
+  k_final<<<1, kRed, 0, h->stream>>>(d, d.nblk_red);
+  if (done()) return STORM_ERR_CUDA;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int capture_graph(StormFvtHandle* h) {
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  size_t dummy = 0;
+  int rc = enqueue_step(h, false, &dummy);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return set_error(STORM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  h->graph = g;
+  size_t n = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &n));
+  h->kernels_per_step = (int)n;
+  CK(cudaGraphInstantiate(&h->exec, g, 0));
+  return 0;
+}
+
+void release(StormFvtHandle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  for (cudaEvent_t e : h->fev) cudaEventDestroy(e);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  if (h->arena) cudaFree(h->arena);
+  if (h->sc_host) cudaFreeHost(h->sc_host);
+  delete h;
+}
+
+int upload(StormFvtHandle* h) {
+  HostLayout& L = h->L;
+  const int T = L.T, N = L.N, K = h->opt.rkorder;
+  const size_t T3 = 3 * (size_t)T, TK = (size_t)L.kst * T;
+  const int nblk = (T + kRed - 1) / kRed;
+  const size_t nbce = std::max(L.nbce, 1), nbdr = std::max(L.nbdr, 1), nwall = std::max(L.nwall, 1);
+  const size_t nnz = std::max(L.n2t_nnz, 1), nts = std::max<size_t>(L.ts_t.size(), 1);
+  const size_t nio = std::max(L.n_in + L.n_out, 1);
+  Arena A;
+  struct Up {
+    size_t off;
+    const void* src;
+    size_t bytes;
+  };
+  std::vector<Up> ups;
+  auto cpy = [&](const auto& vec, size_t n_alloc) {
+    using V = typename std::decay<decltype(vec)>::type::value_type;
+    size_t o = A.take(sizeof(V) * n_alloc);
+    if (!vec.empty()) ups.push_back({o, vec.data(), sizeof(V) * vec.size()});
+    return o;
+  };
+  // constant mesh data
+  size_t o_area = cpy(L.area, T), o_perim = cpy(L.perim, T), o_xc = cpy(L.xc, T), o_yc = cpy(L.yc, T);
+  size_t o_z = cpy(L.z, T), o_dzx = cpy(L.delz_x, T), o_dzy = cpy(L.delz_y, T), o_zmax = cpy(L.zmax, T);
+  size_t o_cd = cpy(L.cd, T), o_la = cpy(L.lsq_a, T), o_lb = cpy(L.lsq_b, T), o_lc = cpy(L.lsq_c, T);
+  size_t o_ld = cpy(L.lsq_det, T);
+  size_t o_nst = cpy(L.nst, T), o_ford = cpy(L.forder, T), o_hvm = cpy(L.hvmask, T), o_fk = cpy(L.fkind, T3);
+  size_t o_vert = cpy(L.vert, T3), o_t3 = cpy(L.t2t3, T3), o_fref = cpy(L.fref, T3), o_sid = cpy(L.st_id, TK);
+  size_t o_rcx = cpy(L.rc_x, T3), o_rcy = cpy(L.rc_y, T3), o_fnx = cpy(L.fnx, T3), o_fny = cpy(L.fny, T3);
+  size_t o_flen = cpy(L.flen, T3), o_fz0 = cpy(L.fz0, T3);
+  size_t o_sw = cpy(L.st_w, TK), o_sdx = cpy(L.st_dx, TK), o_sdy = cpy(L.st_dy, TK);
+  size_t o_wp1 = cpy(L.wall_p1, nwall), o_wp2 = cpy(L.wall_p2, nwall);
+  size_t o_zv = cpy(L.zvtx, N), o_nx = cpy(L.node_x, N), o_ny = cpy(L.node_y, N), o_n2w = cpy(L.n2t_w, nnz);
+  size_t o_n2o = cpy(L.n2t_off, (size_t)N + 1), o_n2c = cpy(L.n2t_cell, nnz), o_nh = cpy(L.node_hbc, N);
+  size_t o_bk = cpy(L.bdr_kind, nbdr), o_bs = cpy(L.bdr_slot, nbdr), o_bo = cpy(L.bdr_off, nbdr);
+  size_t o_bcn = cpy(L.bdr_cnt, nbdr), o_bcc = cpy(L.bce_cell, nbce), o_bcs = cpy(L.bce_slot, nbce);
+  size_t o_bnx = cpy(L.bce_nx, nbce), o_bny = cpy(L.bce_ny, nbce), o_btx = cpy(L.bce_tx, nbce);
+  size_t o_bty = cpy(L.bce_ty, nbce), o_bl = cpy(L.bce_len, nbce), o_bz = cpy(L.bce_zmid, nbce);
+  size_t o_tso = cpy(L.ts_off, nio), o_tsc = cpy(L.ts_cnt, nio), o_ot = cpy(L.out_type, nio);
+  size_t o_tst = cpy(L.ts_t, nts), o_tsv = cpy(L.ts_v, nts);
+  // state
+  const size_t TL = (size_t)(K + 1) * T;
+  size_t o_rkh = A.take(8 * TL), o_rku = A.take(8 * TL), o_rkv = A.take(8 * TL);
+  size_t o_ua = A.take(8 * (size_t)T), o_va = A.take(8 * (size_t)T), o_ub = A.take(8 * (size_t)T),
+         o_vb = A.take(8 * (size_t)T);
+  size_t o_g[6];
+  for (int i = 0; i < 6; i++) o_g[i] = A.take(8 * (size_t)T);
+  size_t o_dra = A.take(T), o_drb = A.take(T), o_hv = A.take(8 * (size_t)N), o_vw = A.take(N);
+  size_t o_pm = A.take(8 * (size_t)T), o_bcc3 = A.take(8 * 3 * nbce), o_rec = A.take(8 * 3 * nbce);
+  size_t o_part = A.take(8 * 8 * (size_t)nblk), o_sc = A.take(sizeof(Scalars));
+  cudaError_t e = cudaMalloc(&h->arena, A.off);
+  if (e != cudaSuccess)
+    return set_error(e == cudaErrorMemoryAllocation ? STORM_ERR_NOMEM : STORM_ERR_CUDA,
+                     std::string("device allocation of ") + std::to_string(A.off) + " bytes: " + cudaGetErrorString(e));
+  CK(cudaMemset(h->arena, 0, A.off));
+  for (const Up& u : ups) CK(cudaMemcpy(static_cast<char*>(h->arena) + u.off, u.src, u.bytes, cudaMemcpyHostToDevice));
+  void* B = h->arena;
+  Dev& d = h->d;
+  const StormFvtOptions& o = h->opt;
+  d.T = T; d.N = N; d.K = K; d.kst = L.kst; d.nbdr = L.nbdr; d.nbce = L.nbce;
+  d.steady = o.steady != 0; d.dt_op = o.dt_op; d.lim = o.opt_limiter; d.btype = o.btype;
+  d.hvalve = o.hvalve != 0; d.vclip = o.vclip != 0; d.fric = o.opt_friction; d.stop_cr = o.stop_cr;
+  d.flux = o.flux; d.last_cell = L.last_cell_new; d.n_in = L.n_in; d.n_out = L.n_out;
+  d.h_dry = o.h_dry; d.h_wet = o.h_wet; d.cfl = o.cfl; d.vceiling = o.vceiling; d.visc = o.visc;
+  d.rstop = o.rstop; d.bch_max = L.bch_max;
+  // RK tables, dataprepFVT.f90:256-273
+  std::memset(d.alpha, 0, sizeof d.alpha);
+  std::memset(d.beta, 0, sizeof d.beta);
+  if (K == 1) { d.alpha[1][0] = 1.0; d.beta[1] = 1.0; }
+  if (K == 2) { d.alpha[1][0] = 1.0; d.beta[1] = 1.0; d.alpha[2][0] = 0.5; d.alpha[2][1] = 0.5; d.beta[2] = 0.5; }
+  if (K == 3) {
+    d.alpha[1][0] = 1.0;
+    d.alpha[2][0] = 0.750; d.alpha[2][1] = 0.250;
+    d.alpha[3][0] = 1.0 / 3.0; d.alpha[3][1] = 0.0; d.alpha[3][2] = 2.0 / 3.0;
+    d.beta[1] = 1.0; d.beta[2] = 0.250; d.beta[3] = 2.0 / 3.0;
+  }
+  d.area = at<double>(B, o_area); d.perim = at<double>(B, o_perim); d.xc = at<double>(B, o_xc);
+  d.yc = at<double>(B, o_yc); d.z = at<double>(B, o_z); d.delz_x = at<double>(B, o_dzx);
+  d.delz_y = at<double>(B, o_dzy); d.zmax = at<double>(B, o_zmax); d.cd = at<double>(B, o_cd);
+  d.lsq_a = at<double>(B, o_la); d.lsq_b = at<double>(B, o_lb); d.lsq_c = at<double>(B, o_lc);
+  d.lsq_det = at<double>(B, o_ld);
+  d.nst = at<uint8_t>(B, o_nst); d.forder = at<uint8_t>(B, o_ford); d.hvmask = at<uint8_t>(B, o_hvm);
+  d.fkind = at<uint8_t>(B, o_fk);
+  d.vert = at<int32_t>(B, o_vert); d.t2t3 = at<int32_t>(B, o_t3); d.fref = at<int32_t>(B, o_fref);
+  d.st_id = at<int32_t>(B, o_sid);
+  d.rc_x = at<double>(B, o_rcx); d.rc_y = at<double>(B, o_rcy); d.fnx = at<double>(B, o_fnx);
+  d.fny = at<double>(B, o_fny); d.flen = at<double>(B, o_flen); d.fz0 = at<double>(B, o_fz0);
+  d.st_w = at<double>(B, o_sw); d.st_dx = at<double>(B, o_sdx); d.st_dy = at<double>(B, o_sdy);
+  d.wall_p1 = at<int32_t>(B, o_wp1); d.wall_p2 = at<int32_t>(B, o_wp2);
+  d.zvtx = at<double>(B, o_zv); d.node_x = at<double>(B, o_nx); d.node_y = at<double>(B, o_ny);
+  d.n2t_w = at<double>(B, o_n2w); d.n2t_off = at<int32_t>(B, o_n2o); d.n2t_cell = at<int32_t>(B, o_n2c);
+  d.node_hbc = at<int16_t>(B, o_nh);
+  d.bdr_kind = at<int32_t>(B, o_bk); d.bdr_slot = at<int32_t>(B, o_bs); d.bdr_off = at<int32_t>(B, o_bo);
+  d.bdr_cnt = at<int32_t>(B, o_bcn); d.bce_cell = at<int32_t>(B, o_bcc); d.bce_slot = at<int32_t>(B, o_bcs);
+  d.bce_nx = at<double>(B, o_bnx); d.bce_ny = at<double>(B, o_bny); d.bce_tx = at<double>(B, o_btx);
+  d.bce_ty = at<double>(B, o_bty); d.bce_len = at<double>(B, o_bl); d.bce_zmid = at<double>(B, o_bz);
+  d.ts_off = at<int32_t>(B, o_tso); d.ts_cnt = at<int32_t>(B, o_tsc); d.out_type = at<int32_t>(B, o_ot);
+  d.ts_t = at<double>(B, o_tst); d.ts_v = at<double>(B, o_tsv);
+  d.rkh = at<double>(B, o_rkh); d.rku = at<double>(B, o_rku); d.rkv = at<double>(B, o_rkv);
+  d.u_a = at<double>(B, o_ua); d.v_a = at<double>(B, o_va); d.u_b = at<double>(B, o_ub); d.v_b = at<double>(B, o_vb);
+  d.delh_x = at<double>(B, o_g[0]); d.delh_y = at<double>(B, o_g[1]); d.delu_x = at<double>(B, o_g[2]);
+  d.delu_y = at<double>(B, o_g[3]); d.delv_x = at<double>(B, o_g[4]); d.delv_y = at<double>(B, o_g[5]);
+  d.dry_a = at<uint8_t>(B, o_dra); d.dry_b = at<uint8_t>(B, o_drb); d.hvtx = at<double>(B, o_hv);
+  d.vwet = at<uint8_t>(B, o_vw); d.phimax = at<double>(B, o_pm); d.bc_c = at<double>(B, o_bcc3);
+  d.bc_rec = at<double>(B, o_rec); d.part = at<double>(B, o_part); d.nblk_red = nblk;
+  d.sc = at<Scalars>(B, o_sc);
+  // boundary values
+  Scalars s0{};
+  for (int b = 0; b < L.n_in; b++) s0.qin[b] = L.qin[b];
+  for (int b = 0; b < L.n_out; b++) s0.hbc[b] = L.hbc[b];
+  CK(cudaMemcpy(d.sc, &s0, sizeof s0, cudaMemcpyHostToDevice));
+  int maxcnt = 1;
+  for (int b = 0; b < L.nbdr; b++) maxcnt = std::max(maxcnt, L.bdr_cnt[b]);
+  h->bc_smem = (size_t)maxcnt * 2 * sizeof(double) + (((size_t)maxcnt + 7) & ~(size_t)7);
+  if (h->bc_smem > 48 * 1024) CK(cudaFuncSetAttribute(k_bc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->bc_smem));
+  return 0;
+}
+
+template <class Tv>
+void scatter_old(const std::vector<int32_t>& new2old, const Tv* src_new, Tv* dst_old, size_t n) {
+  for (size_t i = 0; i < n; i++) dst_old[new2old[i]] = src_new[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* storm_fvt_last_error(void) { return g_err.c_str(); }
+
+void storm_fvt_default_options(StormFvtOptions* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->h_dry = 0.001;
+  o->h_wet = 0.001;
+  o->cfl = 1.0;
+  o->vceiling = 35.0;
+  o->rstop = (double)1.0e-4f;
+  const double t = 18.0;  // viscosity.f90 at temp = 18 C
+  o->visc = (double)1.792e-6f / (1.0 + 0.0337 * t + 0.000221 * t * t);
+  o->steady = 1;
+  o->dt_op = 0;
+  o->rkorder = 2;
+  o->opt_limiter = 2;
+  o->btype = 0;
+  o->hvalve = 1;
+  o->vclip = 0;
+  o->opt_friction = 0;
+  o->stop_cr = 0;
+  o->flux = STORM_FLUX_ROE;
+  o->precision = STORM_PREC_FP64;
+  o->device = 0;
+}
+
+int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, StormFvtHandle** out) {
+  clear_error();
+  if (!mesh || !opt || !out) return set_error(STORM_ERR_ARG, "storm_fvt_create: null argument");
+  *out = nullptr;
+  int rc = check_options(*opt);
+  if (rc) return rc;
+  StormFvtHandle* h = new (std::nothrow) StormFvtHandle();
+  if (!h) return set_error(STORM_ERR_NOMEM, "storm_fvt_create: out of memory");
+  h->opt = *opt;
+  h->device = opt->device;
+  try {
+    rc = build_layout(*mesh, *opt, h->L);
+  } catch (const std::bad_alloc&) {
+    rc = set_error(STORM_ERR_NOMEM, "storm_fvt_create: host out of memory");
+  }
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    delete h;
+    return set_error(STORM_ERR_CUDA, std::string("storm_fvt_create: no CUDA device: ") + cudaGetErrorString(e));
+  }
+  if (h->device < 0 || h->device >= ndev) {
+    delete h;
+    return set_error(STORM_ERR_ARG, "storm_fvt_create: device ordinal out of range");
+  }
+  e = cudaSetDevice(h->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
+  if (e == cudaSuccess) e = cudaMallocHost(&h->sc_host, sizeof(Scalars));
+  if (e != cudaSuccess) {
+    release(h);
+    return set_error(STORM_ERR_CUDA, std::string("storm_fvt_create: ") + cudaGetErrorString(e));
+  }
+  if ((rc = upload(h)) || (rc = capture_graph(h))) {
+    std::string msg = g_err;
+    release(h);
+    return set_error(rc, msg);
+  }
+  *out = h;
+  return STORM_OK;
+}
+
+int storm_fvt_set_state(StormFvtHandle* h, const double* hh, const double* u, const double* v) {
+  clear_error();
+  if (!h || !hh || !u || !v) return set_error(STORM_ERR_ARG, "storm_fvt_set_state: null argument");
+  CK(cudaSetDevice(h->device));
+  const int T = h->L.T;
+  std::vector<double> buf(3 * (size_t)T);
+  for (int c = 0; c < T; c++) {
+    int o = h->L.cell_old[c];
+    buf[c] = hh[o];
+    buf[T + c] = u[o];
+    buf[2 * (size_t)T + c] = v[o];
+  }
+  const Dev& d = h->d;
+  CK(cudaMemcpyAsync(d.rkh, buf.data(), 8 * (size_t)T, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(d.u_a, buf.data() + T, 8 * (size_t)T, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(d.v_a, buf.data() + 2 * (size_t)T, 8 * (size_t)T, cudaMemcpyHostToDevice, h->stream));
+  const int nblk = (T + kRed - 1) / kRed;
+  k_init<<<nblk, kRed, 0, h->stream>>>(d);
+  k_init_final<<<1, kRed, 0, h->stream>>>(d, nblk);
+  CK(cudaGetLastError());
+  h->launches += 2;
+  CK(cudaStreamSynchronize(h->stream));
+  h->have_state = true;
+  return STORM_OK;
+}
+
+int storm_fvt_step(StormFvtHandle* h, int32_t nsteps, StormFvtStepStats* stats) {
+  clear_error();
+  if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_step: null handle");
+  if (!h->have_state) return set_error(STORM_ERR_ARG, "storm_fvt_step: state not set");
+  if (nsteps < 0) return set_error(STORM_ERR_ARG, "storm_fvt_step: negative step count");
+  CK(cudaSetDevice(h->device));
+  const int K = h->opt.rkorder;
+  const int poll = h->opt.steady ? 16 : (1 << 30);
+  h->last_flux_ms = 0.0;
+  h->last_flux_launches = 0;
+  CK(cudaEventRecord(h->ev0, h->stream));
+  if (h->timing) {
+    const size_t need = 2 * (size_t)(h->kernels_per_step + 2) * nsteps;
+    while (h->fev.size() < need) {
+      cudaEvent_t ev;
+      CK(cudaEventCreate(&ev));
+      h->fev.push_back(ev);
+    }
+    h->fev_class.assign(need / 2, 0);
+    size_t used = 0;
+    for (int i = 0; i < nsteps; i++) {
+      int rc = enqueue_step(h, true, &used);
+      if (rc) return rc;
+      h->launches += h->kernels_per_step;
+    }
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < 8; c++) {
+      h->kt_ms[c] = 0.0;
+      h->kt_n[c] = 0;
+    }
+    for (size_t i = 0; i + 1 < used; i += 2) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, h->fev[i], h->fev[i + 1]));
+      const int c = h->fev_class[i / 2];
+      h->kt_ms[c] += ms;
+      h->kt_n[c] += 1;
+    }
+    h->last_flux_ms = h->kt_ms[KT_FLUX];
+    h->last_flux_launches = h->kt_n[KT_FLUX];
+  } else {
+    for (int i = 0; i < nsteps; i++) {
+      CK(cudaGraphLaunch(h->exec, h->stream));
+      h->launches += h->kernels_per_step;
+      if ((i + 1) % poll == 0 && i + 1 < nsteps) {
+        CK(cudaMemcpyAsync(h->sc_host, h->d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->sc_host->converged) break;
+      }
+    }
+    CK(cudaEventRecord(h->ev1, h->stream));
+  }
+  CK(cudaMemcpyAsync(h->sc_host, h->d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->last_step_ms = ms;
+  const Scalars& s = *h->sc_host;
+  if (stats) {
+    std::memset(stats, 0, sizeof *stats);
+    stats->iter = s.iter;
+    stats->converged = s.converged;
+    stats->ttime = s.ttime;
+    stats->stime = s.stime;
+    stats->delt = h->opt.steady ? s.delt_fric : s.delt;
+    stats->rmax = s.rmax;
+    stats->rms_dh = s.rms;
+    stats->tmass = s.tmass;
+    for (int b = 0; b < STORM_MAX_BDR; b++) {
+      stats->cqin3[b] = s.cqin3[b];
+      stats->cqout3[b] = s.cqout3[b];
+    }
+    stats->device_status = s.status;
+  }
+  if (s.status & 1)
+    return set_error(STORM_ERR_DEVICE, "storm_fvt_step: non-finite depth or velocity in the state");
+  return STORM_OK;
+}
+
+int storm_fvt_get_state(StormFvtHandle* h, double* hh, double* u, double* v, double* rkh, double* rku, double* rkv,
+                        double* hvtx) {
+  clear_error();
+  if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_get_state: null handle");
+  CK(cudaSetDevice(h->device));
+  const int T = h->L.T, N = h->L.N;
+  std::vector<double> buf(std::max(T, N));
+  auto pull = [&](const double* dev, double* dst, int n, const std::vector<int32_t>& perm) -> int {
+    if (!dst) return 0;
+    CK(cudaMemcpyAsync(buf.data(), dev, 8 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    scatter_old(perm, buf.data(), dst, n);
+    return 0;
+  };
+  const Dev& d = h->d;
+  int rc;
+  if ((rc = pull(d.rkh, hh, T, h->L.cell_old))) return rc;
+  if ((rc = pull(d.u_a, u, T, h->L.cell_old))) return rc;
+  if ((rc = pull(d.v_a, v, T, h->L.cell_old))) return rc;
+  if ((rc = pull(d.rkh, rkh, T, h->L.cell_old))) return rc;
+  if ((rc = pull(d.rku, rku, T, h->L.cell_old))) return rc;
+  if ((rc = pull(d.rkv, rkv, T, h->L.cell_old))) return rc;
+  if ((rc = pull(d.hvtx, hvtx, N, h->L.node_old))) return rc;
+  return STORM_OK;
+}
+
+int storm_fvt_get_drycell(StormFvtHandle* h, int32_t* dry) {
+  clear_error();
+  if (!h || !dry) return set_error(STORM_ERR_ARG, "storm_fvt_get_drycell: null argument");
+  CK(cudaSetDevice(h->device));
+  const int T = h->L.T;
+  std::vector<uint8_t> b(T);
+  CK(cudaMemcpyAsync(b.data(), h->d.dry_a, T, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < T; c++) dry[h->L.cell_old[c]] = b[c] ? 1 : 0;
+  return STORM_OK;
+}
+
+int64_t storm_fvt_kernel_launches(const StormFvtHandle* h) { return h ? h->launches : 0; }
+
+int storm_fvt_set_kernel_timing(StormFvtHandle* h, int32_t on) {
+  if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_set_kernel_timing: null handle");
+  h->timing = on != 0;
+  return STORM_OK;
+}
+
+int storm_fvt_last_timing(const StormFvtHandle* h, double* step_ms, double* flux_ms, int64_t* flux_launches) {
+  if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_last_timing: null handle");
+  if (step_ms) *step_ms = h->last_step_ms;
+  if (flux_ms) *flux_ms = h->last_flux_ms;
+  if (flux_launches) *flux_launches = h->last_flux_launches;
+  return STORM_OK;
+}
+
+int storm_fvt_kernel_times(const StormFvtHandle* h, double* ms, int64_t* launches) {
+  if (!h || !ms || !launches) return set_error(STORM_ERR_ARG, "storm_fvt_kernel_times: null argument");
+  for (int c = 0; c < 8; c++) {
+    ms[c] = h->kt_ms[c];
+    launches[c] = h->kt_n[c];
+  }
+  return STORM_OK;
+}
+
+int storm_fvt_destroy(StormFvtHandle* h) {
+  clear_error();
+  if (!h) return STORM_OK;
+  release(h);
+  return STORM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// fvt_device.cuh -- device-side data of the FVT step and the per-edge physics shared
+// by the kernels (flux functions, the reference's compare helpers).
+//
+// Every formula below is the reference's expression evaluated in the reference's
+// order (the library is compiled with --fmad=false, so no product is fused into a
+// sum): with the oracle's own inputs the kernels reproduce its results bit for bit
+// except where CUDA's pow() (friction) differs from the host libm.
+#pragma once
+
+#include <cstdint>
+
+namespace storm {
+
+constexpr int kMaxBdrDev = 16;
+
+// Per-handle scalars that live on the device (one struct, written by the kernels).
+struct Scalars {
+  int32_t iter;       // iterations completed
+  int32_t converged;  // steady: rmax < rstop reached (solverFVT.f90:431)
+  int32_t status;     // bit 0: non-finite state; bit 1: HLL wave-speed inversion
+  int32_t pad;
+  double delt;        // dt of the current iteration (unsteady), or the steady
+                      // last-element local dt carried into ttime (solverFVT.f90:155)
+  double delt_fric;   // steady: local dt of element n_elems in the last stage (N3)
+  double ttime, stime, rmax, rms, tmass;
+  double qin[kMaxBdrDev], hbc[kMaxBdrDev];
+  double cqin3[kMaxBdrDev], cqout3[kMaxBdrDev];
+};
+
+// Kernel parameters: options, the device layout and the state buffers.
+struct Dev {
+  int32_t T, N, K, kst, nbdr, nbce;
+  int32_t steady, dt_op, lim, btype, hvalve, vclip, fric, stop_cr, flux, last_cell;
+  int32_t n_in, n_out;
+  double h_dry, h_wet, cfl, vceiling, visc, rstop, bch_max;
+  double alpha[4][4], beta[4];
+  // cells
+  const double *area, *perim, *xc, *yc, *z, *delz_x, *delz_y, *zmax, *cd;
+  const double *lsq_a, *lsq_b, *lsq_c, *lsq_det;
+  const uint8_t *nst, *forder, *hvmask, *fkind;
+  const int32_t *vert, *t2t3, *fref, *st_id;
+  const double *rc_x, *rc_y, *fnx, *fny, *flen, *fz0, *st_w, *st_dx, *st_dy;
+  const int32_t *wall_p1, *wall_p2;
+  // nodes
+  const double *zvtx, *node_x, *node_y, *n2t_w;
+  const int32_t *n2t_off, *n2t_cell;
+  const int16_t* node_hbc;
+  // open boundaries
+  const int32_t *bdr_kind, *bdr_slot, *bdr_off, *bdr_cnt, *bce_cell, *bce_slot;
+  const double *bce_nx, *bce_ny, *bce_tx, *bce_ty, *bce_len, *bce_zmid;
+  const int32_t *ts_off, *ts_cnt, *out_type;
+  const double *ts_t, *ts_v;
+  // state
+  double *rkh, *rku, *rkv;  // [K+1][T]
+  double *u_a, *v_a;        // stage-input velocities (find_dry_cells, LSQ)
+  double *u_b, *v_b;        // velocities after hgradfix2 / to_vertices zeroing (fluxes)
+  double *delh_x, *delh_y, *delu_x, *delu_y, *delv_x, *delv_y;
+  uint8_t *dry_a, *dry_b;   // stage dry flags (ping-pong)
+  double* hvtx;             // vertex depth after enforce_bcs (wall fluxes, output)
+  uint8_t* vwet;            // hvtx > h_dry before enforce_bcs (to_vertices.f90:44-55)
+  double* phimax;           // MAX(|phi|) of the last stage (stop criterion)
+  double* bc_c;             // [3][nbce] boundary contributions to phi
+  double* bc_rec;           // [3][nbce] reconstructed boundary-edge h, u, v
+  double* part;             // [nblk][8] reduction partials
+  int32_t nblk_red;
+  Scalars* sc;
+};
+
+}  // namespace storm

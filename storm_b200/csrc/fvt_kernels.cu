@@ -1,0 +1,1111 @@
+// fvt_kernels.cu -- sm_100a kernels of one SToRM FVT iteration (solverFVT.f90:129-476).
+//
+// One RK stage (solverFVT.f90:161-325) is four launches:
+//   k_node  per node : ctr2vtxWSE type 3 + cap + positivity_vtx + enforce_bcs stage
+//                      nodes (to_vertices.f90:26-41, enforce_bcs.f90:37-56)
+//   k_grad  per cell : find_dry_cells state, lsq_grad_array x3, limiterBJ x3, delh -= delz
+//                      (cell_grads.f90), hgradfix2.f90:48-98, zeroing of cells with a
+//                      vertex depth <= h_dry (to_vertices.f90:44-55)
+//   k_bc    per open boundary (one CTA): inflowQbyH / inflowH / outflowbyH /
+//                      crit_outflow / free_flow, including the inflow fixed-point
+//   k_flux  per cell : every face flux of the cell (Roe/HLL/Rusanov, I1 wet/dry wall,
+//                      wenslp3/weslp2 walls, boundary contributions) gathered in the
+//                      order invisc_fluxes.f90 scatters them, bed_slope_STD + adjustZb,
+//                      the SSP-RK combination, vclip, h >= 0 and wet/dry hysteresis
+// and one iteration ends with
+//   k_fric  per cell : find_dry_cells, fric_terms_impl, the numerical valve, the
+//                      RK level copy, block partials of sumtop/sumbot/tmass/max|phi|/dt
+//   k_final one CTA  : deterministic reduction of the partials, stop test, clocks,
+//                      get_time_bcs.
+// No float atomics: every sum is a fixed-order tree or a serial loop, so the results
+// are reproducible run to run; every interior-edge flux is evaluated by both of its
+// cells with the same inputs in the same order, so both sides agree bit for bit.
+#include <cstdint>
+
+#include "fvt_device.cuh"
+#include "storm_internal.h"
+
+namespace storm {
+
+namespace {
+
+constexpr double kZero = 0.0;
+constexpr double kHalf = 0.5;
+constexpr double kOne = 1.0;
+constexpr double kOneThird = 1.0 / 3.0;
+constexpr double kG = 9.81;
+constexpr double kFmachp = 2.220446049250313e-16;   // EPSILON(zero)
+constexpr double kVsmall = 2.2250738585072014e-308; // TINY(zero)
+constexpr double kVlarge = 1.7976931348623157e+308; // HUGE(zero)
+#define SMALL_F ((double)1.0e-9f)                   // REAL(mp) :: small = 1.0E-9
+
+__device__ __forceinline__ double fmin2(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double fmax2(double a, double b) { return (b > a) ? b : a; }
+
+// equals.f90:1-27
+__device__ __forceinline__ bool equals(double a, double b) {
+  double eps = fabs(a) * kFmachp;
+  if (eps == kZero) eps = kVsmall;
+  return !(fabs(a - b) > eps);
+}
+
+// find_dry_cells.f90:25-42 for one cell; returns drycell and writes u_mag.
+__device__ __forceinline__ bool dry_flag(double h, double u, double v, double h_dry, double h_wet,
+                                         double* umag) {
+  bool dry = h < h_dry;
+  double um = kZero;
+  if (!dry) um = sqrt(u * u + v * v);
+  *umag = um;
+  if (!dry && (h < h_wet) && equals(um, kZero)) dry = true;
+  return dry;
+}
+
+// flux_ac.f90:48-126.  The MATMULs start from zero and add x(i,k)*y(k,j) for
+// k = 1..3; with the diagonal eigenvalue matrix (entries >= delta > 0) the first
+// product reduces exactly to rev(i,j)*eigv(j) + 0.
+__device__ __forceinline__ void flux_roe(double nx, double ny, double hleft, double uleft, double vleft,
+                                         double hright, double uright, double vright, double* flux) {
+  const double delta = 0.10;
+  double fl[3], gl[3], fr[3], gr[3];
+  fl[0] = hleft * uleft;
+  fl[1] = hleft * uleft * uleft + kHalf * kG * hleft * hleft;
+  fl[2] = hleft * uleft * vleft;
+  gl[0] = hleft * vleft;
+  gl[1] = hleft * uleft * vleft;
+  gl[2] = hleft * vleft * vleft + kHalf * kG * hleft * hleft;
+  fr[0] = hright * uright;
+  fr[1] = hright * uright * uright + kHalf * kG * hright * hright;
+  fr[2] = hright * uright * vright;
+  gr[0] = hright * vright;
+  gr[1] = hright * uright * vright;
+  gr[2] = hright * vright * vright + kHalf * kG * hright * hright;
+  hleft = fmax2(hleft, SMALL_F);
+  double hls = sqrt(hleft);
+  hright = fmax2(hright, SMALL_F);
+  double hrs = sqrt(hright);
+  double denom = hrs + hls;
+  double uavg = (uright * hrs + uleft * hls) / denom;
+  double vavg = (vright * hrs + vleft * hls) / denom;
+  double cavg = sqrt(kHalf * kG * (hleft + hright));
+  double q[3];
+  q[0] = hright - hleft;
+  q[1] = hright * uright - hleft * uleft;
+  q[2] = hright * vright - hleft * vleft;
+  double rev[3][3], lev[3][3], t1[3][3], eig[3];
+  rev[0][0] = kZero; rev[0][1] = kOne; rev[0][2] = kOne;
+  rev[1][0] = ny; rev[1][1] = uavg - cavg * nx; rev[1][2] = uavg + cavg * nx;
+  rev[2][0] = -nx; rev[2][1] = vavg - cavg * ny; rev[2][2] = vavg + cavg * ny;
+  lev[0][0] = -(uavg * ny - vavg * nx);
+  lev[0][1] = ny;
+  lev[0][2] = -nx;
+  lev[1][0] = kHalf * (uavg * nx + vavg * ny) / cavg + kHalf;
+  lev[1][1] = -(kHalf * nx / cavg);
+  lev[1][2] = -(kHalf * ny / cavg);
+  lev[2][0] = -(kHalf * (uavg * nx + vavg * ny) / cavg) + kHalf;
+  lev[2][1] = kHalf * nx / cavg;
+  lev[2][2] = kHalf * ny / cavg;
+  eig[0] = fmax2(fabs(uavg * nx + vavg * ny), delta);
+  eig[1] = fmax2(fabs(uavg * nx + vavg * ny - cavg), delta);
+  eig[2] = fmax2(fabs(uavg * nx + vavg * ny + cavg), delta);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) t1[i][j] = __dadd_rn(rev[i][j] * eig[j], kZero);
+  double aq[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    double t2[3];
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      t2[j] = (__dadd_rn(t1[i][0] * lev[0][j], kZero) + t1[i][1] * lev[1][j]) + t1[i][2] * lev[2][j];
+    aq[i] = (__dadd_rn(t2[0] * q[0], kZero) + t2[1] * q[1]) + t2[2] * q[2];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++) flux[i] = kHalf * (fr[i] * nx + gr[i] * ny + fl[i] * nx + gl[i] * ny - aq[i]);
+}
+
+// flux_HLL.f90:41-110 with its two defects fixed (flux(3) assigned; the whole HLL
+// numerator divided by sright - sleft).  The debug stop at :88-91 sets *bad.
+__device__ __forceinline__ void flux_hll(double nx, double ny, double hleft, double uleft, double vleft,
+                                         double hright, double uright, double vright, double h0, double* flux,
+                                         bool* bad) {
+  double cleft = sqrt(kG * hleft);
+  double cright = sqrt(kG * hright);
+  double ustar = kHalf * ((uleft + uright) * nx + (vleft + vright) * ny) + cleft - cright;
+  double cstar = kHalf * (cleft + cright) + ((uleft - uright) * nx + (vleft - vright) * ny) / 4.0;
+  double sleft, sright, aux1, aux2;
+  if (hleft < h0) sleft = uright * nx + vright * ny - 2.0 * cright;
+  else if (hright < h0) sleft = uleft * nx + vleft * ny - cleft;
+  else {
+    aux1 = uleft * nx + vleft * ny - cleft;
+    aux2 = ustar - cstar;
+    sleft = fmin2(aux1, aux2);
+  }
+  if (hleft < h0) sright = uright * nx + vright * ny + cright;
+  else if (hright < h0) sright = uleft * nx + vleft * ny + 2.0 * cleft;
+  else {
+    aux1 = uright * nx + vright * ny - cright;
+    aux2 = ustar + cstar;
+    sright = fmax2(aux1, aux2);
+  }
+  double fl[3], gl[3], fr[3], gr[3];
+  fl[0] = hleft * uleft * nx;
+  fl[1] = (hleft * uleft * uleft + kHalf * kG * hleft * hleft) * nx;
+  fl[2] = hleft * uleft * vleft * nx;
+  gl[0] = hleft * vleft * ny;
+  gl[1] = hleft * uleft * vleft * ny;
+  gl[2] = (hleft * vleft * vleft + kHalf * kG * hleft * hleft) * ny;
+  fr[0] = hright * uright * nx;
+  fr[1] = (hright * uright * uright + kHalf * kG * hright * hright) * nx;
+  fr[2] = hright * uright * vright * nx;
+  gr[0] = hright * vright * ny;
+  gr[1] = hright * uright * vright * ny;
+  gr[2] = (hright * vright * vright + kHalf * kG * hright * hright) * ny;
+  if (sleft > kZero && sright < kZero) *bad = true;
+  if (sleft > kZero) {
+    for (int i = 0; i < 3; i++) flux[i] = fl[i] + gl[i];
+  } else if (sright < kZero) {
+    for (int i = 0; i < 3; i++) flux[i] = fr[i] + gr[i];
+  } else {
+    aux1 = sright - sleft;
+    flux[0] = (sright * (fl[0] + gl[0]) - sleft * (fr[0] + gr[0]) + sleft * sright * (hright - hleft)) / aux1;
+    flux[1] = (sright * (fl[1] + gl[1]) - sleft * (fr[1] + gr[1]) +
+               sleft * sright * (hright * uright - hleft * uleft)) / aux1;
+    flux[2] = (sright * (fl[2] + gl[2]) - sleft * (fr[2] + gr[2]) +
+               sleft * sright * (hright * vright - hleft * vleft)) / aux1;
+  }
+}
+
+// flux_rusanov.f90:47-80
+__device__ __forceinline__ void flux_rusanov(double nx, double ny, double hleft, double uleft, double vleft,
+                                             double cl, double hright, double uright, double vright, double cr,
+                                             double* flux) {
+  double fl[3], gl[3], fr[3], gr[3], q[3];
+  fl[0] = hleft * uleft;
+  fl[1] = hleft * uleft * uleft + kHalf * kG * hleft * hleft;
+  fl[2] = hleft * uleft * vleft;
+  gl[0] = hleft * vleft;
+  gl[1] = hleft * uleft * vleft;
+  gl[2] = hleft * vleft * vleft + kHalf * kG * hleft * hleft;
+  fr[0] = hright * uright;
+  fr[1] = hright * uright * uright + kHalf * kG * hright * hright;
+  fr[2] = hright * uright * vright;
+  gr[0] = hright * vright;
+  gr[1] = hright * uright * vright;
+  gr[2] = hright * vright * vright + kHalf * kG * hright * hright;
+  double ul = uleft * nx + vleft * ny;
+  double ur = uright * nx + vright * ny;
+  double splus = fmax2(fabs(ul) + cl, fabs(ur) + cr);
+  q[0] = hright - hleft;
+  q[1] = hright * uright - hleft * uleft;
+  q[2] = hright * vright - hleft * vleft;
+#pragma unroll
+  for (int i = 0; i < 3; i++) flux[i] = kHalf * (fr[i] * nx + gr[i] * ny + fl[i] * nx + gl[i] * ny - splus * q[i]);
+}
+
+// Block-level reductions in a fixed order (warp xor-shuffle tree, then warps in order).
+template <int NT>
+__device__ __forceinline__ double block_sum(double x, double* sm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = x + __shfl_xor_sync(0xffffffffu, x, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sm[w] = x;
+  __syncthreads();
+  double r = kZero;
+  if (threadIdx.x == 0) {
+    r = sm[0];
+    for (int i = 1; i < NT / 32; i++) r = r + sm[i];
+  }
+  return r;  // valid on thread 0
+}
+template <int NT>
+__device__ __forceinline__ double block_max(double x, double* sm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmax2(x, __shfl_xor_sync(0xffffffffu, x, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sm[w] = x;
+  __syncthreads();
+  double r = kZero;
+  if (threadIdx.x == 0) {
+    r = sm[0];
+    for (int i = 1; i < NT / 32; i++) r = fmax2(r, sm[i]);
+  }
+  return r;
+}
+template <int NT>
+__device__ __forceinline__ double block_min(double x, double* sm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmin2(x, __shfl_xor_sync(0xffffffffu, x, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sm[w] = x;
+  __syncthreads();
+  double r = kZero;
+  if (threadIdx.x == 0) {
+    r = sm[0];
+    for (int i = 1; i < NT / 32; i++) r = fmin2(r, sm[i]);
+  }
+  return r;
+}
+
+// get_time_bcs.f90:31-77 (one thread)
+__device__ void time_bcs(const Dev& d, double time) {
+  Scalars* sc = d.sc;
+  for (int k = 0; k < d.n_out; k++) {
+    if (d.out_type[k] != 1) continue;
+    int n = d.ts_cnt[d.n_in + k];
+    if (n <= 0) continue;
+    const double* tl = d.ts_t + d.ts_off[d.n_in + k];
+    const double* ts = d.ts_v + d.ts_off[d.n_in + k];
+    if (time < tl[0]) sc->hbc[k] = ts[0];
+    else if (time >= tl[n - 1]) sc->hbc[k] = ts[n - 1];
+    else
+      for (int i = 0; i < n - 1; i++)
+        if (time >= tl[i] && time < tl[i + 1]) {
+          double delta = time - tl[i], delta2 = tl[i + 1] - tl[i];
+          sc->hbc[k] = ts[i] + delta * (ts[i + 1] - ts[i]) / delta2;
+          break;
+        }
+  }
+  for (int k = 0; k < d.n_in; k++) {
+    int n = d.ts_cnt[k];
+    if (n <= 0) continue;
+    const double* tl = d.ts_t + d.ts_off[k];
+    const double* ts = d.ts_v + d.ts_off[k];
+    if (time < tl[0]) sc->qin[k] = ts[0];
+    else if (time >= tl[n - 1]) sc->qin[k] = ts[n - 1];
+    else
+      for (int j = 0; j < n - 1; j++)
+        if (time >= tl[j] && time < tl[j + 1]) {
+          double delta = time - tl[j], delta2 = tl[j + 1] - tl[j];
+          sc->qin[k] = ts[j] + delta * (ts[j + 1] - ts[j]) / delta2;
+          break;
+        }
+  }
+}
+
+}  // namespace
+
+constexpr int kRedThreads = 256;
+
+// ---------------------------------------------------------------------------
+// Initial state: rk(:,0) = (h, h*u, h*v) (solverFVT.f90:122-126 then :138-142),
+// first-stage dry flags and the CFL dt partials of the initial state.
+__global__ void __launch_bounds__(kRedThreads) k_init(Dev d) {
+  __shared__ double sm[kRedThreads / 32];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double dtc = kVlarge;
+  if (c < d.T) {
+    double h = d.rkh[c], u = d.u_a[c], v = d.v_a[c];
+    d.rku[c] = h * u;
+    d.rkv[c] = h * v;
+    double um;
+    bool dry = dry_flag(h, u, v, d.h_dry, d.h_wet, &um);
+    d.dry_a[c] = dry;
+    double wc = dry ? kZero : sqrt(kG * h);
+    double dl = um + wc + SMALL_F;
+    dtc = d.cfl * d.area[c] / (dl * d.perim[c]);
+  }
+  double r = block_min<kRedThreads>(dtc, sm);
+  if (threadIdx.x == 0) d.part[8 * blockIdx.x + 4] = r;
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int nblk) {
+  __shared__ double sm[kRedThreads / 32];
+  double m = kVlarge;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) m = fmin2(m, d.part[8 * b + 4]);
+  double dtmin = block_min<kRedThreads>(m, sm);
+  if (threadIdx.x == 0) {
+    Scalars* sc = d.sc;
+    sc->iter = 0;
+    sc->converged = 0;
+    sc->status = 0;
+    sc->ttime = kZero;
+    sc->stime = kZero;
+    sc->rmax = kZero;
+    sc->rms = kZero;
+    sc->tmass = kZero;
+    sc->delt_fric = kZero;
+    for (int b = 0; b < kMaxBdrDev; b++) {
+      sc->cqin3[b] = kZero;
+      sc->cqout3[b] = kZero;
+    }
+    time_bcs(d, kZero);
+    if (d.steady) sc->delt = kZero;  // delt is first set inside the RK loop
+    else sc->delt = (d.dt_op == 0) ? d.cfl : dtmin;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Vertex water surface and depth of one stage.
+__global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N || d.sc->converged) return;
+  const int b0 = d.n2t_off[n], b1 = d.n2t_off[n + 1];
+  const double zv0 = d.zvtx[n];
+  double id = kZero, a = kZero, zetaref = zv0;
+  int counter = 0;
+  for (int q = b0; q < b1; q++) {
+    const int k = d.n2t_cell[q];
+    if (dry[k]) continue;
+    const double zeta = hs[k] + d.z[k];
+    const double w = d.n2t_w[q];
+    counter++;
+    id = id + w;
+    a = a + w * zeta;
+    zetaref = fmax2(zeta, zetaref);
+  }
+  double zv = counter > 0 ? a / id : zv0;
+  zv = fmin2(zv, zetaref);
+  double hv = zv - zv0;
+  if (hv < kZero) hv = kZero;
+  d.vwet[n] = hv > d.h_dry;
+  const int b = d.node_hbc[n];
+  if (b >= 0) hv = fmax2(kZero, d.sc->hbc[b] - zv0);
+  d.hvtx[n] = hv;
+}
+
+// ---------------------------------------------------------------------------
+// Limited LSQ gradients, hgradfix2 and the partially-wet velocity zeroing.
+__global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry,
+                                              double* __restrict__ rku_prev, double* __restrict__ rkv_prev) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.T || d.sc->converged) return;
+  const int T = d.T;
+  const double zeta_c = hs[c] + d.z[c];
+  const double u_c = d.u_a[c], v_c = d.v_a[c];
+  double hx = kZero, hy = kZero, ux = kZero, uy = kZero, vx = kZero, vy = kZero;
+  if (d.lim == 1 || d.lim == 2) {
+    double dz = kZero, ez = kZero, du = kZero, eu = kZero, dv = kZero, ev = kZero;
+    const int n = d.nst[c];
+    for (int k = 0; k < n; k++) {
+      const size_t q = (size_t)k * T + c;
+      const int j = d.st_id[q];
+      const double w = d.st_w[q], dx = d.st_dx[q], dy = d.st_dy[q];
+      const double pz = (hs[j] + d.z[j]) - zeta_c;
+      const double pu = d.u_a[j] - u_c;
+      const double pv = d.v_a[j] - v_c;
+      dz = dz + w * pz * dx;
+      ez = ez + w * pz * dy;
+      du = du + w * pu * dx;
+      eu = eu + w * pu * dy;
+      dv = dv + w * pv * dx;
+      ev = ev + w * pv * dy;
+    }
+    const double ai = d.lsq_a[c], bi = d.lsq_b[c], ci = d.lsq_c[c], det = d.lsq_det[c];
+    hx = (ci * dz - bi * ez) / det;
+    hy = (ai * ez - dz * bi) / det;
+    ux = (ci * du - bi * eu) / det;
+    uy = (ai * eu - du * bi) / det;
+    vx = (ci * dv - bi * ev) / det;
+    vy = (ai * ev - dv * bi) / det;
+  }
+  if (d.lim == 2) {  // limiterBJ.f90:42-81, beta = one
+    double qn[3][3], rcx[3], rcy[3];
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const size_t q = (size_t)j * T + c;
+      const int k = d.t2t3[q];
+      rcx[j] = d.rc_x[q];
+      rcy[j] = d.rc_y[q];
+      if (k < 0) {
+        qn[0][j] = zeta_c; qn[1][j] = u_c; qn[2][j] = v_c;
+      } else {
+        qn[0][j] = hs[k] + d.z[k]; qn[1][j] = d.u_a[k]; qn[2][j] = d.v_a[k];
+      }
+    }
+    double* gx[3] = {&hx, &ux, &vx};
+    double* gy[3] = {&hy, &uy, &vy};
+    const double q0v[3] = {zeta_c, u_c, v_c};
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+      const double q0 = q0v[f];
+      double r[3];
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const double qmin = fmin2(q0, qn[f][j]);
+        const double qmax = fmax2(q0, qn[f][j]);
+        const double qj = q0 + *gx[f] * rcx[j] + *gy[f] * rcy[j];
+        const double delq = qj - q0;
+        double rj;
+        if (equals(delq, kZero)) rj = kOne;
+        else if (delq < 0) rj = (qmin - q0) / delq;
+        else rj = (qmax - q0) / delq;
+        const double a = fmin2(kOne * rj, kOne);
+        const double b = fmin2(rj, kOne);
+        r[j] = fmax2(a, b);
+      }
+      const double phi = fmin2(fmin2(r[0], r[1]), r[2]);
+      *gx[f] = phi * *gx[f];
+      *gy[f] = phi * *gy[f];
+    }
+  }
+  hx = hx - d.delz_x[c];
+  hy = hy - d.delz_y[c];
+  double ub = u_c, vb = v_c;
+  if (!dry[c]) {
+    // hgradfix2.f90:48-98
+    bool setgrad = zeta_c < d.zmax[c];
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const int l = d.t2t3[(size_t)j * T + c];
+      if (l < 0) continue;
+      if (dry[l] && d.z[l] < zeta_c) setgrad = false;
+    }
+    if (setgrad) {
+      hx = -d.delz_x[c];
+      hy = -d.delz_y[c];
+      ub = kZero;
+      vb = kZero;
+      rku_prev[c] = kZero;
+      rkv_prev[c] = kZero;
+      ux = kZero; uy = kZero; vx = kZero; vy = kZero;
+    }
+    // to_vertices.f90:44-55
+    bool flag = true;
+#pragma unroll
+    for (int j = 0; j < 3; j++) flag = flag && d.vwet[d.vert[(size_t)j * T + c]];
+    if (!flag) {
+      ub = kZero;
+      vb = kZero;
+    }
+  }
+  d.delh_x[c] = hx; d.delh_y[c] = hy;
+  d.delu_x[c] = ux; d.delu_y[c] = uy;
+  d.delv_x[c] = vx; d.delv_y[c] = vy;
+  d.u_b[c] = ub;
+  d.v_b[c] = vb;
+}
+
+// ---------------------------------------------------------------------------
+// Open-boundary fluxes (invisc_fluxes.f90:218-238), one CTA per boundary.  The
+// per-edge arithmetic runs on all threads; the sums the reference accumulates
+// serially (atotal, newatotal, qtotal, cqin3/cqout3) are added by thread 0 in
+// string order, so they round exactly as the reference's loops.
+constexpr int kBcThreads = 128;
+
+__global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, const double* __restrict__ hs,
+                                                   const uint8_t* __restrict__ dry) {
+  if (d.sc->converged) return;
+  extern __shared__ double smb[];
+  const int b = blockIdx.x;
+  const int kind = d.bdr_kind[b], slot = d.bdr_slot[b];
+  const int off = d.bdr_off[b], cnt = d.bdr_cnt[b];
+  const int T = d.T, NB = d.nbce;
+  double* tA = smb;            // [cnt]
+  double* tB = smb + cnt;      // [cnt]
+  uint8_t* ok = (uint8_t*)(smb + 2 * cnt);
+  __shared__ double s_atotal;
+  __shared__ int s_done, s_null;
+  const double h_dry = d.h_dry;
+  // reconstructed edge states (the h/u/v + grad . rc of the boundary element)
+  for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+    const int i = d.bce_cell[off + e], m = d.bce_slot[off + e];
+    const size_t q = (size_t)m * T + i;
+    d.bc_rec[off + e] = hs[i] + d.delh_x[i] * d.rc_x[q] + d.delh_y[i] * d.rc_y[q];
+    d.bc_rec[NB + off + e] = d.u_b[i] + d.delu_x[i] * d.rc_x[q] + d.delu_y[i] * d.rc_y[q];
+    d.bc_rec[2 * NB + off + e] = d.v_b[i] + d.delv_x[i] * d.rc_x[q] + d.delv_y[i] * d.rc_y[q];
+  }
+  __syncthreads();
+  auto put = [&](int e, double c1, double c2, double c3) {
+    d.bc_c[off + e] = c1;
+    d.bc_c[NB + off + e] = c2;
+    d.bc_c[2 * NB + off + e] = c3;
+  };
+  if (kind == BC_QBYH || kind == BC_QBYH_WET) {  // inflowQbyH.f90:31-212 / :221-402
+    const bool wet_only = kind == BC_QBYH_WET;
+    const double qin = d.sc->qin[slot];
+    if (qin < kVsmall) {
+      for (int e = threadIdx.x; e < cnt; e += blockDim.x) put(e, kZero, kZero, kZero);
+      if (threadIdx.x == 0) d.sc->cqin3[slot] = kZero;
+      return;
+    }
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+      const int i = d.bce_cell[off + e];
+      const bool dr = dry[i];
+      ok[e] = !(wet_only && dr);
+      double hleft = dr ? kZero : fmax2(d.bc_rec[off + e], kZero);
+      tA[e] = hleft * d.bce_len[off + e];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double at = kZero;
+      for (int e = 0; e < cnt; e++)
+        if (ok[e]) at = at + tA[e];
+      s_atotal = at;
+      s_null = equals(at, kZero);
+      s_done = 0;
+    }
+    __syncthreads();
+    const bool null_area = s_null;
+    // fixed-point iteration on the total flow area (:61-126)
+    double newatotal = kZero;
+    for (int counter = 0;; counter++) {
+      const double atotal = s_atotal;
+      for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+        const int i = d.bce_cell[off + e];
+        bool valid = !(wet_only && dry[i]);
+        double hleft = null_area ? d.bch_max : d.bc_rec[off + e], uedg, vedg;
+        if (hleft < h_dry) {
+          hleft = fmax2(hleft, kZero);
+          uedg = kZero;
+          vedg = kZero;
+        } else {
+          uedg = d.bc_rec[NB + off + e];
+          vedg = d.bc_rec[2 * NB + off + e];
+        }
+        const double nx = d.bce_nx[off + e], ny = d.bce_ny[off + e], len = d.bce_len[off + e];
+        const double qfrac = qin / atotal;
+        double uright = -qfrac;
+        const double uleft = uedg * nx + vedg * ny;
+        const double sq = sqrt(kG * hleft);
+        double hright = 2.0 * sq + uleft - uright;
+        hright = hright * hright / 4.0 / kG;
+        uright = -qfrac * nx;
+        const double vright = -qfrac * ny;
+        if (hright < h_dry) valid = false;
+        ok[e] = valid;
+        tA[e] = hright * len;
+        tB[e] = (uright * nx + vright * ny) * hright * len;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double na = kZero, qt = kZero;
+        for (int e = 0; e < cnt; e++)
+          if (ok[e]) {
+            na = na + tA[e];
+            qt = qt + tB[e];
+          }
+        qt = fabs(qt);
+        if (fabs(qt - qin) / qin < 0.005 || counter > 50) s_done = 1;
+        else s_atotal = na;
+        tA[0] = na;  // hand newatotal to every thread through shared memory
+      }
+      __syncthreads();
+      newatotal = tA[0];
+      const int done = s_done;
+      __syncthreads();
+      if (done) break;
+    }
+    const double atotal = newatotal;  // :130
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+      const int i = d.bce_cell[off + e];
+      bool valid = !(wet_only && dry[i]);
+      double hleft = null_area ? d.bch_max : d.bc_rec[off + e], uedg, vedg;
+      if (hleft < h_dry) {
+        hleft = fmax2(hleft, kZero);
+        uedg = kZero;
+        vedg = kZero;
+      } else {
+        uedg = d.bc_rec[NB + off + e];
+        vedg = d.bc_rec[2 * NB + off + e];
+      }
+      const double nx = d.bce_nx[off + e], ny = d.bce_ny[off + e], len = d.bce_len[off + e];
+      const double qfrac = qin / atotal;
+      double uright = -qfrac;
+      const double uleft = uedg * nx + vedg * ny;
+      const double sq = sqrt(kG * hleft);
+      double hright = 2.0 * sq + uleft - uright;
+      hright = hright * hright / 4.0 / kG;
+      uright = -qfrac * nx;
+      const double vright = -qfrac * ny;
+      if (hright < h_dry) valid = false;
+      ok[e] = valid;
+      if (valid) {
+        const double f1 = hright * (uright * nx + vright * ny);
+        const double f2 = hright * uright * (uright * nx + vright * ny) + kHalf * kG * hright * hright * nx;
+        const double f3 = hright * vright * (uright * nx + vright * ny) + kHalf * kG * hright * hright * ny;
+        tA[e] = f1 * len;
+        put(e, f1 * len, f2 * len, f3 * len);
+      } else {
+        put(e, kZero, kZero, kZero);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double cq = kZero;
+      for (int e = 0; e < cnt; e++)
+        if (ok[e]) cq = cq + tA[e];
+      d.sc->cqin3[slot] = cq;
+    }
+    return;
+  }
+  // The remaining routines have no cross-edge coupling.
+  for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+    const int i = d.bce_cell[off + e];
+    const bool dr = dry[i];
+    const double nx = d.bce_nx[off + e], ny = d.bce_ny[off + e];
+    const double tx = d.bce_tx[off + e], ty = d.bce_ty[off + e];
+    const double len = d.bce_len[off + e], zmid = d.bce_zmid[off + e];
+    double hleft = d.bc_rec[off + e];
+    const double ur0 = d.bc_rec[NB + off + e], vr0 = d.bc_rec[2 * NB + off + e];
+    double f[3] = {kZero, kZero, kZero};
+    bool valid = true;
+    if (kind == BC_HIN) {  // inflowH.f90:28-93
+      double uedg, vedg;
+      hleft = fmax2(hleft, kZero);
+      if (hs[i] < h_dry) { uedg = kZero; vedg = kZero; }
+      else { uedg = ur0; vedg = vr0; }
+      const double hright = fmax2(kZero, d.sc->qin[slot] - zmid);
+      double uleft = uedg * nx + vedg * ny;
+      const double sl = sqrt(kG * hleft), sr = sqrt(kG * hright);
+      double uright = uleft + (sl - sr);
+      const double vright = uright * ny;
+      uright = uright * nx;
+      uleft = uedg;
+      const double vleft = vedg;
+      if (hleft < h_dry && hright < h_dry) valid = false;
+      else flux_roe(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
+      if (valid) { tA[e] = f[0] * len; put(e, f[0] * len, f[1] * len, f[2] * len); }
+    } else if (kind == BC_HOUT) {  // outflowbyH.f90:30-137
+      double uedg, vedg;
+      if (dr || hleft < h_dry) { uedg = kZero; vedg = kZero; hleft = fmax2(hleft, kZero); }
+      else { uedg = ur0; vedg = vr0; }
+      double hright = fmax2(kZero, d.sc->hbc[slot] - zmid);
+      if (hleft < h_dry && hright < h_dry) valid = false;
+      else {
+        double uleft, vleft, uright, vright;
+        if (hright < h_dry) {
+          uright = kZero; uleft = uedg; vright = kZero; vleft = vedg;
+        } else {
+          uleft = uedg * nx + vedg * ny;
+          vleft = uedg * tx + vedg * ty;
+          const double sl = sqrt(kG * hleft), sr = sqrt(kG * hright);
+          uright = uleft + (sl - sr);
+          vright = vleft;
+          uleft = uedg;
+          vleft = vedg;
+          uedg = uright;
+          vedg = vright;
+          uright = uedg * nx + vedg * tx;
+          vright = uedg * ny + vedg * ty;
+        }
+        bool set_wall = false;
+        if (d.hvalve) {
+          const double dot = uright * nx + vright * ny;
+          if (dot < kZero) { set_wall = true; hright = hleft; uright = kZero; vright = kZero; }
+        }
+        flux_roe(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
+        if (set_wall) f[0] = kZero;
+        tA[e] = f[0] * len;
+        put(e, f[0] * len, f[1] * len, f[2] * len);
+      }
+    } else if (kind == BC_CRIT) {  // crit_outflow.f90:29-107
+      double uedg, vedg;
+      if (dr || hleft < h_dry) { uedg = kZero; vedg = kZero; hleft = fmax2(hleft, kZero); }
+      else { uedg = ur0; vedg = vr0; }
+      if (hleft < h_dry) valid = false;
+      else {
+        const double uleft = uedg * nx + vedg * ny;
+        const double vleft = uedg * tx + vedg * ty;
+        double uright = uleft, vright = vleft;
+        double hright = uright * uright / kG;
+        uedg = uright;
+        vedg = vright;
+        uright = uedg * nx + vedg * tx;
+        vright = uedg * ny + vedg * ty;
+        if (d.hvalve) {
+          const double dot = uright * nx + vright * ny;
+          if (dot < kZero) { hright = hleft; uright = kZero; vright = kZero; }
+        }
+        f[0] = hright * (uright * nx + vright * ny);
+        f[1] = hright * uright * (uright * nx + vright * ny) + kHalf * kG * hright * hright * nx;
+        f[2] = hright * vright * (uright * nx + vright * ny) + kHalf * kG * hright * hright * ny;
+        const double dh = kZero;  // :97-99
+        tA[e] = f[0] * len;
+        put(e, f[0] * len, (f[1] + dh * nx) * len, (f[2] + dh * ny) * len);
+      }
+    } else {  // BC_FREE, free_flow.f90:30-93
+      double uedg, vedg;
+      hleft = fmax2(hleft, kZero);
+      if (hleft < h_dry) valid = false;
+      else {
+        if (hs[i] < h_dry) { uedg = kZero; vedg = kZero; }
+        else { uedg = ur0; vedg = vr0; }
+        const double uleft = uedg, vleft = vedg;
+        double hright = hleft, uright = uleft, vright = vleft;
+        bool set_wall = false;
+        if (d.hvalve) {
+          const double dot = uright * nx + vright * ny;
+          if (dot < 0) { set_wall = true; uright = kZero; vright = kZero; }
+        }
+        flux_roe(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
+        if (set_wall) f[0] = kZero;
+        put(e, f[0] * len, f[1] * len, f[2] * len);
+      }
+    }
+    ok[e] = valid;
+    if (!valid) put(e, kZero, kZero, kZero);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && kind != BC_FREE) {
+    double cq = kZero;
+    for (int e = 0; e < cnt; e++)
+      if (ok[e]) cq = cq + tA[e];
+    if (kind == BC_HIN) d.sc->cqin3[slot] = cq;
+    else d.sc->cqout3[slot] = cq;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reconstructed edge state of cell x at its local slot m (invisc_fluxes.f90:53-81).
+struct EdgeState {
+  double h, u, v;
+};
+
+__device__ __forceinline__ EdgeState edge_state(const Dev& d, const double* __restrict__ hs, int x, int m) {
+  const size_t q = (size_t)m * d.T + x;
+  const double rx = d.rc_x[q], ry = d.rc_y[q];
+  EdgeState s;
+  s.h = hs[x] + d.delh_x[x] * rx + d.delh_y[x] * ry;
+  if (s.h < kZero) s.h = kZero;
+  s.u = d.u_b[x] + d.delu_x[x] * rx + d.delu_y[x] * ry;
+  s.v = d.v_b[x] + d.delv_x[x] * rx + d.delv_y[x] * ry;
+  return s;
+}
+
+// invisc_fluxes.f90:39-147 for the interior edge between L=e(1) (slot ml) and
+// R=e(2) (slot mr); returns false when the edge is skipped.
+__device__ __forceinline__ bool interior_flux(const Dev& d, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, int L, int ml, int R, int mr,
+                                              double nx, double ny, double z0e, double* f, bool* bad) {
+  const bool dl = dry[L], dr = dry[R];
+  if (dl && dr) return false;
+  double hleft = kZero, uleft = kZero, vleft = kZero, hright = kZero, uright = kZero, vright = kZero;
+  if (!dl) {
+    EdgeState s = edge_state(d, hs, L, ml);
+    hleft = s.h; uleft = s.u; vleft = s.v;
+  }
+  if (!dr) {
+    EdgeState s = edge_state(d, hs, R, mr);
+    hright = s.h; uright = s.u; vright = s.v;
+  }
+  if (hleft < d.h_dry && hright < d.h_dry) return false;
+  bool set_wall = false;
+  if (dl || dr) {  // ALGORITHM I1
+    double h0 = fmax2(hright, hleft);
+    h0 = h0 + z0e;
+    if (dl)
+      if (d.z[L] + d.h_wet > h0) { set_wall = true; hleft = hright; }
+    if (dr)
+      if (d.z[R] + d.h_wet > h0) { set_wall = true; hright = hleft; }
+  }
+  if (set_wall) {
+    f[0] = kZero;
+    hleft = fmax2(hleft, hright);
+    f[1] = kHalf * kG * hleft * hleft * nx;
+    f[2] = kHalf * kG * hleft * hleft * ny;
+  } else if (d.flux == STORM_FLUX_HLL) {
+    flux_hll(nx, ny, hleft, uleft, vleft, hright, uright, vright, d.h_dry, f, bad);
+  } else if (d.flux == STORM_FLUX_RUSANOV) {
+    const double cl = dl ? kZero : sqrt(kG * hs[L]);  // wavec (solverFVT.f90:180-181)
+    const double cr = dr ? kZero : sqrt(kG * hs[R]);
+    flux_rusanov(nx, ny, hleft, uleft, vleft, cl, hright, uright, vright, cr, f);
+  } else {
+    flux_roe(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
+  }
+  return true;
+}
+
+// Fluxes, sources and the RK update of stage s (1-based) for one cell.
+__global__ void __launch_bounds__(128) k_flux(Dev d, int s, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.T || d.sc->converged) return;
+  const int T = d.T;
+  const bool dry_c = dry[c];
+  const double h_c = hs[c];
+  double p1 = kZero, p2 = kZero, p3 = kZero;  // phi = zero (solverFVT.f90:194)
+  bool bad = false;
+  const uint8_t ord = d.forder[c];
+#pragma unroll 1
+  for (int t = 0; t < 3; t++) {
+    const int j = (ord >> (2 * t)) & 3;
+    const size_t q = (size_t)j * T + c;
+    const uint8_t fk = d.fkind[q];
+    const int kind = fk & 7;
+    if (kind == FACE_LEFT || kind == FACE_RIGHT) {
+      const int nb = d.fref[q], ns = fk >> 4;
+      double f[3];
+      const bool left = kind == FACE_LEFT;
+      if (interior_flux(d, hs, dry, left ? c : nb, left ? j : ns, left ? nb : c, left ? ns : j, d.fnx[q], d.fny[q],
+                        d.fz0[q], f, &bad)) {
+        const double len = d.flen[q];
+        if (left) {
+          p1 = p1 - f[0] * len;
+          p2 = p2 - f[1] * len;
+          p3 = p3 - f[2] * len;
+        } else {
+          p1 = p1 + f[0] * len;
+          p2 = p2 + f[1] * len;
+          p3 = p3 + f[2] * len;
+        }
+      }
+    } else if (kind == FACE_WALL) {
+      if (dry_c) continue;
+      const double nx = d.fnx[q], ny = d.fny[q], len = d.flen[q];
+      if (d.btype == 0) {  // wenslp3_fluxes.f90:34-67
+        const int w = d.fref[q];
+        const double h1 = d.hvtx[d.wall_p1[w]], h2 = d.hvtx[d.wall_p2[w]];
+        double hedge = sqrt((h1 * h1 + h1 * h2 + h2 * h2) * kOneThird);
+        if (hedge < kZero) hedge = kZero;
+        if (hedge < d.h_dry) continue;
+        p2 = p2 - kHalf * kG * hedge * hedge * nx * len;
+        p3 = p3 - kHalf * kG * hedge * hedge * ny * len;
+      } else {  // weslp2_fluxes.f90:34-76
+        const size_t qc = (size_t)j * T + c;
+        const double rx = d.rc_x[qc], ry = d.rc_y[qc];
+        const double hleft = h_c + d.delh_x[c] * rx + d.delh_y[c] * ry;
+        if (hleft < d.h_dry) continue;
+        const double uleft = d.u_b[c] + d.delu_x[c] * rx + d.delu_y[c] * ry;
+        const double vleft = d.v_b[c] + d.delv_x[c] * rx + d.delv_y[c] * ry;
+        const double tx = -ny, ty = nx;  // edges%tang flipped with the normal
+        double uright = uleft * tx + vleft * ty;
+        uright = uright + 2.0 * sqrt(kG * hleft);
+        const double hright = uright * uright / 4.0 / kG;
+        const double f2 = kHalf * kG * hright * hright * nx;
+        const double f3 = kHalf * kG * hright * hright * ny;
+        const double dh = kZero;
+        p2 = p2 - (f2 + dh * nx) * len;
+        p3 = p3 - (f3 + dh * ny) * len;
+      }
+    } else if (kind == FACE_BC) {
+      const int e = d.fref[q];
+      p1 = p1 - d.bc_c[e];
+      p2 = p2 - d.bc_c[d.nbce + e];
+      p3 = p3 - d.bc_c[2 * d.nbce + e];
+    }
+  }
+  // bed_slope_STD.f90:23-70 with adjustZb.f90:41-70
+  if (!dry_c) {
+    const double dhx = d.delh_x[c], dhy = d.delh_y[c], xc = d.xc[c], yc = d.yc[c];
+    int vid[3];
+    double hp[3];
+    bool adjust = false;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      vid[i] = d.vert[(size_t)i * T + c];
+      hp[i] = h_c + dhx * (d.node_x[vid[i]] - xc) + dhy * (d.node_y[vid[i]] - yc);
+      if (hp[i] < kZero) adjust = true;
+    }
+    double gx, gy;
+    if (adjust) {
+      double zp[3], x[3], y[3];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        hp[i] = fmin2(kZero, hp[i]);
+        zp[i] = d.zvtx[vid[i]] + hp[i];
+        x[i] = d.node_x[vid[i]];
+        y[i] = d.node_y[vid[i]];
+      }
+      const double b1 = y[1] - y[2], c1 = x[2] - x[1];
+      const double b2 = y[2] - y[0], c2 = x[0] - x[2];
+      const double b3 = y[0] - y[1], c3 = x[1] - x[0];
+      const double a = kHalf / d.area[c];
+      gx = a * (b1 * zp[0] + b2 * zp[1] + b3 * zp[2]);
+      gy = a * (c1 * zp[0] + c2 * zp[1] + c3 * zp[2]);
+    } else {
+      gx = d.delz_x[c];
+      gy = d.delz_y[c];
+    }
+    p2 = p2 - kG * h_c * gx * d.area[c];
+    p3 = p3 - kG * h_c * gy * d.area[c];
+  }
+  // RK update (solverFVT.f90:259-283)
+  const double u_c = d.u_a[c], v_c = d.v_a[c];
+  double delt;
+  if (d.steady) {
+    const double um = (h_c < d.h_dry) ? kZero : sqrt(u_c * u_c + v_c * v_c);
+    const double wc = dry_c ? kZero : sqrt(kG * h_c);
+    delt = um + wc;
+    if (delt < SMALL_F) delt = 1.044;
+    delt = d.cfl * d.area[c] / (delt * d.perim[c]);
+    if (s == d.K && c == d.last_cell) d.sc->delt_fric = delt;
+  } else {
+    delt = d.sc->delt;
+  }
+  const double dt = delt / d.area[c];
+  double rh = kZero, ru = kZero, rv = kZero;
+  for (int j = 0; j <= s - 1; j++) {
+    const size_t q = (size_t)j * T + c;
+    rh = rh + d.alpha[s][j] * d.rkh[q];
+    ru = ru + d.alpha[s][j] * d.rku[q];
+    rv = rv + d.alpha[s][j] * d.rkv[q];
+  }
+  rh = rh + d.beta[s] * dt * p1;
+  ru = (ru + d.beta[s] * dt * p2);
+  rv = (rv + d.beta[s] * dt * p3);
+  if (d.vclip) {  // :286-296
+    const double heff = fmax2(d.h_dry, rh);
+    const double umag = sqrt(ru * ru + rv * rv) / heff;
+    if (umag > d.vceiling) {
+      ru = d.vceiling * ru / umag;
+      rv = d.vceiling * rv / umag;
+    }
+  }
+  rh = fmax2(rh, kZero);  // :300-325
+  double un, vn;
+  const double h_delta = dry_c ? d.h_wet : d.h_dry;
+  if (rh > h_delta) {
+    un = ru / rh;
+    vn = rv / rh;
+  } else {
+    ru = kZero; rv = kZero; un = kZero; vn = kZero;
+  }
+  const size_t qs = (size_t)s * T + c;
+  d.rkh[qs] = rh;
+  d.rku[qs] = ru;
+  d.rkv[qs] = rv;
+  d.u_a[c] = un;
+  d.v_a[c] = vn;
+  if (s < d.K) {
+    double um;
+    dry_next[c] = dry_flag(rh, un, vn, d.h_dry, d.h_wet, &um);
+  } else {
+    d.phimax[c] = fmax2(fmax2(fmax2(kZero, fabs(p1)), fabs(p2)), fabs(p3));
+  }
+  if (bad) atomicOr(&d.sc->status, 2);
+}
+
+// ---------------------------------------------------------------------------
+// After the RK stages: find_dry_cells, fric_terms_impl, hvalve, rk level copy and the
+// block partials of the iteration's reductions (solverFVT.f90:335-386, 407-445).
+__global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
+  __shared__ double sm[kRedThreads / 32];
+  if (d.sc->converged) return;  // uniform over the grid
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int T = d.T, K = d.K;
+  double st = kZero, sb = kZero, tm = kZero, rm = kZero, dtc = kVlarge;
+  if (c < T) {
+    const size_t qk = (size_t)K * T + c;
+    const double h = d.rkh[qk];
+    double u = d.u_a[c], v = d.v_a[c];
+    double ru = d.rku[qk], rv = d.rkv[qk];
+    const double h0 = d.rkh[c];  // rkh(i,0), the iteration's starting depth
+    double um;
+    const bool dry2 = dry_flag(h, u, v, d.h_dry, d.h_wet, &um);
+    const double cd = d.cd[c];
+    double rough = kZero;
+    switch (d.fric) {
+      case 0:
+        if (!dry2) rough = kG * cd * cd / pow(h, kOneThird);
+        break;
+      case 1:
+        rough = (cd < kFmachp) ? kVlarge : kG / (cd * cd);
+        break;
+      case 2:
+        rough = cd;
+        break;
+      case 3:
+        if (!dry2) {
+          double re = um * h / d.visc;
+          re = fmax2(re, 1000.0);
+          re = fmin2(re, (double)2.5e7f);
+          rough = cd;
+          if (cd / h > 0.20) rough = 0.20 * h;
+          const double ln = log(1.725 / re + pow(rough / (14.8 * h), (double)1.11f));
+          rough = 0.204 / (ln * ln);
+        }
+        break;
+      default:
+        if (!dry2) {
+          rough = pow(100.0 * cd, 0.16666666666666667) / 51.79;
+          rough = kG * rough * rough / pow(h, kOneThird);
+        }
+        break;
+    }
+    const double dtf = d.steady ? d.sc->delt_fric : d.sc->delt;
+    if (!dry2) rough = h / (h + dtf * rough * um);
+    u = u * rough;
+    v = v * rough;
+    if (!dry2) {
+      ru = h * u;
+      rv = h * v;
+    }
+    // numerical valve at stage-boundary edges (solverFVT.f90:357-370)
+    const uint8_t hm = d.hvalve ? d.hvmask[c] : 0;
+    if (hm) {
+      bool zero = false;
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+        if (hm & (1u << j)) {
+          const size_t q = (size_t)j * T + c;
+          const double dot = u * d.fnx[q] + v * d.fny[q];
+          if (dot < 0) zero = true;
+        }
+      if (zero) {
+        u = kZero;
+        v = kZero;
+      }
+    }
+    d.rku[c] = ru;  // rk(:,0) <- rk(:,rkorder) of the next iteration (:138-142)
+    d.rkv[c] = rv;
+    d.rkh[c] = h;
+    d.u_a[c] = u;
+    d.v_a[c] = v;
+    double um1;
+    const bool dry1 = dry_flag(h, u, v, d.h_dry, d.h_wet, &um1);
+    d.dry_a[c] = dry1;
+    st = (h - h0) * (h - h0);
+    sb = h0 * h0;
+    tm = h * d.area[c];
+    rm = dry2 ? kZero : d.phimax[c];
+    const double wc1 = dry1 ? kZero : sqrt(kG * h);
+    dtc = d.cfl * d.area[c] / ((um1 + wc1 + SMALL_F) * d.perim[c]);
+    if (!isfinite(h) || !isfinite(u) || !isfinite(v)) atomicOr(&d.sc->status, 1);
+  }
+  double* pb = d.part + 8 * blockIdx.x;
+  double r0 = block_sum<kRedThreads>(st, sm);
+  if (threadIdx.x == 0) pb[0] = r0;
+  double r1 = block_sum<kRedThreads>(sb, sm);
+  if (threadIdx.x == 0) pb[1] = r1;
+  double r2 = block_sum<kRedThreads>(tm, sm);
+  if (threadIdx.x == 0) pb[2] = r2;
+  double r3 = block_max<kRedThreads>(rm, sm);
+  if (threadIdx.x == 0) pb[3] = r3;
+  double r4 = block_min<kRedThreads>(dtc, sm);
+  if (threadIdx.x == 0) pb[4] = r4;
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_final(Dev d, int nblk) {
+  __shared__ double sm[kRedThreads / 32];
+  if (d.sc->converged) return;
+  double a0 = kZero, a1 = kZero, a2 = kZero, a3 = kZero, a4 = kVlarge;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    const double* pb = d.part + 8 * b;
+    a0 = a0 + pb[0];
+    a1 = a1 + pb[1];
+    a2 = a2 + pb[2];
+    a3 = fmax2(a3, pb[3]);
+    a4 = fmin2(a4, pb[4]);
+  }
+  const double sumtop = block_sum<kRedThreads>(a0, sm);
+  const double sumbot = block_sum<kRedThreads>(a1, sm);
+  const double tmass = block_sum<kRedThreads>(a2, sm);
+  const double rmax_phi = block_max<kRedThreads>(a3, sm);
+  const double dtmin = block_min<kRedThreads>(a4, sm);
+  if (threadIdx.x == 0) {
+    Scalars* sc = d.sc;
+    sc->iter = sc->iter + 1;
+    sc->ttime = sc->ttime + sc->delt;
+    double sbot = sumbot;
+    if (equals(sbot, kZero)) sbot = kOne;
+    sc->rms = sqrt(sumtop / sbot);
+    sc->tmass = tmass;
+    if (d.steady) {
+      sc->rmax = (d.stop_cr == 0) ? rmax_phi : sc->rms;
+      sc->stime = (double)sc->iter;
+      sc->delt = sc->delt_fric;  // carried into the next iteration's ttime
+      if (sc->rmax < d.rstop) sc->converged = 1;
+    } else {
+      sc->stime = sc->stime + sc->delt;
+      sc->rmax = rmax_phi;
+      time_bcs(d, sc->stime);
+      sc->delt = (d.dt_op == 0) ? d.cfl : dtmin;
+    }
+  }
+}
+
+}  // namespace storm

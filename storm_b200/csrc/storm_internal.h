@@ -1,0 +1,81 @@
+// storm_internal.h -- shared declarations of the FVT step library (not part of the ABI).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/storm_fvt.h"
+
+namespace storm {
+
+// ---- error reporting (thread-local last error, storm_fvt_last_error) -------
+int set_error(int code, const std::string& msg);
+void clear_error();
+
+// ---- face kinds of the per-cell face table ---------------------------------
+enum FaceKind : uint8_t {
+  FACE_NONE = 0,   // boundary edge with no flux routine (e.g. between two BC strings)
+  FACE_LEFT = 1,   // interior edge, this cell is edges(k)%e(1)
+  FACE_RIGHT = 2,  // interior edge, this cell is edges(k)%e(2)
+  FACE_WALL = 3,   // walledg1 edge
+  FACE_BC = 4      // open-boundary edge; contribution computed by the boundary kernel
+};
+
+// Open-boundary routine kinds, in the order invisc_fluxes.f90:218-238 calls them.
+enum BcKind : int32_t {
+  BC_QBYH = 0,      // inflowQbyH vtype 1
+  BC_QBYH_WET = 1,  // inflowQbyH vtype 5
+  BC_HIN = 2,       // inflowH vtype 4
+  BC_HOUT = 3,      // outflowbyH htype 1
+  BC_CRIT = 4,      // crit_outflow htype 2
+  BC_FREE = 5       // free_flow htype 0
+};
+
+constexpr int kMaxStencil = 19;   // elemnt_db.f90:42 maxdim = 20 (count + 19 ids)
+constexpr int kMaxBcEdges = 8192; // edges per open boundary handled by one CTA
+
+// Host-side image of the device layout: cells and nodes renumbered along a Morton
+// curve, structure-of-arrays, per-cell face table in local-slot order.
+struct HostLayout {
+  int32_t T = 0, N = 0, kst = 0, nwall = 0, nbce = 0, nbdr = 0, n2t_nnz = 0;
+  std::vector<int32_t> cell_old;  // new -> old (0-based)
+  std::vector<int32_t> node_old;
+  std::vector<int32_t> cell_new;  // old -> new
+  std::vector<int32_t> node_new;
+  // cells [T]
+  std::vector<double> area, perim, xc, yc, z, delz_x, delz_y, zmax, cd;
+  std::vector<double> lsq_a, lsq_b, lsq_c, lsq_det;
+  std::vector<uint8_t> nst, forder, hvmask;
+  // [3][T]
+  std::vector<int32_t> vert, t2t3, fref;
+  std::vector<double> rc_x, rc_y, fnx, fny, flen, fz0;
+  std::vector<uint8_t> fkind;
+  // stencil [kst][T]
+  std::vector<int32_t> st_id;
+  std::vector<double> st_w, st_dx, st_dy;
+  // walls [nwall]
+  std::vector<int32_t> wall_p1, wall_p2;
+  // nodes [N]
+  std::vector<double> zvtx, node_x, node_y;
+  std::vector<int32_t> n2t_off, n2t_cell;  // CSR [N+1], [nnz]
+  std::vector<double> n2t_w;               // c2v_weights_id [nnz]
+  std::vector<int16_t> node_hbc;           // htype-1 boundary (slot in hbc[]) or -1
+  // open boundaries [nbdr], in call order; edges [nbce]
+  std::vector<int32_t> bdr_kind, bdr_slot, bdr_off, bdr_cnt;
+  std::vector<int32_t> bce_cell, bce_slot;
+  std::vector<double> bce_nx, bce_ny, bce_tx, bce_ty, bce_len, bce_zmid;
+  // boundary values and time series (vbc_arrays / dep_vars)
+  int32_t n_in = 0, n_out = 0;
+  std::vector<int32_t> in_type, out_type;
+  std::vector<double> qin, hbc;
+  std::vector<int32_t> ts_off, ts_cnt;  // [n_in + n_out] into ts_t/ts_v (inflows first)
+  std::vector<double> ts_t, ts_v;
+  double bch_max = 0.0;
+  int32_t last_cell_new = 0;  // new id of element n_elems (steady friction dt)
+};
+
+// Build the device layout from the prepared (Fortran-layout) mesh.
+int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& L);
+
+}  // namespace storm

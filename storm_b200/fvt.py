@@ -1,0 +1,194 @@
+"""Python host binding of the FVT step library (ctypes over include/storm_fvt.h).
+
+This mirrors the reference's call sequence at Source_xsy-64bit/solver.f90:50-57:
+``read_data`` + ``dataprepFVT`` (here :func:`build_mesh`, or a prepared
+:class:`~storm_b200.abi.Mesh` supplied by the caller), then ``solverFVT`` (here
+:class:`Solver`: ``set_state`` once, ``step`` as often as output is wanted).  Errors
+are raised as :class:`StormError` carrying the library's status code and message,
+where the reference would call ``byebye`` and stop.
+
+There is no CPU fallback: loading fails loudly if ``libstorm_fvt.so`` was not built
+(``python -m storm_b200.build``) and creating a solver fails without a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libstorm_fvt.so")
+_lib = None
+
+EXPORTS = (
+    "storm_fvt_default_options", "storm_fvt_last_error", "storm_fvt_mesh_build", "storm_fvt_mesh_free",
+    "storm_fvt_create", "storm_fvt_set_state", "storm_fvt_step", "storm_fvt_get_state",
+    "storm_fvt_get_drycell", "storm_fvt_kernel_launches", "storm_fvt_set_kernel_timing",
+    "storm_fvt_last_timing", "storm_fvt_kernel_times", "storm_fvt_destroy",
+)
+
+KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final")
+
+
+class StormError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def lib_path() -> str:
+    return _LIB_PATH
+
+
+def lib():
+    """Load libstorm_fvt.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} is not built; run `python -m storm_b200.build`")
+    L = C.CDLL(_LIB_PATH)
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int32)
+    L.storm_fvt_default_options.argtypes = [C.POINTER(abi.Options)]
+    L.storm_fvt_default_options.restype = None
+    L.storm_fvt_last_error.restype = C.c_char_p
+    L.storm_fvt_mesh_build.argtypes = [C.POINTER(abi.Problem), C.POINTER(C.POINTER(abi.Mesh))]
+    L.storm_fvt_mesh_free.argtypes = [C.POINTER(abi.Mesh)]
+    L.storm_fvt_mesh_free.restype = None
+    L.storm_fvt_create.argtypes = [C.POINTER(abi.Mesh), C.POINTER(abi.Options), C.POINTER(C.c_void_p)]
+    L.storm_fvt_set_state.argtypes = [C.c_void_p, dp, dp, dp]
+    L.storm_fvt_step.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.StepStats)]
+    L.storm_fvt_get_state.argtypes = [C.c_void_p] + [dp] * 7
+    L.storm_fvt_get_drycell.argtypes = [C.c_void_p, ip]
+    L.storm_fvt_kernel_launches.argtypes = [C.c_void_p]
+    L.storm_fvt_kernel_launches.restype = C.c_int64
+    L.storm_fvt_set_kernel_timing.argtypes = [C.c_void_p, C.c_int32]
+    L.storm_fvt_last_timing.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int64)]
+    L.storm_fvt_kernel_times.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64)]
+    L.storm_fvt_destroy.argtypes = [C.c_void_p]
+    _lib = L
+    return L
+
+
+def _chk(rc: int):
+    if rc != 0:
+        raise StormError(rc, lib().storm_fvt_last_error().decode())
+
+
+def default_options(**kw) -> abi.Options:
+    """The library's defaults (initialize_options.f90) with keyword overrides."""
+    o = abi.Options()
+    lib().storm_fvt_default_options(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise AttributeError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+class PreparedMesh:
+    """A prepared mesh built by the library (owns the C allocation)."""
+
+    def __init__(self, problem: abi.ProblemHolder):
+        self.problem = problem  # keep the input arrays alive
+        p = C.POINTER(abi.Mesh)()
+        _chk(lib().storm_fvt_mesh_build(C.byref(problem.problem), C.byref(p)))
+        self._p = p
+
+    @property
+    def mesh(self) -> abi.Mesh:
+        return self._p.contents
+
+    def numpy(self) -> dict:
+        return abi.mesh_to_numpy(self.mesh)
+
+    def close(self):
+        if self._p:
+            lib().storm_fvt_mesh_free(self._p)
+            self._p = C.POINTER(abi.Mesh)()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def build_mesh(problem: abi.ProblemHolder) -> PreparedMesh:
+    return PreparedMesh(problem)
+
+
+class Solver:
+    """One FVT solver on one GPU (``storm_fvt_create``)."""
+
+    def __init__(self, mesh, options: abi.Options, *, keep=None):
+        self._keep = keep  # e.g. the PreparedMesh / oracle owning `mesh`'s arrays
+        m = mesh.mesh if isinstance(mesh, PreparedMesh) else mesh
+        self.T = m.n_elems
+        self.N = m.n_pts
+        self.options = options
+        h = C.c_void_p()
+        _chk(lib().storm_fvt_create(C.byref(m), C.byref(options), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().storm_fvt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_state(self, h, u, v):
+        h, u, v = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, u, v))
+        if not (len(h) == len(u) == len(v) == self.T):
+            raise ValueError("state arrays must have n_elems entries")
+        _chk(lib().storm_fvt_set_state(self._h, abi.dptr(h), abi.dptr(u), abi.dptr(v)))
+
+    def step(self, n: int = 1) -> dict:
+        st = abi.StepStats()
+        _chk(lib().storm_fvt_step(self._h, int(n), C.byref(st)))
+        return st.as_dict()
+
+    def state(self) -> dict:
+        out = {k: np.empty(self.T) for k in ("h", "u", "v", "rkh", "rku", "rkv")}
+        out["hvtx"] = np.empty(self.N)
+        _chk(lib().storm_fvt_get_state(self._h, *(abi.dptr(out[k]) for k in
+                                                 ("h", "u", "v", "rkh", "rku", "rkv", "hvtx"))))
+        return out
+
+    def drycell(self) -> np.ndarray:
+        d = np.empty(self.T, dtype=np.int32)
+        _chk(lib().storm_fvt_get_drycell(self._h, abi.iptr(d)))
+        return d
+
+    def kernel_launches(self) -> int:
+        return int(lib().storm_fvt_kernel_launches(self._h))
+
+    def set_kernel_timing(self, on: bool):
+        _chk(lib().storm_fvt_set_kernel_timing(self._h, int(bool(on))))
+
+    def last_timing(self) -> dict:
+        a, b = C.c_double(), C.c_double()
+        n = C.c_int64()
+        _chk(lib().storm_fvt_last_timing(self._h, C.byref(a), C.byref(b), C.byref(n)))
+        return {"step_ms": a.value, "flux_ms": b.value, "flux_launches": n.value}
+
+    def kernel_times(self) -> dict:
+        """Per-kernel device ms and launch counts of the last step in timing mode."""
+        ms = (C.c_double * 8)()
+        n = (C.c_int64 * 8)()
+        _chk(lib().storm_fvt_kernel_times(self._h, ms, n))
+        return {k: (ms[i], n[i]) for i, k in enumerate(KERNEL_CLASSES)}

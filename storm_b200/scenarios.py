@@ -128,7 +128,7 @@ def _delaunay(x, y):
 def _boundary_string(x, y, tri1, sel):
     """Nodes on the mesh boundary selected by `sel` (bool per node), ordered as a
     chain of boundary edges.  tri1 is 1-based."""
-    t = tri1 - 1
+    t = tri1.astype(np.int64) - 1
     e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
     key = np.minimum(e[:, 0], e[:, 1]) * (len(x) + 1) + np.maximum(e[:, 0], e[:, 1])
     uk, cnt = np.unique(key, return_counts=True)

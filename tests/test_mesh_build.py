@@ -1,0 +1,112 @@
+"""Host-side builder of the prepared mesh vs the oracle's restatement, bit for bit,
+and the C-ABI surface of libstorm_fvt.so (no GPU needed)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from storm_b200 import abi, fvt, scenarios
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bits(a):
+    a = np.asarray(a)
+    return a.view(np.uint64) if a.dtype == np.float64 else a
+
+
+def assert_mesh_equal(mo, mp):
+    assert set(mo) == set(mp)
+    for k in mo:
+        a, b = mo[k], mp[k]
+        if isinstance(a, np.ndarray):
+            assert a.shape == b.shape, k
+            assert np.array_equal(_bits(a), _bits(b)), f"{k} differs"
+        else:
+            assert a == b, (k, a, b)
+
+
+CASES = {
+    "channel": lambda: scenarios.channel(),
+    "meander": lambda: scenarios.meander(n_target=12000, seed=7),
+    "dambreak": lambda: scenarios.dambreak(n_target=12000, seed=8),
+    "channel_cellbed": lambda: _cell_bed_channel(),
+}
+
+
+def _cell_bed_channel():
+    sc = scenarios.channel(nx=40, ny=6)
+    p = sc.problem
+    t = p.tri.reshape(-1, 3) - 1
+    zc = p.zb[t].mean(axis=1)
+    cdv = np.full(p.n_pts, 0.03)
+    prob = abi.ProblemHolder(p.x, p.y, p.tri, zc, cdv, zb_at_vertices=False, cd_at_vertices=True,
+                             inflow=p.inflow_spec, outflow=p.outflow_spec)
+    sc.problem = prob
+    return sc
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_builder_matches_oracle(case, storm_lib, oracle_mod):
+    sc = CASES[case]()
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    pm = fvt.build_mesh(sc.problem)
+    assert_mesh_equal(o.mesh_numpy(), pm.numpy())
+
+
+def test_channel_counts(storm_lib):
+    """The 8,000-cell channel: N=4,221, E=12,220, 440 boundary edges (20 in, 20 out, 400 walls)."""
+    sc = scenarios.channel()
+    m = fvt.build_mesh(sc.problem).numpy()
+    assert (m["n_pts"], m["n_elems"], m["n_edges"]) == (4221, 8000, 12220)
+    assert m["wall_edges1"] == 400 and m["n_bcedges"] == 40
+    assert m["flow_edges1"] == 12220 - 440
+
+
+def test_builder_errors(storm_lib):
+    sc = scenarios.channel(nx=10, ny=4)
+    p = sc.problem
+    bad = abi.ProblemHolder(p.x, p.y, p.tri, p.zb, p.cd,
+                            inflow=[{"type": 1, "nodes": [1, 7], "value": 1.0}],  # not an edge
+                            outflow=p.outflow_spec)
+    with pytest.raises(fvt.StormError) as e:
+        fvt.build_mesh(bad)
+    assert e.value.code == abi.STORM_ERR_MESH
+    tri = p.tri.copy()
+    tri[0] = p.n_pts + 5
+    bad2 = abi.ProblemHolder(p.x, p.y, tri, p.zb, p.cd, inflow=p.inflow_spec, outflow=p.outflow_spec)
+    with pytest.raises(fvt.StormError) as e:
+        fvt.build_mesh(bad2)
+    assert e.value.code == abi.STORM_ERR_MESH
+
+
+def test_library_exports_every_declared_symbol(storm_lib):
+    hdr = open(os.path.join(ROOT, "include", "storm_fvt.h")).read()
+    declared = set(re.findall(r"STORM_FVT_API\s+[\w\s\*]+?\b(storm_fvt_\w+)\s*\(", hdr))
+    assert declared == set(fvt.EXPORTS)
+    lib = C.CDLL(fvt.lib_path())
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_option_checks_run_before_device_use(storm_lib):
+    """Invalid options are rejected on the host (STORM_ERR_ARG / UNSUPPORTED)."""
+    sc = scenarios.channel(nx=10, ny=4)
+    pm = fvt.build_mesh(sc.problem)
+    for kw, code in [({"rkorder": 4}, abi.STORM_ERR_ARG), ({"opt_limiter": 3}, abi.STORM_ERR_ARG),
+                     ({"opt_friction": 5}, abi.STORM_ERR_UNSUPPORTED), ({"flux": 7}, abi.STORM_ERR_ARG),
+                     ({"precision": abi.PREC_MIXED}, abi.STORM_ERR_UNSUPPORTED)]:
+        with pytest.raises(fvt.StormError) as e:
+            fvt.Solver(pm, fvt.default_options(**kw))
+        assert e.value.code == code, kw
+
+
+def test_default_options_match_reference_defaults(storm_lib):
+    lo = fvt.default_options()
+    po = abi.default_options()
+    for name, _ in abi.Options._fields_:
+        if name == "reserved":
+            continue
+        assert getattr(lo, name) == getattr(po, name), name

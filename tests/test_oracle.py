@@ -1,0 +1,143 @@
+"""CPU oracle: pinned against the reference's Tutorial_1 fixture, plus the physical and
+structural properties of solverFVT that hold for any correct restatement."""
+import os
+
+import numpy as np
+import pytest
+
+from storm_b200 import abi, fvt, scenarios
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _tutorial1(with_edges=True):
+    f = np.load(os.path.join(GOLDEN, "tutorial1_topology.npz"))
+    n = int(f["n_pts"])
+    rng = np.random.default_rng(0)  # coordinates are not part of the fixture
+    x, y = rng.uniform(0, 100, n), rng.uniform(0, 100, n)
+    tri = f["tri"]
+    kw = {}
+    if with_edges:
+        kw = dict(edge_p=f["edge_p"], edge_e=f["edge_e"])
+    prob = abi.ProblemHolder(x, y, tri, np.zeros(n), np.full(len(tri), 0.03), **kw)
+    return prob, f
+
+
+def test_tutorial1_topology_known_answers(oracle_mod):
+    """Counts of the reference's Tutorial_1 mesh (triangle -vepq30aD output)."""
+    prob, f = _tutorial1()
+    o = oracle_mod.Oracle(prob, abi.default_options())
+    m = o.mesh_numpy()
+    assert (m["n_pts"], m["n_elems"], m["n_edges"]) == (7081, 13729, 20809)
+    nb = int((f["edge_e"][:, 1] < 0).sum())
+    assert nb == 431 == int((f["marker"] == 1).sum())
+    assert m["wall_edges1"] == 431 and m["flow_edges1"] == 20809 - 431
+    assert m["n_pts"] - m["n_edges"] + m["n_elems"] == 1  # Euler, one boundary loop
+    # .v.edge element pairs survive unchanged (ray swap only touches negative ids)
+    e = m["edge_e"].reshape(-1, 2)
+    assert np.array_equal(e[:, 0], f["edge_e"][:, 0])
+    # every grid%edge entry refers back to an edge of that element
+    ge = m["tri_edge"].reshape(-1, 3)
+    assert (ge != 0).all()
+    k = np.abs(ge) - 1
+    owner = np.arange(1, m["n_elems"] + 1)[:, None]
+    assert ((e[k, 0] == owner) | (e[k, 1] == owner)).all()
+
+
+def test_tutorial1_product_builder_bitwise(oracle_mod, storm_lib):
+    from test_mesh_build import assert_mesh_equal
+    prob, _ = _tutorial1()
+    o = oracle_mod.Oracle(prob, abi.default_options())
+    assert_mesh_equal(o.mesh_numpy(), fvt.build_mesh(prob).numpy())
+
+
+def test_tutorial1_derived_edges_agree_with_triangle_files(oracle_mod):
+    """find_edges without the .edge data rebuilds the same edge set and neighbours."""
+    pe, f = _tutorial1(True)
+    pd, _ = _tutorial1(False)
+    me = oracle_mod.Oracle(pe, abi.default_options()).mesh_numpy()
+    md = oracle_mod.Oracle(pd, abi.default_options()).mesh_numpy()
+    key = lambda p: set(map(tuple, np.sort(p.reshape(-1, 2), axis=1)))  # noqa: E731
+    assert key(me["edge_p"]) == key(md["edge_p"])
+    assert np.array_equal(me["t2t3"], md["t2t3"]) or \
+        np.array_equal(np.sort(me["t2t3"].reshape(-1, 3), 1), np.sort(md["t2t3"].reshape(-1, 3), 1))
+    assert np.array_equal(me["n2t"], md["n2t"])
+
+
+def test_threads_bitwise(oracle_mod):
+    sc = scenarios.meander(n_target=12000, seed=9)
+    outs = []
+    for th in (1, 4):
+        o = oracle_mod.Oracle(sc.problem, sc.options, threads=th)
+        o.set_state(sc.h0, sc.u0, sc.v0)
+        st = o.step(10)
+        outs.append((o.state(), st))
+    for k in ("h", "u", "v", "rku", "rkv", "hvtx"):
+        assert np.array_equal(outs[0][0][k], outs[1][0][k]), k
+    assert outs[0][1] == outs[1][1]
+
+
+def _basin(n=30, flat=True):
+    sc = scenarios.channel(nx=n, ny=n, length=30.0, width=30.0, slope=0.0, noise=0.0 if flat else 0.05,
+                           steady=0, dt_op=1, cfl=0.5, rkorder=3, flux=abi.FLUX_ROE)
+    p = sc.problem
+    prob = abi.ProblemHolder(p.x, p.y, p.tri, p.zb, np.zeros_like(p.cd))  # all walls, no friction
+    sc.problem = prob
+    return sc
+
+
+def test_lake_at_rest_flat_bed(oracle_mod):
+    sc = _basin()
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    o.set_state(np.full(sc.n_elems, 2.0), np.zeros(sc.n_elems), np.zeros(sc.n_elems))
+    o.step(50)
+    s = o.state()
+    assert np.abs(s["u"]).max() < 1e-12 and np.abs(s["v"]).max() < 1e-12
+    assert np.abs(s["h"] - 2.0).max() < 1e-12
+
+
+def test_closed_basin_conserves_mass(oracle_mod):
+    sc = _basin(flat=False)
+    T = sc.n_elems
+    rng = np.random.default_rng(1)
+    h0 = 1.0 + 0.2 * rng.random(T)
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    o.set_state(h0, np.zeros(T), np.zeros(T))
+    m0 = o.mesh_numpy()
+    mass0 = float(np.sum(h0 * m0["tri_area"]))
+    st = o.step(100)
+    assert st["tmass"] == pytest.approx(mass0, rel=1e-12)
+
+
+def test_channel_reaches_steady_state(oracle_mod):
+    """A short channel converges and passes the inflow discharge to the outlet.  (With
+    the Barth-Jespersen limiter the RMS relative dh stalls near 3e-6 on this mesh, a
+    limiter cycle of the reference scheme, so the threshold is 1e-5.)"""
+    sc = scenarios.channel(nx=40, ny=4, length=20.0, width=2.0, q=1.0, rstop=1e-5, stop_cr=1)
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    o.set_state(sc.h0, sc.u0, sc.v0)
+    st = o.step(20000)
+    assert st["converged"], st
+    assert abs(st["cqin3"][0]) == pytest.approx(1.0, rel=2e-3)
+    assert st["cqout3"][0] == pytest.approx(1.0, rel=2e-2)
+
+
+def test_hll_is_consistent(oracle_mod):
+    """HLL as fixed (flux(3) set, the whole numerator divided by sright-sleft) keeps a
+    uniform flow uniform: after one RK3 step only cells near the walls have moved.
+    With the reference's literal formula F(q,q) = (sright-sleft)*F(q) and the uniform
+    state would not be an equilibrium."""
+    sc = _basin()
+    sc.options.flux = abi.FLUX_HLL
+    T = sc.n_elems
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    o.set_state(np.full(T, 1.0), np.full(T, 0.3), np.full(T, -0.2))
+    m = o.mesh_numpy()
+    o.step(1)
+    s = o.state()
+    xc, yc = m["tri_xc"], m["tri_yc"]
+    cells = np.where((xc > 9) & (xc < 21) & (yc > 9) & (yc < 21))[0]
+    assert len(cells) > T // 10
+    assert np.abs(s["h"][cells] - 1.0).max() < 1e-12
+    assert np.abs(s["u"][cells] - 0.3).max() < 1e-12
+    assert np.abs(s["v"][cells] + 0.2).max() < 1e-12
