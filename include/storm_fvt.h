@@ -289,6 +289,25 @@ STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, i
 
 STORM_FVT_API int storm_fvt_destroy(StormFvtHandle* hd);
 
+/*
+ * CFL time step without any device allocation.  No counterpart in the reference:
+ * it exists for callers that cannot call cudaMalloc -- a host whose device memory
+ * is owned by an external pool, code running while a CUDA graph is captured, or a
+ * loop that cannot take the synchronisation an allocation may bring.  It computes,
+ * from device arrays in any cell order, the value storm_fvt_step reports as the next
+ * dt for dt_op = 1:  *d_dt = MIN over cells of cfl*area/((|u|+c+small)*perim) with
+ * |u| and c = sqrt(g h) of the find_dry_cells classification (deltatFVT.f90:32-38,
+ * with the cell area and perimeter).  Its scratch is a 32 KiB static device array,
+ * so at most 1,048,576 cells per call (larger n: STORM_ERR_ARG, nothing launched).
+ * Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).  The
+ * first call on a device resolves the array's address (make it before any stream
+ * capture); calls share the array, so calls that overlap on the GPU race.
+ */
+STORM_FVT_API int storm_fvt_cfl_dt_noalloc(const double* d_h, const double* d_u, const double* d_v,
+                                           const double* d_area, const double* d_perim, int32_t n,
+                                           double cfl, double h_dry, double h_wet, double* d_dt,
+                                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ EXPORTS = (
     "storm_fvt_create", "storm_fvt_set_state", "storm_fvt_step", "storm_fvt_get_state",
     "storm_fvt_get_drycell", "storm_fvt_kernel_launches", "storm_fvt_set_kernel_timing",
     "storm_fvt_last_timing", "storm_fvt_kernel_times", "storm_fvt_destroy",
+    "storm_fvt_cfl_dt_noalloc",
 )
 
 KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final")
@@ -69,6 +70,8 @@ def lib():
     L.storm_fvt_last_timing.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int64)]
     L.storm_fvt_kernel_times.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64)]
     L.storm_fvt_destroy.argtypes = [C.c_void_p]
+    L.storm_fvt_cfl_dt_noalloc.argtypes = [C.c_void_p] * 5 + [C.c_int32, C.c_double, C.c_double, C.c_double,
+                                                                C.c_void_p, C.c_void_p]
     _lib = L
     return L
 
