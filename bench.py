@@ -267,7 +267,7 @@ def main():
     solver.step(kt_steps)
     kt = solver.kernel_times()
     solver.set_kernel_timing(False)
-    stage_ms = sum(kt[k][0] for k in ("node", "grad", "bc", "flux"))
+    stage_ms = sum(kt[k][0] for k in ("node", "grad", "bc", "eflux", "flux"))
     B = scenarios.algorithmic_bytes_per_cell_stage(T, E, N)
     pk = peaks()
     achieved = B * T * K_rk * kt_steps / (stage_ms / 1e3) / 1e9
@@ -275,7 +275,7 @@ def main():
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
         "frac": achieved / pk["hbm_gbs"], "traffic": None,
-        "kernel": "one RK stage: k_node + k_grad + k_bc + k_flux",
+        "kernel": "one RK stage: k_node + k_grad + k_bc + k_eflux + k_flux",
         "bytes_per_cell_stage": B, "peak_source": pk["source"],
         "kernel_ms_share": {k: round(v[0] / iter_ms, 4) for k, v in kt.items()},
         "flux_kernel_avg_ms": kt["flux"][0] / max(1, kt["flux"][1]),

@@ -283,8 +283,9 @@ STORM_FVT_API int storm_fvt_last_timing(const StormFvtHandle* hd, double* step_m
 
 /* Per-kernel device time (ms) and launch counts of the last storm_fvt_step call in
  * kernel timing mode, indexed 0 node (vertex depth), 1 grad (gradients/limiter),
- * 2 bc (open boundaries), 3 flux (fluxes + sources + RK update), 4 fric (friction
- * and reduction partials), 5 final (iteration scalars); 6-7 are zero. */
+ * 2 bc (open boundaries), 3 flux (per-cell gather of the face fluxes + sources + RK
+ * update), 4 fric (friction and reduction partials), 5 final (iteration scalars),
+ * 6 eflux (interior-edge fluxes); 7 is zero. */
 STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, int64_t* launches);
 
 STORM_FVT_API int storm_fvt_destroy(StormFvtHandle* hd);

@@ -25,6 +25,8 @@ __global__ void k_node(Dev d, const double* hs, const uint8_t* dry);
 __global__ void k_grad(Dev d, const double* hs, const uint8_t* dry, double* rku_prev, double* rkv_prev);
 __global__ void k_bc(Dev d, const double* hs, const uint8_t* dry);
 __global__ void k_flux(Dev d, int s, const double* hs, const uint8_t* dry, uint8_t* dry_next);
+__global__ void k_flux_bc(Dev d, int s, const double* hs, const uint8_t* dry, uint8_t* dry_next);
+__global__ void k_eflux(Dev d, const double* hs, const uint8_t* dry);
 __global__ void k_fric(Dev d);
 __global__ void k_final(Dev d, int nblk);
 
@@ -45,6 +47,8 @@ struct StormFvtHandle {
   HostLayout L;
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;       // boundary kernel, overlapped with k_flux
+  cudaEvent_t fork_ev[4] = {}, join_ev[4] = {};
   void* arena = nullptr;
   Dev d{};
   Scalars* sc_host = nullptr;  // pinned
@@ -112,7 +116,7 @@ T* at(void* base, size_t off) {
 }
 
 // Kernel classes of the per-kernel timing mode.
-enum { KT_NODE = 0, KT_GRAD, KT_BC, KT_FLUX, KT_FRIC, KT_FINAL, KT_COUNT };
+enum { KT_NODE = 0, KT_GRAD, KT_BC, KT_FLUX, KT_FRIC, KT_FINAL, KT_EFLUX, KT_COUNT };
 
 int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
   const Dev& d = h->d;
@@ -120,6 +124,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
   const int gT = (T + kCellThreads - 1) / kCellThreads;
   const int gF = (T + kFluxThreads - 1) / kFluxThreads;
   const int gN = (N + kNodeThreads - 1) / kNodeThreads;
+  const int gE = (d.ne + kFluxThreads - 1) / kFluxThreads;
   // in timing mode every launch is bracketed by an event pair tagged with its class
   auto mark = [&](int cls) -> int {
     if (!timing) return 0;
@@ -142,14 +147,35 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     if (done() || mark(KT_GRAD)) return STORM_ERR_CUDA;
     k_grad<<<gT, kCellThreads, 0, h->stream>>>(d, hs, dry, d.rku + (size_t)(s - 1) * T, d.rkv + (size_t)(s - 1) * T);
     if (done()) return STORM_ERR_CUDA;
-    if (d.nbdr > 0) {
-      if (mark(KT_BC)) return STORM_ERR_CUDA;
-      k_bc<<<d.nbdr, 128, h->bc_smem, h->stream>>>(d, hs, dry);
+    if (d.nbdr > 0 && !timing) {
+      // k_bc on the side stream overlaps k_eflux and k_flux of the cells without
+      // boundary faces; the boundary cells are finished once both are done
+      CK(cudaEventRecord(h->fork_ev[s], h->stream));
+      CK(cudaStreamWaitEvent(h->side, h->fork_ev[s], 0));
+      k_bc<<<d.nbdr, 128, h->bc_smem, h->side>>>(d, hs, dry);
+      CK(cudaEventRecord(h->join_ev[s], h->side));
+      if (gE > 0) k_eflux<<<gE, kFluxThreads, 0, h->stream>>>(d, hs, dry);
+      k_flux<<<gF, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
+      CK(cudaStreamWaitEvent(h->stream, h->join_ev[s], 0));
+      const int gB = (d.nbc_cells + kFluxThreads - 1) / kFluxThreads;
+      if (gB > 0) k_flux_bc<<<gB, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
+    } else {
+      if (d.nbdr > 0) {
+        if (mark(KT_BC)) return STORM_ERR_CUDA;
+        k_bc<<<d.nbdr, 128, h->bc_smem, h->stream>>>(d, hs, dry);
+        if (done()) return STORM_ERR_CUDA;
+      }
+      if (gE > 0) {
+        if (mark(KT_EFLUX)) return STORM_ERR_CUDA;
+        k_eflux<<<gE, kFluxThreads, 0, h->stream>>>(d, hs, dry);
+        if (done()) return STORM_ERR_CUDA;
+      }
+      if (mark(KT_FLUX)) return STORM_ERR_CUDA;
+      k_flux<<<gF, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
+      const int gB = (d.nbc_cells + kFluxThreads - 1) / kFluxThreads;
+      if (gB > 0) k_flux_bc<<<gB, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
       if (done()) return STORM_ERR_CUDA;
     }
-    if (mark(KT_FLUX)) return STORM_ERR_CUDA;
-    k_flux<<<gF, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
-    if (done()) return STORM_ERR_CUDA;
   }
   if (mark(KT_FRIC)) return STORM_ERR_CUDA;
   k_fric<<<d.nblk_red, kRed, 0, h->stream>>>(d);
@@ -187,6 +213,11 @@ void release(StormFvtHandle* h) {
   for (cudaEvent_t e : h->fev) cudaEventDestroy(e);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  for (int i = 0; i < 4; i++) {
+    if (h->fork_ev[i]) cudaEventDestroy(h->fork_ev[i]);
+    if (h->join_ev[i]) cudaEventDestroy(h->join_ev[i]);
+  }
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->arena) cudaFree(h->arena);
   if (h->sc_host) cudaFreeHost(h->sc_host);
@@ -233,6 +264,10 @@ int upload(StormFvtHandle* h) {
   size_t o_bty = cpy(L.bce_ty, nbce), o_bl = cpy(L.bce_len, nbce), o_bz = cpy(L.bce_zmid, nbce);
   size_t o_tso = cpy(L.ts_off, nio), o_tsc = cpy(L.ts_cnt, nio), o_ot = cpy(L.out_type, nio);
   size_t o_tst = cpy(L.ts_t, nts), o_tsv = cpy(L.ts_v, nts);
+  size_t o_bcl = cpy(L.bc_cells, std::max<size_t>(L.bc_cells.size(), 1));
+  const size_t ne1 = std::max(L.ne, 1);
+  size_t o_eL = cpy(L.eL, ne1), o_eR = cpy(L.eR, ne1), o_es = cpy(L.eslot, ne1);
+  size_t o_enx = cpy(L.enx, ne1), o_eny = cpy(L.eny, ne1), o_el = cpy(L.elen, ne1), o_ez0 = cpy(L.ez0, ne1);
   // state
   const size_t TL = (size_t)(K + 1) * T;
   size_t o_rkh = A.take(8 * TL), o_rku = A.take(8 * TL), o_rkv = A.take(8 * TL);
@@ -243,6 +278,7 @@ int upload(StormFvtHandle* h) {
   size_t o_dra = A.take(T), o_drb = A.take(T), o_hv = A.take(8 * (size_t)N), o_vw = A.take(N);
   size_t o_pm = A.take(8 * (size_t)T), o_bcc3 = A.take(8 * 3 * nbce), o_rec = A.take(8 * 3 * nbce);
   size_t o_part = A.take(8 * 8 * (size_t)nblk), o_sc = A.take(sizeof(Scalars));
+  size_t o_efx = A.take(8 * 3 * ne1), o_eok = A.take(ne1);
   cudaError_t e = cudaMalloc(&h->arena, A.off);
   if (e != cudaSuccess)
     return set_error(e == cudaErrorMemoryAllocation ? STORM_ERR_NOMEM : STORM_ERR_CUDA,
@@ -299,6 +335,12 @@ int upload(StormFvtHandle* h) {
   d.vwet = at<uint8_t>(B, o_vw); d.phimax = at<double>(B, o_pm); d.bc_c = at<double>(B, o_bcc3);
   d.bc_rec = at<double>(B, o_rec); d.part = at<double>(B, o_part); d.nblk_red = nblk;
   d.sc = at<Scalars>(B, o_sc);
+  d.nbc_cells = (int32_t)L.bc_cells.size();
+  d.ne = L.ne;
+  d.eL = at<int32_t>(B, o_eL); d.eR = at<int32_t>(B, o_eR); d.eslot = at<uint8_t>(B, o_es);
+  d.enx = at<double>(B, o_enx); d.eny = at<double>(B, o_eny); d.elen = at<double>(B, o_el);
+  d.ez0 = at<double>(B, o_ez0); d.efx = at<double>(B, o_efx); d.eok = at<uint8_t>(B, o_eok);
+  d.bc_cells = at<int32_t>(B, o_bcl);
   // boundary values
   Scalars s0{};
   for (int b = 0; b < L.n_in; b++) s0.qin[b] = L.qin[b];
@@ -377,6 +419,11 @@ int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, Storm
   }
   e = cudaSetDevice(h->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+  for (int i = 0; i < 4 && e == cudaSuccess; i++) {
+    e = cudaEventCreateWithFlags(&h->fork_ev[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming);
+  }
   if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
   if (e == cudaSuccess) e = cudaMallocHost(&h->sc_host, sizeof(Scalars));

@@ -41,6 +41,13 @@ struct Dev {
   const int32_t *vert, *t2t3, *fref, *st_id;
   const double *rc_x, *rc_y, *fnx, *fny, *flen, *fz0, *st_w, *st_dx, *st_dy;
   const int32_t *wall_p1, *wall_p2;
+  // interior edges
+  int32_t ne;
+  const int32_t *eL, *eR;
+  const uint8_t* eslot;
+  const double *enx, *eny, *elen, *ez0;
+  double* efx;              // [3][ne] flux * length of the last k_eflux
+  uint8_t* eok;             // [ne] the edge produced a flux (not skipped)
   // nodes
   const double *zvtx, *node_x, *node_y, *n2t_w;
   const int32_t *n2t_off, *n2t_cell;
@@ -62,6 +69,8 @@ struct Dev {
   double* bc_c;             // [3][nbce] boundary contributions to phi
   double* bc_rec;           // [3][nbce] reconstructed boundary-edge h, u, v
   double* part;             // [nblk][8] reduction partials
+  int32_t nbc_cells;        // cells with an open-boundary face (finished after k_bc)
+  const int32_t* bc_cells;
   int32_t nblk_red;
   Scalars* sc;
 };

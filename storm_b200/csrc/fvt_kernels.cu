@@ -380,7 +380,36 @@ __global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ 
   if (d.lim == 1 || d.lim == 2) {
     double dz = kZero, ez = kZero, du = kZero, eu = kZero, dv = kZero, ev = kZero;
     const int n = d.nst[c];
-    for (int k = 0; k < n; k++) {
+    int k0 = 0;
+    if (n >= 3) {  // interior cells: the three face neighbours, all gathers issued together
+      int jj[3];
+      double w[3], dx[3], dy[3], pz[3], pu[3], pv[3];
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const size_t q = (size_t)k * T + c;
+        jj[k] = d.st_id[q];
+        w[k] = d.st_w[q];
+        dx[k] = d.st_dx[q];
+        dy[k] = d.st_dy[q];
+      }
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        pz[k] = (hs[jj[k]] + d.z[jj[k]]) - zeta_c;
+        pu[k] = d.u_a[jj[k]] - u_c;
+        pv[k] = d.v_a[jj[k]] - v_c;
+      }
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        dz = dz + w[k] * pz[k] * dx[k];
+        ez = ez + w[k] * pz[k] * dy[k];
+        du = du + w[k] * pu[k] * dx[k];
+        eu = eu + w[k] * pu[k] * dy[k];
+        dv = dv + w[k] * pv[k] * dx[k];
+        ev = ev + w[k] * pv[k] * dy[k];
+      }
+      k0 = 3;
+    }
+    for (int k = k0; k < n; k++) {
       const size_t q = (size_t)k * T + c;
       const int j = d.st_id[q];
       const double w = d.st_w[q], dx = d.st_dx[q], dy = d.st_dy[q];
@@ -431,8 +460,13 @@ __global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ 
         const double delq = qj - q0;
         double rj;
         if (equals(delq, kZero)) rj = kOne;
-        else if (delq < 0) rj = (qmin - q0) / delq;
-        else rj = (qmax - q0) / delq;
+        else {
+          // r = (qmin-q0)/delq for delq < 0, (qmax-q0)/delq otherwise; both are >= 0.
+          // When |num| > |delq| the exact quotient exceeds one, so the rounded one is
+          // >= 1 and the limiter's min(r,1) is 1: the division is skipped, same bits.
+          const double num = (delq < 0) ? (qmin - q0) : (qmax - q0);
+          rj = (fabs(num) > fabs(delq)) ? kOne : num / delq;
+        }
         const double a = fmin2(kOne * rj, kOne);
         const double b = fmin2(rj, kOne);
         r[j] = fmax2(a, b);
@@ -809,11 +843,34 @@ __device__ __forceinline__ bool interior_flux(const Dev& d, const double* __rest
   return true;
 }
 
-// Fluxes, sources and the RK update of stage s (1-based) for one cell.
-__global__ void __launch_bounds__(128) k_flux(Dev d, int s, const double* __restrict__ hs,
-                                              const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.T || d.sc->converged) return;
+// Interior-edge fluxes of one stage (invisc_fluxes.f90:39-147), one thread per edge:
+// the flux of edge k is evaluated once, in the reference's orientation (left =
+// edges(k)%e(1)), and stored as f*length, the amount the reference subtracts from
+// phi(e(1),:) and adds to phi(e(2),:).
+__global__ void __launch_bounds__(128) k_eflux(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.ne || d.sc->converged) return;
+  const int L = d.eL[e], R = d.eR[e];
+  const uint8_t sl = d.eslot[e];
+  double f[3];
+  bool bad = false;
+  const bool ok = interior_flux(d, hs, dry, L, sl & 3, R, (sl >> 2) & 3, d.enx[e], d.eny[e],
+                                (dry[L] || dry[R]) ? d.ez0[e] : kZero, f, &bad);
+  d.eok[e] = ok;
+  if (ok) {
+    const double len = d.elen[e];
+    d.efx[e] = f[0] * len;
+    d.efx[d.ne + e] = f[1] * len;
+    d.efx[2 * d.ne + e] = f[2] * len;
+  }
+  if (bad) atomicOr(&d.sc->status, 2);
+}
+
+// Fluxes, sources and the RK update of stage s (1-based) for cell c: the faces are
+// added to phi in the order invisc_fluxes.f90 visits them (phi = zero first,
+// solverFVT.f90:194), then the bed slope, then the RK update.
+__device__ __forceinline__ void flux_cell(const Dev& d, int s, int c, const double* __restrict__ hs,
+                                          const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
   const int T = d.T;
   const bool dry_c = dry[c];
   const double h_c = hs[c];
@@ -827,20 +884,17 @@ __global__ void __launch_bounds__(128) k_flux(Dev d, int s, const double* __rest
     const uint8_t fk = d.fkind[q];
     const int kind = fk & 7;
     if (kind == FACE_LEFT || kind == FACE_RIGHT) {
-      const int nb = d.fref[q], ns = fk >> 4;
-      double f[3];
-      const bool left = kind == FACE_LEFT;
-      if (interior_flux(d, hs, dry, left ? c : nb, left ? j : ns, left ? nb : c, left ? ns : j, d.fnx[q], d.fny[q],
-                        d.fz0[q], f, &bad)) {
-        const double len = d.flen[q];
-        if (left) {
-          p1 = p1 - f[0] * len;
-          p2 = p2 - f[1] * len;
-          p3 = p3 - f[2] * len;
+      const int e = d.fref[q];  // flux*length of the edge, evaluated once by k_eflux
+      if (d.eok[e]) {
+        const double f0 = d.efx[e], f1 = d.efx[d.ne + e], f2 = d.efx[2 * d.ne + e];
+        if (kind == FACE_LEFT) {
+          p1 = p1 - f0;
+          p2 = p2 - f1;
+          p3 = p3 - f2;
         } else {
-          p1 = p1 + f[0] * len;
-          p2 = p2 + f[1] * len;
-          p3 = p3 + f[2] * len;
+          p1 = p1 + f0;
+          p2 = p2 + f1;
+          p3 = p3 + f2;
         }
       }
     } else if (kind == FACE_WALL) {
@@ -967,6 +1021,23 @@ __global__ void __launch_bounds__(128) k_flux(Dev d, int s, const double* __rest
     d.phimax[c] = fmax2(fmax2(fmax2(kZero, fabs(p1)), fabs(p2)), fabs(p3));
   }
   if (bad) atomicOr(&d.sc->status, 2);
+}
+
+// All cells without an open-boundary face (those wait for k_bc in k_flux_bc).
+__global__ void __launch_bounds__(128) k_flux(Dev d, int s, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.T || d.sc->converged) return;
+  if (d.forder[c] & kOrderHasBc) return;
+  flux_cell(d, s, c, hs, dry, dry_next);
+}
+
+// The cells with an open-boundary face, after k_bc.
+__global__ void __launch_bounds__(128) k_flux_bc(Dev d, int s, const double* __restrict__ hs,
+                                                 const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.nbc_cells || d.sc->converged) return;
+  flux_cell(d, s, d.bc_cells[i], hs, dry, dry_next);
 }
 
 // ---------------------------------------------------------------------------

@@ -250,12 +250,36 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
     L.wall_p1.push_back(NN(EP(k, 1)));
     L.wall_p2.push_back(NN(EP(k, 2)));
   }
-  // bc visiting-order keys: (routine rank, boundary, position) -> a single rank
+  // ---- interior edges (one flux evaluation each) ----------------------------
+  std::vector<int32_t> ie_of((size_t)E + 1, -1);
   {
-    int32_t r = 0;
-    for (int32_t b = 0; b < L.nbdr; b++)
-      for (int32_t l = 0; l < L.bdr_cnt[b]; l++) r++;
-    (void)r;
+    std::vector<int32_t> ks(m.flowedg1, m.flowedg1 + m.flow_edges1);
+    auto key = [&](int32_t k) {
+      int32_t a = CN(EE(k, 1)), b = CN(EE(k, 2));
+      return ((int64_t)std::min(a, b) << 32) | (uint32_t)std::max(a, b);
+    };
+    std::stable_sort(ks.begin(), ks.end(), [&](int32_t x, int32_t y) { return key(x) < key(y); });
+    L.ne = (int32_t)ks.size();
+    L.eL.resize(L.ne); L.eR.resize(L.ne); L.eslot.resize(L.ne);
+    L.enx.resize(L.ne); L.eny.resize(L.ne); L.elen.resize(L.ne); L.ez0.resize(L.ne);
+    for (int32_t e = 0; e < L.ne; e++) {
+      const int32_t k = ks[e], e1 = EE(k, 1), e2 = EE(k, 2);
+      const int m1 = local_edge(e1, k), m2 = local_edge(e2, k);
+      if (m1 < 1 || m2 < 1) return set_error(STORM_ERR_MESH, "storm_fvt_create: edge not in its element");
+      double nx = m.edge_normal[2 * (size_t)(k - 1)], ny = m.edge_normal[2 * (size_t)(k - 1) + 1];
+      if (GE(e1, m1) < 0) {  // invert_edge_dirs: the normal points out of e(1)
+        nx = -nx;
+        ny = -ny;
+      }
+      ie_of[k] = e;
+      L.eL[e] = CN(e1);
+      L.eR[e] = CN(e2);
+      L.eslot[e] = (uint8_t)((m1 - 1) | ((m2 - 1) << 2));
+      L.enx[e] = nx;
+      L.eny[e] = ny;
+      L.elen[e] = m.edge_length[k - 1];
+      L.ez0[e] = kHalf * (m.zvtx[EP(k, 1) - 1] + m.zvtx[EP(k, 2) - 1]);
+    }
   }
 
   // ---- cells ---------------------------------------------------------------
@@ -339,7 +363,7 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
         int mo = local_edge(other, k);
         if (mo < 1) return set_error(STORM_ERR_MESH, "storm_fvt_create: edge not in its element");
         L.fkind[q] = (uint8_t)((e1 == i1 ? FACE_LEFT : FACE_RIGHT) | ((mo - 1) << 4));
-        L.fref[q] = CN(other);
+        L.fref[q] = ie_of[k];  // the interior-edge record holding this face's flux
         L.fz0[q] = kHalf * (m.zvtx[EP(k, 1) - 1] + m.zvtx[EP(k, 2) - 1]);
         key[j - 1] = (int64_t)k;
       } else {
@@ -370,6 +394,9 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
     int ord[3] = {0, 1, 2};
     std::sort(ord, ord + 3, [&](int a, int b) { return key[a] < key[b]; });
     L.forder[c] = (uint8_t)(ord[0] | (ord[1] << 2) | (ord[2] << 4));
+    for (int j = 0; j < 3; j++)
+      if (L.fkind[(size_t)j * T + c] == FACE_BC) L.forder[c] |= kOrderHasBc;
+    if (L.forder[c] & kOrderHasBc) L.bc_cells.push_back(c);
   }
   // numerical valve targets (solverFVT.f90:357-370)
   for (int32_t j = 0; j < m.n_bcedges; j++) {

@@ -32,6 +32,7 @@ enum BcKind : int32_t {
   BC_FREE = 5       // free_flow htype 0
 };
 
+constexpr uint8_t kOrderHasBc = 0x40;  // forder flag: the cell has an open-boundary face
 constexpr int kMaxStencil = 19;   // elemnt_db.f90:42 maxdim = 20 (count + 19 ids)
 constexpr int kMaxBcEdges = 8192; // edges per open boundary handled by one CTA
 
@@ -47,6 +48,7 @@ struct HostLayout {
   std::vector<double> area, perim, xc, yc, z, delz_x, delz_y, zmax, cd;
   std::vector<double> lsq_a, lsq_b, lsq_c, lsq_det;
   std::vector<uint8_t> nst, forder, hvmask;
+  std::vector<int32_t> bc_cells;  // cells with an open-boundary face, increasing
   // [3][T]
   std::vector<int32_t> vert, t2t3, fref;
   std::vector<double> rc_x, rc_y, fnx, fny, flen, fz0;
@@ -54,6 +56,11 @@ struct HostLayout {
   // stencil [kst][T]
   std::vector<int32_t> st_id;
   std::vector<double> st_w, st_dx, st_dy;
+  // interior edges [ne], ordered by (min, max) of their two cells' new ids
+  int32_t ne = 0;
+  std::vector<int32_t> eL, eR;       // edges(k)%e(1), e(2)
+  std::vector<uint8_t> eslot;        // local slot of the edge in L | (in R) << 2
+  std::vector<double> enx, eny, elen, ez0;  // normal out of e(1), length, midpoint bed
   // walls [nwall]
   std::vector<int32_t> wall_p1, wall_p2;
   // nodes [N]

@@ -30,7 +30,7 @@ EXPORTS = (
     "storm_fvt_cfl_dt_noalloc",
 )
 
-KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final")
+KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux")
 
 
 class StormError(RuntimeError):
