@@ -162,6 +162,9 @@ def main():
     ap.add_argument("--cells", type=int, default=2_000_000)
     ap.add_argument("--cpu-steps", type=int, default=3, help="oracle iterations timed for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="arithmetic of the headline run")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the secondary mixed-precision run")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0, help="CPU seconds of the reference arm")
     ap.add_argument("--e2e-steps", type=int, default=200, help="iterations of the end-to-end pass")
     ap.add_argument("--kt-steps", type=int, default=5, help="iterations of the per-kernel timing pass")
@@ -215,6 +218,8 @@ def main():
     build.build()
     sc = build_workload(args)
     sc.options.device = local
+    if args.precision == "mixed":
+        sc.options.precision = 1
     pm, T, E, N = mesh_ratios(sc)
     K_rk = sc.options.rkorder
     solver = fvt.Solver(pm, sc.options, keep=pm)
@@ -235,6 +240,7 @@ def main():
         barrier()
     ms = solver.last_timing()["step_ms"]
     gpu_launches = solver.kernel_launches() - launches0
+    ref_state = solver.state() if not args.no_mixed else None
     ms_max = ms
     if dist is not None:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -260,6 +266,38 @@ def main():
     h2d = 3 * 8 * T / e2e_steps
     d2h = 224 + (6 * 8 * T + 8 * N) / e2e_steps  # StepStats per call + the final state
 
+    # ---- secondary run in the other precision: speed and error vs this run ----
+    other = None
+    if not args.no_mixed:
+        import ctypes
+        from storm_b200 import abi
+        o2 = abi.Options.from_buffer_copy(sc.options)
+        o2.precision = 0 if args.precision == "mixed" else 1
+        s2 = fvt.Solver(pm, o2, keep=pm)
+        s2.set_state(sc.h0, sc.u0, sc.v0)
+        s2.step(args.warmup)
+        barrier()
+        st2 = s2.step(args.steps)
+        barrier()
+        ms2 = s2.last_timing()["step_ms"]
+        b_state = s2.state()
+        a_state = ref_state
+        if args.precision == "mixed":
+            a_state, b_state = b_state, a_state
+        hu_a, hv_a = a_state["h"] * a_state["u"], a_state["h"] * a_state["v"]
+        hu_b, hv_b = b_state["h"] * b_state["u"], b_state["h"] * b_state["v"]
+        qs = max(float(np.abs(hu_a).max()), float(np.abs(hv_a).max()), 1e-12)
+        other = {
+            "precision": "mixed" if args.precision == "fp64" else "fp64",
+            "value": T * K_rk * args.steps / (ms2 / 1e3), "ms_per_step": ms2 / args.steps,
+            "error_vs_fp64_after_steps": args.warmup + args.steps,
+            "depth_max_abs_m": float(np.abs(a_state["h"] - b_state["h"]).max()),
+            "depth_rms_m": float(np.sqrt(np.mean((a_state["h"] - b_state["h"]) ** 2))),
+            "momentum_max_rel": float(max(np.abs(hu_a - hu_b).max(), np.abs(hv_a - hv_b).max()) / qs),
+            "mass_rel": abs(st2["tmass"] - stats["tmass"]) / stats["tmass"],
+        }
+        s2.close()
+
     # ---- per-kernel timing pass (roofline of the RK-stage kernel chain) ----
     solver.set_state(sc.h0, sc.u0, sc.v0)
     solver.set_kernel_timing(True)
@@ -284,10 +322,10 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
         "data": "synthetic (seeded generator; no public dataset exists for this path)",
         "config": {"workload": f"{args.config}-{T}", "cells": T, "edges": E, "nodes": N, "rkorder": K_rk,
-                   "flux": int(sc.options.flux), "precision": "fp64", "parallelism": f"replicas x{world}",
+                   "flux": int(sc.options.flux), "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": "working set > L2 (inputs larger than the 126 MB L2)",
                    "dry_fraction": sc.info.get("dry_fraction")},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -297,6 +335,8 @@ def main():
         "clocks": clk.summary(),
         "final": {"iter": stats["iter"], "tmass": stats["tmass"], "status": stats["device_status"]},
     }
+    if other is not None:
+        out["other_precision"] = other
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cv, secs = run_cpu(sc, args.cpu_steps, threads)

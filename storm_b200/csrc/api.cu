@@ -22,11 +22,6 @@ namespace storm {
 __global__ void k_init(Dev d);
 __global__ void k_init_final(Dev d, int nblk);
 __global__ void k_node(Dev d, const double* hs, const uint8_t* dry);
-__global__ void k_grad(Dev d, const double* hs, const uint8_t* dry, double* rku_prev, double* rkv_prev);
-__global__ void k_bc(Dev d, const double* hs, const uint8_t* dry);
-__global__ void k_flux(Dev d, int s, const double* hs, const uint8_t* dry, uint8_t* dry_next);
-__global__ void k_flux_bc(Dev d, int s, const double* hs, const uint8_t* dry, uint8_t* dry_next);
-__global__ void k_eflux(Dev d, const double* hs, const uint8_t* dry);
 __global__ void k_fric(Dev d);
 __global__ void k_final(Dev d, int nblk);
 
@@ -50,7 +45,11 @@ struct StormFvtHandle {
   cudaStream_t side = nullptr;       // boundary kernel, overlapped with k_flux
   cudaEvent_t fork_ev[4] = {}, join_ev[4] = {};
   void* arena = nullptr;
+  void* arena32 = nullptr;  // FP32 geometry copies (mixed precision only)
   Dev d{};
+  Geo<double> gd{};  // FP64 views
+  Geo<float> gf{};   // FP32 copies (mixed precision)
+  bool mixed = false;
   Scalars* sc_host = nullptr;  // pinned
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -90,8 +89,8 @@ int check_options(const StormFvtOptions& o) {
     return set_error(STORM_ERR_UNSUPPORTED, "opt_friction must be 0..4 (5, the vegetation model, is not built)");
   if (o.flux < 0 || o.flux > 2) return set_error(STORM_ERR_ARG, "flux must be ROE, HLL or RUSANOV");
   if (o.stop_cr != 0 && o.stop_cr != 1) return set_error(STORM_ERR_ARG, "stop_cr must be 0 or 1");
-  if (o.precision != STORM_PREC_FP64)
-    return set_error(STORM_ERR_UNSUPPORTED, "only STORM_PREC_FP64 is available in this version");
+  if (o.precision != STORM_PREC_FP64 && o.precision != STORM_PREC_MIXED)
+    return set_error(STORM_ERR_ARG, "precision must be STORM_PREC_FP64 or STORM_PREC_MIXED");
   if (!(o.h_dry > 0.0) || !(o.h_wet >= o.h_dry)) return set_error(STORM_ERR_ARG, "need 0 < h_dry <= h_wet");
   if (!(o.cfl > 0.0)) return set_error(STORM_ERR_ARG, "cfl must be positive");
   for (int i = 0; i < 6; i++)
@@ -138,42 +137,57 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     CK(cudaEventRecord(h->fev[(*fev_used)++], h->stream));
     return 0;
   };
+  auto launch = [&](int which, int grid, int block, size_t smem, cudaStream_t st, int s, const double* hs,
+                    uint8_t* dry, uint8_t* dry_next) {
+    StageLaunch L;
+    L.which = which;
+    L.grid = dim3(grid);
+    L.block = dim3(block);
+    L.smem = smem;
+    L.stream = st;
+    L.s = s;
+    L.hs = hs;
+    L.dry = dry;
+    L.dry_next = dry_next;
+    L.rku_prev = d.rku + (size_t)(s - 1) * T;
+    L.rkv_prev = d.rkv + (size_t)(s - 1) * T;
+    launch_stage(L, d, h->gd, h->gf, h->mixed);
+  };
   for (int s = 1; s <= K; s++) {
     const double* hs = d.rkh + (size_t)(s - 1) * T;
     uint8_t* dry = (s & 1) ? d.dry_a : d.dry_b;
     uint8_t* dry_next = (s & 1) ? d.dry_b : d.dry_a;
+    const int gB = (d.nbc_cells + kFluxThreads - 1) / kFluxThreads;
     if (mark(KT_NODE)) return STORM_ERR_CUDA;
     k_node<<<gN, kNodeThreads, 0, h->stream>>>(d, hs, dry);
     if (done() || mark(KT_GRAD)) return STORM_ERR_CUDA;
-    k_grad<<<gT, kCellThreads, 0, h->stream>>>(d, hs, dry, d.rku + (size_t)(s - 1) * T, d.rkv + (size_t)(s - 1) * T);
+    launch(STAGE_GRAD, gT, kCellThreads, 0, h->stream, s, hs, dry, dry_next);
     if (done()) return STORM_ERR_CUDA;
     if (d.nbdr > 0 && !timing) {
       // k_bc on the side stream overlaps k_eflux and k_flux of the cells without
       // boundary faces; the boundary cells are finished once both are done
       CK(cudaEventRecord(h->fork_ev[s], h->stream));
       CK(cudaStreamWaitEvent(h->side, h->fork_ev[s], 0));
-      k_bc<<<d.nbdr, 128, h->bc_smem, h->side>>>(d, hs, dry);
+      launch(STAGE_BC, d.nbdr, 128, h->bc_smem, h->side, s, hs, dry, dry_next);
       CK(cudaEventRecord(h->join_ev[s], h->side));
-      if (gE > 0) k_eflux<<<gE, kFluxThreads, 0, h->stream>>>(d, hs, dry);
-      k_flux<<<gF, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
+      if (gE > 0) launch(STAGE_EFLUX, gE, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+      launch(STAGE_FLUX, gF, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
       CK(cudaStreamWaitEvent(h->stream, h->join_ev[s], 0));
-      const int gB = (d.nbc_cells + kFluxThreads - 1) / kFluxThreads;
-      if (gB > 0) k_flux_bc<<<gB, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
+      if (gB > 0) launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
     } else {
       if (d.nbdr > 0) {
         if (mark(KT_BC)) return STORM_ERR_CUDA;
-        k_bc<<<d.nbdr, 128, h->bc_smem, h->stream>>>(d, hs, dry);
+        launch(STAGE_BC, d.nbdr, 128, h->bc_smem, h->stream, s, hs, dry, dry_next);
         if (done()) return STORM_ERR_CUDA;
       }
       if (gE > 0) {
         if (mark(KT_EFLUX)) return STORM_ERR_CUDA;
-        k_eflux<<<gE, kFluxThreads, 0, h->stream>>>(d, hs, dry);
+        launch(STAGE_EFLUX, gE, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
         if (done()) return STORM_ERR_CUDA;
       }
       if (mark(KT_FLUX)) return STORM_ERR_CUDA;
-      k_flux<<<gF, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
-      const int gB = (d.nbc_cells + kFluxThreads - 1) / kFluxThreads;
-      if (gB > 0) k_flux_bc<<<gB, kFluxThreads, 0, h->stream>>>(d, s, hs, dry, dry_next);
+      launch(STAGE_FLUX, gF, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+      if (gB > 0) launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
       if (done()) return STORM_ERR_CUDA;
     }
   }
@@ -220,6 +234,7 @@ void release(StormFvtHandle* h) {
   if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (h->arena) cudaFree(h->arena);
+  if (h->arena32) cudaFree(h->arena32);
   if (h->sc_host) cudaFreeHost(h->sc_host);
   delete h;
 }
@@ -340,6 +355,57 @@ int upload(StormFvtHandle* h) {
   d.eL = at<int32_t>(B, o_eL); d.eR = at<int32_t>(B, o_eR); d.eslot = at<uint8_t>(B, o_es);
   d.enx = at<double>(B, o_enx); d.eny = at<double>(B, o_eny); d.elen = at<double>(B, o_el);
   d.ez0 = at<double>(B, o_ez0); d.efx = at<double>(B, o_efx); d.eok = at<uint8_t>(B, o_eok);
+  // FP64 views of the arithmetic-type arrays
+  Geo<double>& gd = h->gd;
+  gd.rc_x = d.rc_x; gd.rc_y = d.rc_y; gd.st_w = d.st_w; gd.st_dx = d.st_dx; gd.st_dy = d.st_dy;
+  gd.lsq_a = d.lsq_a; gd.lsq_b = d.lsq_b; gd.lsq_c = d.lsq_c; gd.lsq_det = d.lsq_det;
+  gd.delz_x = d.delz_x; gd.delz_y = d.delz_y; gd.enx = d.enx; gd.eny = d.eny; gd.elen = d.elen;
+  gd.delh_x = d.delh_x; gd.delh_y = d.delh_y; gd.delu_x = d.delu_x; gd.delu_y = d.delu_y;
+  gd.delv_x = d.delv_x; gd.delv_y = d.delv_y; gd.efx = d.efx;
+  // FP32 copies for the mixed-precision path: the gradients and edge fluxes reuse the
+  // FP64 buffers (a float array fits in the same bytes)
+  Geo<float>& gf = h->gf;
+  gf.delh_x = reinterpret_cast<float*>(d.delh_x); gf.delh_y = reinterpret_cast<float*>(d.delh_y);
+  gf.delu_x = reinterpret_cast<float*>(d.delu_x); gf.delu_y = reinterpret_cast<float*>(d.delu_y);
+  gf.delv_x = reinterpret_cast<float*>(d.delv_x); gf.delv_y = reinterpret_cast<float*>(d.delv_y);
+  gf.efx = reinterpret_cast<float*>(d.efx);
+  if (h->mixed) {
+    auto f32 = [&](const std::vector<double>& v) {
+      std::vector<float> f(v.size());
+      for (size_t i = 0; i < v.size(); i++) f[i] = (float)v[i];
+      return f;
+    };
+    struct FCopy {
+      const float** dst;
+      std::vector<float> host;
+    };
+    std::vector<FCopy> fc;
+    fc.push_back({&gf.rc_x, f32(L.rc_x)});
+    fc.push_back({&gf.rc_y, f32(L.rc_y)});
+    fc.push_back({&gf.st_w, f32(L.st_w)});
+    fc.push_back({&gf.st_dx, f32(L.st_dx)});
+    fc.push_back({&gf.st_dy, f32(L.st_dy)});
+    fc.push_back({&gf.lsq_a, f32(L.lsq_a)});
+    fc.push_back({&gf.lsq_b, f32(L.lsq_b)});
+    fc.push_back({&gf.lsq_c, f32(L.lsq_c)});
+    fc.push_back({&gf.lsq_det, f32(L.lsq_det)});
+    fc.push_back({&gf.delz_x, f32(L.delz_x)});
+    fc.push_back({&gf.delz_y, f32(L.delz_y)});
+    fc.push_back({&gf.enx, f32(L.enx)});
+    fc.push_back({&gf.eny, f32(L.eny)});
+    fc.push_back({&gf.elen, f32(L.elen)});
+    size_t total = 0;
+    for (auto& c : fc) total += (c.host.size() * 4 + 255) & ~(size_t)255;
+    cudaError_t ef = cudaMalloc(&h->arena32, std::max<size_t>(total, 256));
+    if (ef != cudaSuccess) return set_error(STORM_ERR_NOMEM, std::string("device allocation (mixed): ") + cudaGetErrorString(ef));
+    size_t off = 0;
+    for (auto& c : fc) {
+      float* p = reinterpret_cast<float*>(static_cast<char*>(h->arena32) + off);
+      if (!c.host.empty()) CK(cudaMemcpy(p, c.host.data(), c.host.size() * 4, cudaMemcpyHostToDevice));
+      *c.dst = p;
+      off += (c.host.size() * 4 + 255) & ~(size_t)255;
+    }
+  }
   d.bc_cells = at<int32_t>(B, o_bcl);
   // boundary values
   Scalars s0{};
@@ -349,7 +415,7 @@ int upload(StormFvtHandle* h) {
   int maxcnt = 1;
   for (int b = 0; b < L.nbdr; b++) maxcnt = std::max(maxcnt, L.bdr_cnt[b]);
   h->bc_smem = (size_t)maxcnt * 2 * sizeof(double) + (((size_t)maxcnt + 7) & ~(size_t)7);
-  if (h->bc_smem > 48 * 1024) CK(cudaFuncSetAttribute(k_bc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->bc_smem));
+  if (h->bc_smem > 48 * 1024) set_bc_smem_limit((int)h->bc_smem);
   return 0;
 }
 
@@ -398,6 +464,7 @@ int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, Storm
   if (!h) return set_error(STORM_ERR_NOMEM, "storm_fvt_create: out of memory");
   h->opt = *opt;
   h->device = opt->device;
+  h->mixed = opt->precision == STORM_PREC_MIXED;
   try {
     rc = build_layout(*mesh, *opt, h->L);
   } catch (const std::bad_alloc&) {

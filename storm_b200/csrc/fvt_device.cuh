@@ -9,6 +9,8 @@
 
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 namespace storm {
 
 constexpr int kMaxBdrDev = 16;
@@ -74,5 +76,31 @@ struct Dev {
   int32_t nblk_red;
   Scalars* sc;
 };
+
+// Geometry and per-stage arrays read or written in the flux/gradient arithmetic type R:
+// double views of the FP64 arrays, or float copies for the mixed-precision path.
+template <class R>
+struct Geo {
+  const R *rc_x, *rc_y, *st_w, *st_dx, *st_dy, *lsq_a, *lsq_b, *lsq_c, *lsq_det, *delz_x, *delz_y;
+  const R *enx, *eny, *elen;
+  R *delh_x, *delh_y, *delu_x, *delu_y, *delv_x, *delv_y;
+  R* efx;  // [3][ne]
+};
+
+// One launch of a templated stage kernel (see launch_stage in fvt_kernels.cu).
+enum StageKernel { STAGE_GRAD, STAGE_BC, STAGE_EFLUX, STAGE_FLUX, STAGE_FLUX_BC };
+struct StageLaunch {
+  int which;
+  dim3 grid, block;
+  size_t smem;
+  cudaStream_t stream;
+  int s;
+  const double* hs;
+  const uint8_t* dry;
+  uint8_t* dry_next;
+  double *rku_prev, *rkv_prev;
+};
+void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed);
+void set_bc_smem_limit(int bytes);
 
 }  // namespace storm

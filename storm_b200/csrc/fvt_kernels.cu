@@ -60,81 +60,91 @@ __device__ __forceinline__ bool dry_flag(double h, double u, double v, double h_
   return dry;
 }
 
+// Arithmetic type of the flux, gradient and source kernels: double reproduces the
+// reference bit for bit; float is the mixed-precision path (state, the eta - zb
+// reconstruction at the faces and the RK accumulation stay in double).
+__device__ __forceinline__ float fmin2(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float fmax2(float a, float b) { return (b > a) ? b : a; }
+// x + 0: the first step of each MATMUL sum (turns a -0 product into +0)
+__device__ __forceinline__ double add0(double x) { return __dadd_rn(x, 0.0); }
+__device__ __forceinline__ float add0(float x) { return __fadd_rn(x, 0.0f); }
+
 // flux_ac.f90:48-126.  The MATMULs start from zero and add x(i,k)*y(k,j) for
 // k = 1..3; with the diagonal eigenvalue matrix (entries >= delta > 0) the first
 // product reduces exactly to rev(i,j)*eigv(j) + 0.
-__device__ __forceinline__ void flux_roe(double nx, double ny, double hleft, double uleft, double vleft,
-                                         double hright, double uright, double vright, double* flux) {
-  const double delta = 0.10;
-  double fl[3], gl[3], fr[3], gr[3];
+template <class R>
+__device__ __forceinline__ void flux_roe(R nx, R ny, R hleft, R uleft, R vleft, R hright, R uright, R vright,
+                                         R* flux) {
+  const R delta = R(0.10);
+  R fl[3], gl[3], fr[3], gr[3];
   fl[0] = hleft * uleft;
-  fl[1] = hleft * uleft * uleft + kHalf * kG * hleft * hleft;
+  fl[1] = hleft * uleft * uleft + R(kHalf) * R(kG) * hleft * hleft;
   fl[2] = hleft * uleft * vleft;
   gl[0] = hleft * vleft;
   gl[1] = hleft * uleft * vleft;
-  gl[2] = hleft * vleft * vleft + kHalf * kG * hleft * hleft;
+  gl[2] = hleft * vleft * vleft + R(kHalf) * R(kG) * hleft * hleft;
   fr[0] = hright * uright;
-  fr[1] = hright * uright * uright + kHalf * kG * hright * hright;
+  fr[1] = hright * uright * uright + R(kHalf) * R(kG) * hright * hright;
   fr[2] = hright * uright * vright;
   gr[0] = hright * vright;
   gr[1] = hright * uright * vright;
-  gr[2] = hright * vright * vright + kHalf * kG * hright * hright;
-  hleft = fmax2(hleft, SMALL_F);
-  double hls = sqrt(hleft);
-  hright = fmax2(hright, SMALL_F);
-  double hrs = sqrt(hright);
-  double denom = hrs + hls;
-  double uavg = (uright * hrs + uleft * hls) / denom;
-  double vavg = (vright * hrs + vleft * hls) / denom;
-  double cavg = sqrt(kHalf * kG * (hleft + hright));
-  double q[3];
+  gr[2] = hright * vright * vright + R(kHalf) * R(kG) * hright * hright;
+  hleft = fmax2(hleft, R(SMALL_F));
+  R hls = sqrt(hleft);
+  hright = fmax2(hright, R(SMALL_F));
+  R hrs = sqrt(hright);
+  R denom = hrs + hls;
+  R uavg = (uright * hrs + uleft * hls) / denom;
+  R vavg = (vright * hrs + vleft * hls) / denom;
+  R cavg = sqrt(R(kHalf) * R(kG) * (hleft + hright));
+  R q[3];
   q[0] = hright - hleft;
   q[1] = hright * uright - hleft * uleft;
   q[2] = hright * vright - hleft * vleft;
-  double rev[3][3], lev[3][3], t1[3][3], eig[3];
-  rev[0][0] = kZero; rev[0][1] = kOne; rev[0][2] = kOne;
+  R rev[3][3], lev[3][3], t1[3][3], eig[3];
+  rev[0][0] = R(kZero); rev[0][1] = R(kOne); rev[0][2] = R(kOne);
   rev[1][0] = ny; rev[1][1] = uavg - cavg * nx; rev[1][2] = uavg + cavg * nx;
   rev[2][0] = -nx; rev[2][1] = vavg - cavg * ny; rev[2][2] = vavg + cavg * ny;
   lev[0][0] = -(uavg * ny - vavg * nx);
   lev[0][1] = ny;
   lev[0][2] = -nx;
-  lev[1][0] = kHalf * (uavg * nx + vavg * ny) / cavg + kHalf;
-  lev[1][1] = -(kHalf * nx / cavg);
-  lev[1][2] = -(kHalf * ny / cavg);
-  lev[2][0] = -(kHalf * (uavg * nx + vavg * ny) / cavg) + kHalf;
-  lev[2][1] = kHalf * nx / cavg;
-  lev[2][2] = kHalf * ny / cavg;
+  lev[1][0] = R(kHalf) * (uavg * nx + vavg * ny) / cavg + R(kHalf);
+  lev[1][1] = -(R(kHalf) * nx / cavg);
+  lev[1][2] = -(R(kHalf) * ny / cavg);
+  lev[2][0] = -(R(kHalf) * (uavg * nx + vavg * ny) / cavg) + R(kHalf);
+  lev[2][1] = R(kHalf) * nx / cavg;
+  lev[2][2] = R(kHalf) * ny / cavg;
   eig[0] = fmax2(fabs(uavg * nx + vavg * ny), delta);
   eig[1] = fmax2(fabs(uavg * nx + vavg * ny - cavg), delta);
   eig[2] = fmax2(fabs(uavg * nx + vavg * ny + cavg), delta);
 #pragma unroll
   for (int i = 0; i < 3; i++)
 #pragma unroll
-    for (int j = 0; j < 3; j++) t1[i][j] = __dadd_rn(rev[i][j] * eig[j], kZero);
-  double aq[3];
+    for (int j = 0; j < 3; j++) t1[i][j] = add0(rev[i][j] * eig[j]);
+  R aq[3];
 #pragma unroll
   for (int i = 0; i < 3; i++) {
-    double t2[3];
+    R t2[3];
 #pragma unroll
     for (int j = 0; j < 3; j++)
-      t2[j] = (__dadd_rn(t1[i][0] * lev[0][j], kZero) + t1[i][1] * lev[1][j]) + t1[i][2] * lev[2][j];
-    aq[i] = (__dadd_rn(t2[0] * q[0], kZero) + t2[1] * q[1]) + t2[2] * q[2];
+      t2[j] = (add0(t1[i][0] * lev[0][j]) + t1[i][1] * lev[1][j]) + t1[i][2] * lev[2][j];
+    aq[i] = (add0(t2[0] * q[0]) + t2[1] * q[1]) + t2[2] * q[2];
   }
 #pragma unroll
-  for (int i = 0; i < 3; i++) flux[i] = kHalf * (fr[i] * nx + gr[i] * ny + fl[i] * nx + gl[i] * ny - aq[i]);
+  for (int i = 0; i < 3; i++) flux[i] = R(kHalf) * (fr[i] * nx + gr[i] * ny + fl[i] * nx + gl[i] * ny - aq[i]);
 }
 
 // flux_HLL.f90:41-110 with its two defects fixed (flux(3) assigned; the whole HLL
 // numerator divided by sright - sleft).  The debug stop at :88-91 sets *bad.
-__device__ __forceinline__ void flux_hll(double nx, double ny, double hleft, double uleft, double vleft,
-                                         double hright, double uright, double vright, double h0, double* flux,
-                                         bool* bad) {
-  double cleft = sqrt(kG * hleft);
-  double cright = sqrt(kG * hright);
-  double ustar = kHalf * ((uleft + uright) * nx + (vleft + vright) * ny) + cleft - cright;
-  double cstar = kHalf * (cleft + cright) + ((uleft - uright) * nx + (vleft - vright) * ny) / 4.0;
-  double sleft, sright, aux1, aux2;
-  if (hleft < h0) sleft = uright * nx + vright * ny - 2.0 * cright;
+template <class R>
+__device__ __forceinline__ void flux_hll(R nx, R ny, R hleft, R uleft, R vleft, R hright, R uright, R vright,
+                                         R h0, R* flux, bool* bad) {
+  R cleft = sqrt(R(kG) * hleft);
+  R cright = sqrt(R(kG) * hright);
+  R ustar = R(kHalf) * ((uleft + uright) * nx + (vleft + vright) * ny) + cleft - cright;
+  R cstar = R(kHalf) * (cleft + cright) + ((uleft - uright) * nx + (vleft - vright) * ny) / R(4.0);
+  R sleft, sright, aux1, aux2;
+  if (hleft < h0) sleft = uright * nx + vright * ny - R(2.0) * cright;
   else if (hright < h0) sleft = uleft * nx + vleft * ny - cleft;
   else {
     aux1 = uleft * nx + vleft * ny - cleft;
@@ -142,29 +152,29 @@ __device__ __forceinline__ void flux_hll(double nx, double ny, double hleft, dou
     sleft = fmin2(aux1, aux2);
   }
   if (hleft < h0) sright = uright * nx + vright * ny + cright;
-  else if (hright < h0) sright = uleft * nx + vleft * ny + 2.0 * cleft;
+  else if (hright < h0) sright = uleft * nx + vleft * ny + R(2.0) * cleft;
   else {
     aux1 = uright * nx + vright * ny - cright;
     aux2 = ustar + cstar;
     sright = fmax2(aux1, aux2);
   }
-  double fl[3], gl[3], fr[3], gr[3];
+  R fl[3], gl[3], fr[3], gr[3];
   fl[0] = hleft * uleft * nx;
-  fl[1] = (hleft * uleft * uleft + kHalf * kG * hleft * hleft) * nx;
+  fl[1] = (hleft * uleft * uleft + R(kHalf) * R(kG) * hleft * hleft) * nx;
   fl[2] = hleft * uleft * vleft * nx;
   gl[0] = hleft * vleft * ny;
   gl[1] = hleft * uleft * vleft * ny;
-  gl[2] = (hleft * vleft * vleft + kHalf * kG * hleft * hleft) * ny;
+  gl[2] = (hleft * vleft * vleft + R(kHalf) * R(kG) * hleft * hleft) * ny;
   fr[0] = hright * uright * nx;
-  fr[1] = (hright * uright * uright + kHalf * kG * hright * hright) * nx;
+  fr[1] = (hright * uright * uright + R(kHalf) * R(kG) * hright * hright) * nx;
   fr[2] = hright * uright * vright * nx;
   gr[0] = hright * vright * ny;
   gr[1] = hright * uright * vright * ny;
-  gr[2] = (hright * vright * vright + kHalf * kG * hright * hright) * ny;
-  if (sleft > kZero && sright < kZero) *bad = true;
-  if (sleft > kZero) {
+  gr[2] = (hright * vright * vright + R(kHalf) * R(kG) * hright * hright) * ny;
+  if (sleft > R(kZero) && sright < R(kZero)) *bad = true;
+  if (sleft > R(kZero)) {
     for (int i = 0; i < 3; i++) flux[i] = fl[i] + gl[i];
-  } else if (sright < kZero) {
+  } else if (sright < R(kZero)) {
     for (int i = 0; i < 3; i++) flux[i] = fr[i] + gr[i];
   } else {
     aux1 = sright - sleft;
@@ -177,30 +187,30 @@ __device__ __forceinline__ void flux_hll(double nx, double ny, double hleft, dou
 }
 
 // flux_rusanov.f90:47-80
-__device__ __forceinline__ void flux_rusanov(double nx, double ny, double hleft, double uleft, double vleft,
-                                             double cl, double hright, double uright, double vright, double cr,
-                                             double* flux) {
-  double fl[3], gl[3], fr[3], gr[3], q[3];
+template <class R>
+__device__ __forceinline__ void flux_rusanov(R nx, R ny, R hleft, R uleft, R vleft, R cl, R hright, R uright,
+                                             R vright, R cr, R* flux) {
+  R fl[3], gl[3], fr[3], gr[3], q[3];
   fl[0] = hleft * uleft;
-  fl[1] = hleft * uleft * uleft + kHalf * kG * hleft * hleft;
+  fl[1] = hleft * uleft * uleft + R(kHalf) * R(kG) * hleft * hleft;
   fl[2] = hleft * uleft * vleft;
   gl[0] = hleft * vleft;
   gl[1] = hleft * uleft * vleft;
-  gl[2] = hleft * vleft * vleft + kHalf * kG * hleft * hleft;
+  gl[2] = hleft * vleft * vleft + R(kHalf) * R(kG) * hleft * hleft;
   fr[0] = hright * uright;
-  fr[1] = hright * uright * uright + kHalf * kG * hright * hright;
+  fr[1] = hright * uright * uright + R(kHalf) * R(kG) * hright * hright;
   fr[2] = hright * uright * vright;
   gr[0] = hright * vright;
   gr[1] = hright * uright * vright;
-  gr[2] = hright * vright * vright + kHalf * kG * hright * hright;
-  double ul = uleft * nx + vleft * ny;
-  double ur = uright * nx + vright * ny;
-  double splus = fmax2(fabs(ul) + cl, fabs(ur) + cr);
+  gr[2] = hright * vright * vright + R(kHalf) * R(kG) * hright * hright;
+  R ul = uleft * nx + vleft * ny;
+  R ur = uright * nx + vright * ny;
+  R splus = fmax2(fabs(ul) + cl, fabs(ur) + cr);
   q[0] = hright - hleft;
   q[1] = hright * uright - hleft * uleft;
   q[2] = hright * vright - hleft * vleft;
 #pragma unroll
-  for (int i = 0; i < 3; i++) flux[i] = kHalf * (fr[i] * nx + gr[i] * ny + fl[i] * nx + gl[i] * ny - splus * q[i]);
+  for (int i = 0; i < 3; i++) flux[i] = R(kHalf) * (fr[i] * nx + gr[i] * ny + fl[i] * nx + gl[i] * ny - splus * q[i]);
 }
 
 // Block-level reductions in a fixed order (warp xor-shuffle tree, then warps in order).
@@ -367,36 +377,77 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ 
   d.hvtx[n] = hv;
 }
 
+// The face value of a cell field, x + grad . rc (invisc_fluxes.f90:58-64): in double as
+// the reference writes it; on the mixed path the FP32 correction is added to the FP64
+// value, so the depth at a wet/dry front keeps its eta - zb precision.
+__device__ __forceinline__ double recon(double x, double gx, double rx, double gy, double ry) {
+  return x + gx * rx + gy * ry;
+}
+__device__ __forceinline__ double recon(double x, float gx, float rx, float gy, float ry) {
+  return x + (double)(gx * rx + gy * ry);
+}
+
 // ---------------------------------------------------------------------------
-// Limited LSQ gradients, hgradfix2 and the partially-wet velocity zeroing.
-__global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry,
-                                              double* __restrict__ rku_prev, double* __restrict__ rkv_prev) {
+// Limited LSQ gradients, hgradfix2 and the partially-wet velocity zeroing
+// (lsq_grad_array.f90:60-73, limiterBJ.f90:42-81 with beta = one, cell_grads.f90:72-75,
+// hgradfix2.f90:48-98, to_vertices.f90:44-55).  Differences of the FP64 fields are
+// taken in double and then rounded to R.
+__device__ __forceinline__ double limited_r(double q0, double qn, double g_x, double g_y, double rx, double ry) {
+  const double qmin = fmin2(q0, qn);
+  const double qmax = fmax2(q0, qn);
+  const double qj = q0 + g_x * rx + g_y * ry;
+  const double delq = qj - q0;
+  double rj;
+  if (equals(delq, kZero)) rj = kOne;
+  else {
+    // r = (qmin-q0)/delq for delq < 0, (qmax-q0)/delq otherwise; both are >= 0.
+    // When |num| > |delq| the exact quotient exceeds one, so the rounded one is
+    // >= 1 and the limiter's min(r,1) is 1: the division is skipped, same bits.
+    const double num = (delq < 0) ? (qmin - q0) : (qmax - q0);
+    rj = (fabs(num) > fabs(delq)) ? kOne : num / delq;
+  }
+  const double a = fmin2(kOne * rj, kOne);
+  const double b = fmin2(rj, kOne);
+  return fmax2(a, b);
+}
+__device__ __forceinline__ float limited_r(double q0, double qn, float g_x, float g_y, float rx, float ry) {
+  const float dmin = (float)(fmin2(q0, qn) - q0), dmax = (float)(fmax2(q0, qn) - q0);
+  const float delq = g_x * rx + g_y * ry;
+  if (fabsf(delq) <= 1e-30f) return 1.0f;
+  const float num = (delq < 0) ? dmin : dmax;
+  return (fabsf(num) >= fabsf(delq)) ? 1.0f : num / delq;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, double* __restrict__ rku_prev,
+                                              double* __restrict__ rkv_prev) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.T || d.sc->converged) return;
   const int T = d.T;
   const double zeta_c = hs[c] + d.z[c];
   const double u_c = d.u_a[c], v_c = d.v_a[c];
-  double hx = kZero, hy = kZero, ux = kZero, uy = kZero, vx = kZero, vy = kZero;
+  R hx = R(0), hy = R(0), ux = R(0), uy = R(0), vx = R(0), vy = R(0);
   if (d.lim == 1 || d.lim == 2) {
-    double dz = kZero, ez = kZero, du = kZero, eu = kZero, dv = kZero, ev = kZero;
+    R dz = R(0), ez = R(0), du = R(0), eu = R(0), dv = R(0), ev = R(0);
     const int n = d.nst[c];
     int k0 = 0;
     if (n >= 3) {  // interior cells: the three face neighbours, all gathers issued together
       int jj[3];
-      double w[3], dx[3], dy[3], pz[3], pu[3], pv[3];
+      R w[3], dx[3], dy[3], pz[3], pu[3], pv[3];
 #pragma unroll
       for (int k = 0; k < 3; k++) {
         const size_t q = (size_t)k * T + c;
         jj[k] = d.st_id[q];
-        w[k] = d.st_w[q];
-        dx[k] = d.st_dx[q];
-        dy[k] = d.st_dy[q];
+        w[k] = G.st_w[q];
+        dx[k] = G.st_dx[q];
+        dy[k] = G.st_dy[q];
       }
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        pz[k] = (hs[jj[k]] + d.z[jj[k]]) - zeta_c;
-        pu[k] = d.u_a[jj[k]] - u_c;
-        pv[k] = d.v_a[jj[k]] - v_c;
+        pz[k] = (R)((hs[jj[k]] + d.z[jj[k]]) - zeta_c);
+        pu[k] = (R)(d.u_a[jj[k]] - u_c);
+        pv[k] = (R)(d.v_a[jj[k]] - v_c);
       }
 #pragma unroll
       for (int k = 0; k < 3; k++) {
@@ -412,10 +463,10 @@ __global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ 
     for (int k = k0; k < n; k++) {
       const size_t q = (size_t)k * T + c;
       const int j = d.st_id[q];
-      const double w = d.st_w[q], dx = d.st_dx[q], dy = d.st_dy[q];
-      const double pz = (hs[j] + d.z[j]) - zeta_c;
-      const double pu = d.u_a[j] - u_c;
-      const double pv = d.v_a[j] - v_c;
+      const R w = G.st_w[q], dx = G.st_dx[q], dy = G.st_dy[q];
+      const R pz = (R)((hs[j] + d.z[j]) - zeta_c);
+      const R pu = (R)(d.u_a[j] - u_c);
+      const R pv = (R)(d.v_a[j] - v_c);
       dz = dz + w * pz * dx;
       ez = ez + w * pz * dy;
       du = du + w * pu * dx;
@@ -423,7 +474,7 @@ __global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ 
       dv = dv + w * pv * dx;
       ev = ev + w * pv * dy;
     }
-    const double ai = d.lsq_a[c], bi = d.lsq_b[c], ci = d.lsq_c[c], det = d.lsq_det[c];
+    const R ai = G.lsq_a[c], bi = G.lsq_b[c], ci = G.lsq_c[c], det = G.lsq_det[c];
     hx = (ci * dz - bi * ez) / det;
     hy = (ai * ez - dz * bi) / det;
     ux = (ci * du - bi * eu) / det;
@@ -432,52 +483,28 @@ __global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ 
     vy = (ai * ev - dv * bi) / det;
   }
   if (d.lim == 2) {  // limiterBJ.f90:42-81, beta = one
-    double qn[3][3], rcx[3], rcy[3];
+    R rz[3], ru[3], rv[3];
 #pragma unroll
     for (int j = 0; j < 3; j++) {
       const size_t q = (size_t)j * T + c;
       const int k = d.t2t3[q];
-      rcx[j] = d.rc_x[q];
-      rcy[j] = d.rc_y[q];
-      if (k < 0) {
-        qn[0][j] = zeta_c; qn[1][j] = u_c; qn[2][j] = v_c;
-      } else {
-        qn[0][j] = hs[k] + d.z[k]; qn[1][j] = d.u_a[k]; qn[2][j] = d.v_a[k];
-      }
+      const R rx = G.rc_x[q], ry = G.rc_y[q];
+      const double qz = k < 0 ? zeta_c : hs[k] + d.z[k];
+      const double qu = k < 0 ? u_c : d.u_a[k];
+      const double qv = k < 0 ? v_c : d.v_a[k];
+      rz[j] = limited_r(zeta_c, qz, hx, hy, rx, ry);
+      ru[j] = limited_r(u_c, qu, ux, uy, rx, ry);
+      rv[j] = limited_r(v_c, qv, vx, vy, rx, ry);
     }
-    double* gx[3] = {&hx, &ux, &vx};
-    double* gy[3] = {&hy, &uy, &vy};
-    const double q0v[3] = {zeta_c, u_c, v_c};
-#pragma unroll
-    for (int f = 0; f < 3; f++) {
-      const double q0 = q0v[f];
-      double r[3];
-#pragma unroll
-      for (int j = 0; j < 3; j++) {
-        const double qmin = fmin2(q0, qn[f][j]);
-        const double qmax = fmax2(q0, qn[f][j]);
-        const double qj = q0 + *gx[f] * rcx[j] + *gy[f] * rcy[j];
-        const double delq = qj - q0;
-        double rj;
-        if (equals(delq, kZero)) rj = kOne;
-        else {
-          // r = (qmin-q0)/delq for delq < 0, (qmax-q0)/delq otherwise; both are >= 0.
-          // When |num| > |delq| the exact quotient exceeds one, so the rounded one is
-          // >= 1 and the limiter's min(r,1) is 1: the division is skipped, same bits.
-          const double num = (delq < 0) ? (qmin - q0) : (qmax - q0);
-          rj = (fabs(num) > fabs(delq)) ? kOne : num / delq;
-        }
-        const double a = fmin2(kOne * rj, kOne);
-        const double b = fmin2(rj, kOne);
-        r[j] = fmax2(a, b);
-      }
-      const double phi = fmin2(fmin2(r[0], r[1]), r[2]);
-      *gx[f] = phi * *gx[f];
-      *gy[f] = phi * *gy[f];
-    }
+    const R pz = fmin2(fmin2(rz[0], rz[1]), rz[2]);
+    const R pu = fmin2(fmin2(ru[0], ru[1]), ru[2]);
+    const R pv = fmin2(fmin2(rv[0], rv[1]), rv[2]);
+    hx = pz * hx; hy = pz * hy;
+    ux = pu * ux; uy = pu * uy;
+    vx = pv * vx; vy = pv * vy;
   }
-  hx = hx - d.delz_x[c];
-  hy = hy - d.delz_y[c];
+  hx = hx - G.delz_x[c];
+  hy = hy - G.delz_y[c];
   double ub = u_c, vb = v_c;
   if (!dry[c]) {
     // hgradfix2.f90:48-98
@@ -489,13 +516,13 @@ __global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ 
       if (dry[l] && d.z[l] < zeta_c) setgrad = false;
     }
     if (setgrad) {
-      hx = -d.delz_x[c];
-      hy = -d.delz_y[c];
+      hx = -G.delz_x[c];
+      hy = -G.delz_y[c];
       ub = kZero;
       vb = kZero;
       rku_prev[c] = kZero;
       rkv_prev[c] = kZero;
-      ux = kZero; uy = kZero; vx = kZero; vy = kZero;
+      ux = R(0); uy = R(0); vx = R(0); vy = R(0);
     }
     // to_vertices.f90:44-55
     bool flag = true;
@@ -506,9 +533,9 @@ __global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ 
       vb = kZero;
     }
   }
-  d.delh_x[c] = hx; d.delh_y[c] = hy;
-  d.delu_x[c] = ux; d.delu_y[c] = uy;
-  d.delv_x[c] = vx; d.delv_y[c] = vy;
+  G.delh_x[c] = hx; G.delh_y[c] = hy;
+  G.delu_x[c] = ux; G.delu_y[c] = uy;
+  G.delv_x[c] = vx; G.delv_y[c] = vy;
   d.u_b[c] = ub;
   d.v_b[c] = vb;
 }
@@ -520,7 +547,8 @@ __global__ void __launch_bounds__(256) k_grad(Dev d, const double* __restrict__ 
 // string order, so they round exactly as the reference's loops.
 constexpr int kBcThreads = 128;
 
-__global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, const double* __restrict__ hs,
+template <class R>
+__global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double* __restrict__ hs,
                                                    const uint8_t* __restrict__ dry) {
   if (d.sc->converged) return;
   extern __shared__ double smb[];
@@ -538,9 +566,9 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, const double* __restri
   for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
     const int i = d.bce_cell[off + e], m = d.bce_slot[off + e];
     const size_t q = (size_t)m * T + i;
-    d.bc_rec[off + e] = hs[i] + d.delh_x[i] * d.rc_x[q] + d.delh_y[i] * d.rc_y[q];
-    d.bc_rec[NB + off + e] = d.u_b[i] + d.delu_x[i] * d.rc_x[q] + d.delu_y[i] * d.rc_y[q];
-    d.bc_rec[2 * NB + off + e] = d.v_b[i] + d.delv_x[i] * d.rc_x[q] + d.delv_y[i] * d.rc_y[q];
+    d.bc_rec[off + e] = recon(hs[i], G.delh_x[i], G.rc_x[q], G.delh_y[i], G.rc_y[q]);
+    d.bc_rec[NB + off + e] = recon(d.u_b[i], G.delu_x[i], G.rc_x[q], G.delu_y[i], G.rc_y[q]);
+    d.bc_rec[2 * NB + off + e] = recon(d.v_b[i], G.delv_x[i], G.rc_x[q], G.delv_y[i], G.rc_y[q]);
   }
   __syncthreads();
   auto put = [&](int e, double c1, double c2, double c3) {
@@ -691,7 +719,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, const double* __restri
       uleft = uedg;
       const double vleft = vedg;
       if (hleft < h_dry && hright < h_dry) valid = false;
-      else flux_roe(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
+      else flux_roe<double>(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
       if (valid) { tA[e] = f[0] * len; put(e, f[0] * len, f[1] * len, f[2] * len); }
     } else if (kind == BC_HOUT) {  // outflowbyH.f90:30-137
       double uedg, vedg;
@@ -721,7 +749,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, const double* __restri
           const double dot = uright * nx + vright * ny;
           if (dot < kZero) { set_wall = true; hright = hleft; uright = kZero; vright = kZero; }
         }
-        flux_roe(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
+        flux_roe<double>(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
         if (set_wall) f[0] = kZero;
         tA[e] = f[0] * len;
         put(e, f[0] * len, f[1] * len, f[2] * len);
@@ -765,7 +793,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, const double* __restri
           const double dot = uright * nx + vright * ny;
           if (dot < 0) { set_wall = true; uright = kZero; vright = kZero; }
         }
-        flux_roe(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
+        flux_roe<double>(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
         if (set_wall) f[0] = kZero;
         put(e, f[0] * len, f[1] * len, f[2] * len);
       }
@@ -789,31 +817,35 @@ struct EdgeState {
   double h, u, v;
 };
 
-__device__ __forceinline__ EdgeState edge_state(const Dev& d, const double* __restrict__ hs, int x, int m) {
+template <class R>
+__device__ __forceinline__ EdgeState edge_state(const Dev& d, const Geo<R>& G, const double* __restrict__ hs, int x,
+                                                int m) {
   const size_t q = (size_t)m * d.T + x;
-  const double rx = d.rc_x[q], ry = d.rc_y[q];
+  const R rx = G.rc_x[q], ry = G.rc_y[q];
   EdgeState s;
-  s.h = hs[x] + d.delh_x[x] * rx + d.delh_y[x] * ry;
+  s.h = recon(hs[x], G.delh_x[x], rx, G.delh_y[x], ry);
   if (s.h < kZero) s.h = kZero;
-  s.u = d.u_b[x] + d.delu_x[x] * rx + d.delu_y[x] * ry;
-  s.v = d.v_b[x] + d.delv_x[x] * rx + d.delv_y[x] * ry;
+  s.u = recon(d.u_b[x], G.delu_x[x], rx, G.delu_y[x], ry);
+  s.v = recon(d.v_b[x], G.delv_x[x], rx, G.delv_y[x], ry);
   return s;
 }
 
 // invisc_fluxes.f90:39-147 for the interior edge between L=e(1) (slot ml) and
-// R=e(2) (slot mr); returns false when the edge is skipped.
-__device__ __forceinline__ bool interior_flux(const Dev& d, const double* __restrict__ hs,
-                                              const uint8_t* __restrict__ dry, int L, int ml, int R, int mr,
-                                              double nx, double ny, double z0e, double* f, bool* bad) {
-  const bool dl = dry[L], dr = dry[R];
+// R=e(2) (slot mr); returns false when the edge is skipped.  The wet/dry tests and
+// the I1 stage comparison run on the FP64 face states; the flux function in R.
+template <class R>
+__device__ __forceinline__ bool interior_flux(const Dev& d, const Geo<R>& G, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, int L, int ml, int Rc, int mr, R nx,
+                                              R ny, double z0e, R* f, bool* bad) {
+  const bool dl = dry[L], dr = dry[Rc];
   if (dl && dr) return false;
   double hleft = kZero, uleft = kZero, vleft = kZero, hright = kZero, uright = kZero, vright = kZero;
   if (!dl) {
-    EdgeState s = edge_state(d, hs, L, ml);
+    EdgeState s = edge_state(d, G, hs, L, ml);
     hleft = s.h; uleft = s.u; vleft = s.v;
   }
   if (!dr) {
-    EdgeState s = edge_state(d, hs, R, mr);
+    EdgeState s = edge_state(d, G, hs, Rc, mr);
     hright = s.h; uright = s.u; vright = s.v;
   }
   if (hleft < d.h_dry && hright < d.h_dry) return false;
@@ -824,21 +856,21 @@ __device__ __forceinline__ bool interior_flux(const Dev& d, const double* __rest
     if (dl)
       if (d.z[L] + d.h_wet > h0) { set_wall = true; hleft = hright; }
     if (dr)
-      if (d.z[R] + d.h_wet > h0) { set_wall = true; hright = hleft; }
+      if (d.z[Rc] + d.h_wet > h0) { set_wall = true; hright = hleft; }
   }
   if (set_wall) {
-    f[0] = kZero;
-    hleft = fmax2(hleft, hright);
-    f[1] = kHalf * kG * hleft * hleft * nx;
-    f[2] = kHalf * kG * hleft * hleft * ny;
+    f[0] = R(kZero);
+    const R hw = (R)fmax2(hleft, hright);
+    f[1] = R(kHalf) * R(kG) * hw * hw * nx;
+    f[2] = R(kHalf) * R(kG) * hw * hw * ny;
   } else if (d.flux == STORM_FLUX_HLL) {
-    flux_hll(nx, ny, hleft, uleft, vleft, hright, uright, vright, d.h_dry, f, bad);
+    flux_hll<R>(nx, ny, (R)hleft, (R)uleft, (R)vleft, (R)hright, (R)uright, (R)vright, (R)d.h_dry, f, bad);
   } else if (d.flux == STORM_FLUX_RUSANOV) {
-    const double cl = dl ? kZero : sqrt(kG * hs[L]);  // wavec (solverFVT.f90:180-181)
-    const double cr = dr ? kZero : sqrt(kG * hs[R]);
-    flux_rusanov(nx, ny, hleft, uleft, vleft, cl, hright, uright, vright, cr, f);
+    const R cl = dl ? R(kZero) : (R)sqrt(kG * hs[L]);  // wavec (solverFVT.f90:180-181)
+    const R cr = dr ? R(kZero) : (R)sqrt(kG * hs[Rc]);
+    flux_rusanov<R>(nx, ny, (R)hleft, (R)uleft, (R)vleft, cl, (R)hright, (R)uright, (R)vright, cr, f);
   } else {
-    flux_roe(nx, ny, hleft, uleft, vleft, hright, uright, vright, f);
+    flux_roe<R>(nx, ny, (R)hleft, (R)uleft, (R)vleft, (R)hright, (R)uright, (R)vright, f);
   }
   return true;
 }
@@ -847,35 +879,111 @@ __device__ __forceinline__ bool interior_flux(const Dev& d, const double* __rest
 // the flux of edge k is evaluated once, in the reference's orientation (left =
 // edges(k)%e(1)), and stored as f*length, the amount the reference subtracts from
 // phi(e(1),:) and adds to phi(e(2),:).
-__global__ void __launch_bounds__(128) k_eflux(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry) {
+template <class R>
+__global__ void __launch_bounds__(128, 8) k_eflux(Dev d, Geo<R> G, const double* __restrict__ hs,
+                                               const uint8_t* __restrict__ dry) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.ne || d.sc->converged) return;
-  const int L = d.eL[e], R = d.eR[e];
+  const int L = d.eL[e], Rc = d.eR[e];
   const uint8_t sl = d.eslot[e];
-  double f[3];
+  R f[3];
   bool bad = false;
-  const bool ok = interior_flux(d, hs, dry, L, sl & 3, R, (sl >> 2) & 3, d.enx[e], d.eny[e],
-                                (dry[L] || dry[R]) ? d.ez0[e] : kZero, f, &bad);
+  const bool ok = interior_flux<R>(d, G, hs, dry, L, sl & 3, Rc, (sl >> 2) & 3, G.enx[e], G.eny[e],
+                                   (dry[L] || dry[Rc]) ? d.ez0[e] : kZero, f, &bad);
   d.eok[e] = ok;
   if (ok) {
-    const double len = d.elen[e];
-    d.efx[e] = f[0] * len;
-    d.efx[d.ne + e] = f[1] * len;
-    d.efx[2 * d.ne + e] = f[2] * len;
+    const R len = G.elen[e];
+    G.efx[e] = f[0] * len;
+    G.efx[d.ne + e] = f[1] * len;
+    G.efx[2 * d.ne + e] = f[2] * len;
   }
   if (bad) atomicOr(&d.sc->status, 2);
 }
 
+// bed_slope_STD.f90:23-70 with adjustZb.f90:41-70: the amounts g*h*gradzb*area that
+// are subtracted from phi(i,2:3).  The adjust test (a negative reconstructed vertex
+// depth) and the adjusted gradient run in double on both paths.
+__device__ __forceinline__ void bed_source(const Dev& d, const Geo<double>& G, int c, double h_c, double* s2,
+                                           double* s3) {
+  const int T = d.T;
+  const double dhx = G.delh_x[c], dhy = G.delh_y[c], xc = d.xc[c], yc = d.yc[c];
+  int vid[3];
+  double hp[3];
+  bool adjust = false;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    vid[i] = d.vert[(size_t)i * T + c];
+    hp[i] = h_c + dhx * (d.node_x[vid[i]] - xc) + dhy * (d.node_y[vid[i]] - yc);
+    if (hp[i] < kZero) adjust = true;
+  }
+  double gx, gy;
+  if (adjust) {
+    double zp[3], x[3], y[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      hp[i] = fmin2(kZero, hp[i]);
+      zp[i] = d.zvtx[vid[i]] + hp[i];
+      x[i] = d.node_x[vid[i]];
+      y[i] = d.node_y[vid[i]];
+    }
+    const double b1 = y[1] - y[2], c1 = x[2] - x[1];
+    const double b2 = y[2] - y[0], c2 = x[0] - x[2];
+    const double b3 = y[0] - y[1], c3 = x[1] - x[0];
+    const double a = kHalf / d.area[c];
+    gx = a * (b1 * zp[0] + b2 * zp[1] + b3 * zp[2]);
+    gy = a * (c1 * zp[0] + c2 * zp[1] + c3 * zp[2]);
+  } else {
+    gx = G.delz_x[c];
+    gy = G.delz_y[c];
+  }
+  *s2 = kG * h_c * gx * d.area[c];
+  *s3 = kG * h_c * gy * d.area[c];
+}
+__device__ __forceinline__ void bed_source(const Dev& d, const Geo<float>& G, int c, double h_c, double* s2,
+                                           double* s3) {
+  const int T = d.T;
+  const float dhx = G.delh_x[c], dhy = G.delh_y[c];
+  const double xc = d.xc[c], yc = d.yc[c];
+  int vid[3];
+  double hp[3];
+  bool adjust = false;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    vid[i] = d.vert[(size_t)i * T + c];
+    hp[i] = h_c + (double)(dhx * (float)(d.node_x[vid[i]] - xc) + dhy * (float)(d.node_y[vid[i]] - yc));
+    if (hp[i] < kZero) adjust = true;
+  }
+  if (adjust) {
+    double zp[3], x[3], y[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      zp[i] = d.zvtx[vid[i]] + fmin2(kZero, hp[i]);
+      x[i] = d.node_x[vid[i]];
+      y[i] = d.node_y[vid[i]];
+    }
+    const double a = kHalf / d.area[c];
+    const double gx = a * ((y[1] - y[2]) * zp[0] + (y[2] - y[0]) * zp[1] + (y[0] - y[1]) * zp[2]);
+    const double gy = a * ((x[2] - x[1]) * zp[0] + (x[0] - x[2]) * zp[1] + (x[1] - x[0]) * zp[2]);
+    *s2 = kG * h_c * gx * d.area[c];
+    *s3 = kG * h_c * gy * d.area[c];
+  } else {
+    const float ga = 9.81f * (float)h_c * (float)d.area[c];
+    *s2 = (double)(ga * G.delz_x[c]);
+    *s3 = (double)(ga * G.delz_y[c]);
+  }
+}
+
 // Fluxes, sources and the RK update of stage s (1-based) for cell c: the faces are
 // added to phi in the order invisc_fluxes.f90 visits them (phi = zero first,
-// solverFVT.f90:194), then the bed slope, then the RK update.
-__device__ __forceinline__ void flux_cell(const Dev& d, int s, int c, const double* __restrict__ hs,
+// solverFVT.f90:194), then the bed slope, then the RK update.  phi and the RK
+// combination are FP64 on both paths.
+template <class R>
+__device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, int c, const double* __restrict__ hs,
                                           const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
   const int T = d.T;
   const bool dry_c = dry[c];
   const double h_c = hs[c];
-  double p1 = kZero, p2 = kZero, p3 = kZero;  // phi = zero (solverFVT.f90:194)
-  bool bad = false;
+  double p1 = kZero, p2 = kZero, p3 = kZero;
   const uint8_t ord = d.forder[c];
 #pragma unroll 1
   for (int t = 0; t < 3; t++) {
@@ -886,7 +994,7 @@ __device__ __forceinline__ void flux_cell(const Dev& d, int s, int c, const doub
     if (kind == FACE_LEFT || kind == FACE_RIGHT) {
       const int e = d.fref[q];  // flux*length of the edge, evaluated once by k_eflux
       if (d.eok[e]) {
-        const double f0 = d.efx[e], f1 = d.efx[d.ne + e], f2 = d.efx[2 * d.ne + e];
+        const double f0 = G.efx[e], f1 = G.efx[d.ne + e], f2 = G.efx[2 * d.ne + e];
         if (kind == FACE_LEFT) {
           p1 = p1 - f0;
           p2 = p2 - f1;
@@ -910,11 +1018,10 @@ __device__ __forceinline__ void flux_cell(const Dev& d, int s, int c, const doub
         p3 = p3 - kHalf * kG * hedge * hedge * ny * len;
       } else {  // weslp2_fluxes.f90:34-76
         const size_t qc = (size_t)j * T + c;
-        const double rx = d.rc_x[qc], ry = d.rc_y[qc];
-        const double hleft = h_c + d.delh_x[c] * rx + d.delh_y[c] * ry;
+        const double hleft = recon(h_c, G.delh_x[c], G.rc_x[qc], G.delh_y[c], G.rc_y[qc]);
         if (hleft < d.h_dry) continue;
-        const double uleft = d.u_b[c] + d.delu_x[c] * rx + d.delu_y[c] * ry;
-        const double vleft = d.v_b[c] + d.delv_x[c] * rx + d.delv_y[c] * ry;
+        const double uleft = recon(d.u_b[c], G.delu_x[c], G.rc_x[qc], G.delu_y[c], G.rc_y[qc]);
+        const double vleft = recon(d.v_b[c], G.delv_x[c], G.rc_x[qc], G.delv_y[c], G.rc_y[qc]);
         const double tx = -ny, ty = nx;  // edges%tang flipped with the normal
         double uright = uleft * tx + vleft * ty;
         uright = uright + 2.0 * sqrt(kG * hleft);
@@ -932,40 +1039,11 @@ __device__ __forceinline__ void flux_cell(const Dev& d, int s, int c, const doub
       p3 = p3 - d.bc_c[2 * d.nbce + e];
     }
   }
-  // bed_slope_STD.f90:23-70 with adjustZb.f90:41-70
   if (!dry_c) {
-    const double dhx = d.delh_x[c], dhy = d.delh_y[c], xc = d.xc[c], yc = d.yc[c];
-    int vid[3];
-    double hp[3];
-    bool adjust = false;
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-      vid[i] = d.vert[(size_t)i * T + c];
-      hp[i] = h_c + dhx * (d.node_x[vid[i]] - xc) + dhy * (d.node_y[vid[i]] - yc);
-      if (hp[i] < kZero) adjust = true;
-    }
-    double gx, gy;
-    if (adjust) {
-      double zp[3], x[3], y[3];
-#pragma unroll
-      for (int i = 0; i < 3; i++) {
-        hp[i] = fmin2(kZero, hp[i]);
-        zp[i] = d.zvtx[vid[i]] + hp[i];
-        x[i] = d.node_x[vid[i]];
-        y[i] = d.node_y[vid[i]];
-      }
-      const double b1 = y[1] - y[2], c1 = x[2] - x[1];
-      const double b2 = y[2] - y[0], c2 = x[0] - x[2];
-      const double b3 = y[0] - y[1], c3 = x[1] - x[0];
-      const double a = kHalf / d.area[c];
-      gx = a * (b1 * zp[0] + b2 * zp[1] + b3 * zp[2]);
-      gy = a * (c1 * zp[0] + c2 * zp[1] + c3 * zp[2]);
-    } else {
-      gx = d.delz_x[c];
-      gy = d.delz_y[c];
-    }
-    p2 = p2 - kG * h_c * gx * d.area[c];
-    p3 = p3 - kG * h_c * gy * d.area[c];
+    double s2, s3;
+    bed_source(d, G, c, h_c, &s2, &s3);
+    p2 = p2 - s2;
+    p3 = p3 - s3;
   }
   // RK update (solverFVT.f90:259-283)
   const double u_c = d.u_a[c], v_c = d.v_a[c];
@@ -1020,24 +1098,25 @@ __device__ __forceinline__ void flux_cell(const Dev& d, int s, int c, const doub
   } else {
     d.phimax[c] = fmax2(fmax2(fmax2(kZero, fabs(p1)), fabs(p2)), fabs(p3));
   }
-  if (bad) atomicOr(&d.sc->status, 2);
 }
 
 // All cells without an open-boundary face (those wait for k_bc in k_flux_bc).
-__global__ void __launch_bounds__(128) k_flux(Dev d, int s, const double* __restrict__ hs,
+template <class R>
+__global__ void __launch_bounds__(128, 10) k_flux(Dev d, Geo<R> G, int s, const double* __restrict__ hs,
                                               const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.T || d.sc->converged) return;
   if (d.forder[c] & kOrderHasBc) return;
-  flux_cell(d, s, c, hs, dry, dry_next);
+  flux_cell<R>(d, G, s, c, hs, dry, dry_next);
 }
 
 // The cells with an open-boundary face, after k_bc.
-__global__ void __launch_bounds__(128) k_flux_bc(Dev d, int s, const double* __restrict__ hs,
+template <class R>
+__global__ void __launch_bounds__(128) k_flux_bc(Dev d, Geo<R> G, int s, const double* __restrict__ hs,
                                                  const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.nbc_cells || d.sc->converged) return;
-  flux_cell(d, s, d.bc_cells[i], hs, dry, dry_next);
+  flux_cell<R>(d, G, s, d.bc_cells[i], hs, dry, dry_next);
 }
 
 // ---------------------------------------------------------------------------
@@ -1177,6 +1256,39 @@ __global__ void __launch_bounds__(kRedThreads) k_final(Dev d, int nblk) {
       sc->delt = (d.dt_op == 0) ? d.cfl : dtmin;
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers of the templated stage kernels (api.cu is not templated).
+template <class R>
+static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) {
+  switch (L.which) {
+    case STAGE_GRAD:
+      k_grad<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev);
+      break;
+    case STAGE_BC:
+      k_bc<R><<<L.grid, L.block, L.smem, L.stream>>>(d, G, L.hs, L.dry);
+      break;
+    case STAGE_EFLUX:
+      k_eflux<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry);
+      break;
+    case STAGE_FLUX:
+      k_flux<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.s, L.hs, L.dry, L.dry_next);
+      break;
+    case STAGE_FLUX_BC:
+      k_flux_bc<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.s, L.hs, L.dry, L.dry_next);
+      break;
+  }
+}
+
+void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed) {
+  if (mixed) launch_stage_t<float>(L, d, Gf);
+  else launch_stage_t<double>(L, d, Gd);
+}
+
+void set_bc_smem_limit(int bytes) {
+  cudaFuncSetAttribute(k_bc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_bc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 }  // namespace storm

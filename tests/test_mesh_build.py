@@ -97,7 +97,7 @@ def test_option_checks_run_before_device_use(storm_lib):
     pm = fvt.build_mesh(sc.problem)
     for kw, code in [({"rkorder": 4}, abi.STORM_ERR_ARG), ({"opt_limiter": 3}, abi.STORM_ERR_ARG),
                      ({"opt_friction": 5}, abi.STORM_ERR_UNSUPPORTED), ({"flux": 7}, abi.STORM_ERR_ARG),
-                     ({"precision": abi.PREC_MIXED}, abi.STORM_ERR_UNSUPPORTED)]:
+                     ({"precision": 7}, abi.STORM_ERR_ARG)]:
         with pytest.raises(fvt.StormError) as e:
             fvt.Solver(pm, fvt.default_options(**kw))
         assert e.value.code == code, kw
