@@ -247,6 +247,25 @@ STORM_FVT_API void storm_fvt_mesh_free(StormFvtMesh* mesh);
 STORM_FVT_API int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt,
                      StormFvtHandle** out);
 
+/*
+ * Batched solver: `n` independent scenarios (meshes of any sizes, same options,
+ * each with its own boundary values) advance together, one launch per kernel for
+ * all of them (the step graph covers every scenario).  Each scenario keeps its own
+ * dt, clocks, stop test and statistics; a converged scenario is skipped by every
+ * kernel.  No counterpart in the reference (it runs one mesh per process).
+ */
+STORM_FVT_API int storm_fvt_create_batch(const StormFvtMesh* const* meshes, int32_t n,
+                                         const StormFvtOptions* opt, StormFvtHandle** out);
+STORM_FVT_API int32_t storm_fvt_num_scenarios(const StormFvtHandle* hd);
+STORM_FVT_API int storm_fvt_set_scenario_state(StormFvtHandle* hd, int32_t scenario, const double* h,
+                                               const double* u, const double* v);
+STORM_FVT_API int storm_fvt_get_scenario_state(StormFvtHandle* hd, int32_t scenario, double* h, double* u,
+                                               double* v, double* rkh, double* rku, double* rkv,
+                                               double* hvtx);
+/* Statistics of one scenario after the last storm_fvt_step call. */
+STORM_FVT_API int storm_fvt_scenario_stats(const StormFvtHandle* hd, int32_t scenario,
+                                           StormFvtStepStats* stats);
+
 /* Set the cell state h, u, v [n_elems] (dep_vars.f90 arrays, element order) and
  * reset the iteration counters; rk*(:,rkorder) = h, h*u, h*v (solverFVT.f90:122-126). */
 STORM_FVT_API int storm_fvt_set_state(StormFvtHandle* hd, const double* h, const double* u,
@@ -254,8 +273,10 @@ STORM_FVT_API int storm_fvt_set_state(StormFvtHandle* hd, const double* h, const
 
 /*
  * Advance up to `nsteps` iterations of the main loop (solverFVT.f90:129-478).  In
- * steady mode the loop stops early once rmax < rstop, like the EXIT at :431.
- * `stats` (may be NULL) receives the scalars after the last iteration done.
+ * steady mode the loop stops early once rmax < rstop, like the EXIT at :431 (for a
+ * batch: once every scenario has stopped).  `stats` (may be NULL) receives the
+ * scalars after the last iteration done (scenario 0 of a batch).
+ * storm_fvt_set_state / get_state / get_drycell address single-scenario handles.
  */
 STORM_FVT_API int storm_fvt_step(StormFvtHandle* hd, int32_t nsteps, StormFvtStepStats* stats);
 

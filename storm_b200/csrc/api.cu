@@ -19,11 +19,11 @@
 
 namespace storm {
 
-__global__ void k_init(Dev d);
-__global__ void k_init_final(Dev d, int nblk);
+__global__ void k_init(Dev d, int c0);
+__global__ void k_init_final(Dev d, int sid);
 __global__ void k_node(Dev d, const double* hs, const uint8_t* dry);
 __global__ void k_fric(Dev d);
-__global__ void k_final(Dev d, int nblk);
+__global__ void k_final(Dev d);
 
 static thread_local std::string g_err;
 
@@ -39,7 +39,11 @@ using namespace storm;
 
 struct StormFvtHandle {
   StormFvtOptions opt{};
-  HostLayout L;
+  std::vector<HostLayout> parts;  // per-scenario layouts (permutations for state I/O)
+  std::vector<ScenarioInfo> info; // placement of each scenario in the merged arrays
+  HostLayout L;                   // merged layout that is on the device
+  int nscen = 1;
+  std::vector<uint8_t> have_scen_state;
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;       // boundary kernel, overlapped with k_flux
@@ -50,7 +54,7 @@ struct StormFvtHandle {
   Geo<double> gd{};  // FP64 views
   Geo<float> gf{};   // FP32 copies (mixed precision)
   bool mixed = false;
-  Scalars* sc_host = nullptr;  // pinned
+  Scalars* sc_host = nullptr;  // pinned, [nscen]
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int kernels_per_step = 0;
@@ -194,7 +198,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
   if (mark(KT_FRIC)) return STORM_ERR_CUDA;
   k_fric<<<d.nblk_red, kRed, 0, h->stream>>>(d);
   if (done() || mark(KT_FINAL)) return STORM_ERR_CUDA;
-  k_final<<<1, kRed, 0, h->stream>>>(d, d.nblk_red);
+  k_final<<<d.nscen, kRed, 0, h->stream>>>(d);
   if (done()) return STORM_ERR_CUDA;
   CK(cudaGetLastError());
   return 0;
@@ -246,7 +250,6 @@ int upload(StormFvtHandle* h) {
   const int nblk = (T + kRed - 1) / kRed;
   const size_t nbce = std::max(L.nbce, 1), nbdr = std::max(L.nbdr, 1), nwall = std::max(L.nwall, 1);
   const size_t nnz = std::max(L.n2t_nnz, 1), nts = std::max<size_t>(L.ts_t.size(), 1);
-  const size_t nio = std::max(L.n_in + L.n_out, 1);
   Arena A;
   struct Up {
     size_t off;
@@ -277,8 +280,9 @@ int upload(StormFvtHandle* h) {
   size_t o_bcn = cpy(L.bdr_cnt, nbdr), o_bcc = cpy(L.bce_cell, nbce), o_bcs = cpy(L.bce_slot, nbce);
   size_t o_bnx = cpy(L.bce_nx, nbce), o_bny = cpy(L.bce_ny, nbce), o_btx = cpy(L.bce_tx, nbce);
   size_t o_bty = cpy(L.bce_ty, nbce), o_bl = cpy(L.bce_len, nbce), o_bz = cpy(L.bce_zmid, nbce);
-  size_t o_tso = cpy(L.ts_off, nio), o_tsc = cpy(L.ts_cnt, nio), o_ot = cpy(L.out_type, nio);
   size_t o_tst = cpy(L.ts_t, nts), o_tsv = cpy(L.ts_v, nts);
+  size_t o_csid = cpy(L.cell_sid, T), o_nsid = cpy(L.node_sid, N);
+  size_t o_esid = cpy(L.edge_sid, std::max(L.ne, 1)), o_bsid = cpy(L.bdr_sid, nbdr);
   size_t o_bcl = cpy(L.bc_cells, std::max<size_t>(L.bc_cells.size(), 1));
   const size_t ne1 = std::max(L.ne, 1);
   size_t o_eL = cpy(L.eL, ne1), o_eR = cpy(L.eR, ne1), o_es = cpy(L.eslot, ne1);
@@ -292,7 +296,7 @@ int upload(StormFvtHandle* h) {
   for (int i = 0; i < 6; i++) o_g[i] = A.take(8 * (size_t)T);
   size_t o_dra = A.take(T), o_drb = A.take(T), o_hv = A.take(8 * (size_t)N), o_vw = A.take(N);
   size_t o_pm = A.take(8 * (size_t)T), o_bcc3 = A.take(8 * 3 * nbce), o_rec = A.take(8 * 3 * nbce);
-  size_t o_part = A.take(8 * 8 * (size_t)nblk), o_sc = A.take(sizeof(Scalars));
+  size_t o_part = A.take(8 * 8 * (size_t)nblk), o_sc = A.take(sizeof(Scalars) * (size_t)h->nscen);
   size_t o_efx = A.take(8 * 3 * ne1), o_eok = A.take(ne1);
   cudaError_t e = cudaMalloc(&h->arena, A.off);
   if (e != cudaSuccess)
@@ -306,9 +310,9 @@ int upload(StormFvtHandle* h) {
   d.T = T; d.N = N; d.K = K; d.kst = L.kst; d.nbdr = L.nbdr; d.nbce = L.nbce;
   d.steady = o.steady != 0; d.dt_op = o.dt_op; d.lim = o.opt_limiter; d.btype = o.btype;
   d.hvalve = o.hvalve != 0; d.vclip = o.vclip != 0; d.fric = o.opt_friction; d.stop_cr = o.stop_cr;
-  d.flux = o.flux; d.last_cell = L.last_cell_new; d.n_in = L.n_in; d.n_out = L.n_out;
+  d.flux = o.flux;
   d.h_dry = o.h_dry; d.h_wet = o.h_wet; d.cfl = o.cfl; d.vceiling = o.vceiling; d.visc = o.visc;
-  d.rstop = o.rstop; d.bch_max = L.bch_max;
+  d.rstop = o.rstop;
   // RK tables, dataprepFVT.f90:256-273
   std::memset(d.alpha, 0, sizeof d.alpha);
   std::memset(d.beta, 0, sizeof d.beta);
@@ -340,8 +344,10 @@ int upload(StormFvtHandle* h) {
   d.bdr_cnt = at<int32_t>(B, o_bcn); d.bce_cell = at<int32_t>(B, o_bcc); d.bce_slot = at<int32_t>(B, o_bcs);
   d.bce_nx = at<double>(B, o_bnx); d.bce_ny = at<double>(B, o_bny); d.bce_tx = at<double>(B, o_btx);
   d.bce_ty = at<double>(B, o_bty); d.bce_len = at<double>(B, o_bl); d.bce_zmid = at<double>(B, o_bz);
-  d.ts_off = at<int32_t>(B, o_tso); d.ts_cnt = at<int32_t>(B, o_tsc); d.out_type = at<int32_t>(B, o_ot);
   d.ts_t = at<double>(B, o_tst); d.ts_v = at<double>(B, o_tsv);
+  d.cell_sid = at<int32_t>(B, o_csid); d.node_sid = at<int32_t>(B, o_nsid);
+  d.edge_sid = at<int32_t>(B, o_esid); d.bdr_sid = at<int32_t>(B, o_bsid);
+  d.nscen = h->nscen;
   d.rkh = at<double>(B, o_rkh); d.rku = at<double>(B, o_rku); d.rkv = at<double>(B, o_rkv);
   d.u_a = at<double>(B, o_ua); d.v_a = at<double>(B, o_va); d.u_b = at<double>(B, o_ub); d.v_b = at<double>(B, o_vb);
   d.delh_x = at<double>(B, o_g[0]); d.delh_y = at<double>(B, o_g[1]); d.delu_x = at<double>(B, o_g[2]);
@@ -407,11 +413,36 @@ int upload(StormFvtHandle* h) {
     }
   }
   d.bc_cells = at<int32_t>(B, o_bcl);
-  // boundary values
-  Scalars s0{};
-  for (int b = 0; b < L.n_in; b++) s0.qin[b] = L.qin[b];
-  for (int b = 0; b < L.n_out; b++) s0.hbc[b] = L.hbc[b];
-  CK(cudaMemcpy(d.sc, &s0, sizeof s0, cudaMemcpyHostToDevice));
+  // per-scenario scalars: boundary values, series offsets, ranges
+  std::vector<Scalars> s0(h->nscen);
+  int32_t ts_base = 0;
+  for (int sI = 0; sI < h->nscen; sI++) {
+    const HostLayout& P = h->parts[sI];
+    const ScenarioInfo& I = h->info[sI];
+    Scalars& x = s0[sI];
+    std::memset(&x, 0, sizeof x);
+    x.n_in = P.n_in;
+    x.n_out = P.n_out;
+    for (int b = 0; b < P.n_in; b++) x.qin[b] = P.qin[b];
+    for (int b = 0; b < P.n_out; b++) {
+      x.hbc[b] = P.hbc[b];
+      x.out_type[b] = P.out_type[b];
+    }
+    for (int b = 0; b < P.n_in; b++) {
+      x.ts_off[b] = P.ts_off[b] + ts_base;
+      x.ts_cnt[b] = P.ts_cnt[b];
+    }
+    for (int b = 0; b < P.n_out; b++) {
+      x.ts_off[kMaxBdrDev + b] = P.ts_off[P.n_in + b] + ts_base;
+      x.ts_cnt[kMaxBdrDev + b] = P.ts_cnt[P.n_in + b];
+    }
+    ts_base += (int32_t)P.ts_t.size();
+    x.bch_max = P.bch_max;
+    x.last_cell = I.last_cell;
+    x.blk_off = I.blk_off;
+    x.blk_cnt = I.blk_cnt;
+  }
+  CK(cudaMemcpy(d.sc, s0.data(), sizeof(Scalars) * s0.size(), cudaMemcpyHostToDevice));
   int maxcnt = 1;
   for (int b = 0; b < L.nbdr; b++) maxcnt = std::max(maxcnt, L.bdr_cnt[b]);
   h->bc_smem = (size_t)maxcnt * 2 * sizeof(double) + (((size_t)maxcnt + 7) & ~(size_t)7);
@@ -454,10 +485,13 @@ void storm_fvt_default_options(StormFvtOptions* o) {
   o->device = 0;
 }
 
-int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, StormFvtHandle** out) {
+int storm_fvt_create_batch(const StormFvtMesh* const* meshes, int32_t n, const StormFvtOptions* opt,
+                           StormFvtHandle** out) {
   clear_error();
-  if (!mesh || !opt || !out) return set_error(STORM_ERR_ARG, "storm_fvt_create: null argument");
+  if (!meshes || !opt || !out || n < 1) return set_error(STORM_ERR_ARG, "storm_fvt_create: null argument or n < 1");
   *out = nullptr;
+  for (int32_t i = 0; i < n; i++)
+    if (!meshes[i]) return set_error(STORM_ERR_ARG, "storm_fvt_create: null mesh");
   int rc = check_options(*opt);
   if (rc) return rc;
   StormFvtHandle* h = new (std::nothrow) StormFvtHandle();
@@ -465,8 +499,11 @@ int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, Storm
   h->opt = *opt;
   h->device = opt->device;
   h->mixed = opt->precision == STORM_PREC_MIXED;
+  h->nscen = n;
   try {
-    rc = build_layout(*mesh, *opt, h->L);
+    h->parts.resize(n);
+    for (int32_t i = 0; i < n && !rc; i++) rc = build_layout(*meshes[i], *opt, h->parts[i]);
+    if (!rc) merge_layouts(h->parts, kRed, h->L, h->info);
   } catch (const std::bad_alloc&) {
     rc = set_error(STORM_ERR_NOMEM, "storm_fvt_create: host out of memory");
   }
@@ -474,6 +511,7 @@ int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, Storm
     delete h;
     return rc;
   }
+  h->have_scen_state.assign(n, 0);
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) {
@@ -493,7 +531,7 @@ int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, Storm
   }
   if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
-  if (e == cudaSuccess) e = cudaMallocHost(&h->sc_host, sizeof(Scalars));
+  if (e == cudaSuccess) e = cudaMallocHost(&h->sc_host, sizeof(Scalars) * (size_t)n);
   if (e != cudaSuccess) {
     release(h);
     return set_error(STORM_ERR_CUDA, std::string("storm_fvt_create: ") + cudaGetErrorString(e));
@@ -507,30 +545,64 @@ int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, Storm
   return STORM_OK;
 }
 
-int storm_fvt_set_state(StormFvtHandle* h, const double* hh, const double* u, const double* v) {
+int storm_fvt_create(const StormFvtMesh* mesh, const StormFvtOptions* opt, StormFvtHandle** out) {
+  return storm_fvt_create_batch(&mesh, 1, opt, out);
+}
+
+int32_t storm_fvt_num_scenarios(const StormFvtHandle* h) { return h ? h->nscen : 0; }
+
+int storm_fvt_set_scenario_state(StormFvtHandle* h, int32_t sid, const double* hh, const double* u, const double* v) {
   clear_error();
   if (!h || !hh || !u || !v) return set_error(STORM_ERR_ARG, "storm_fvt_set_state: null argument");
+  if (sid < 0 || sid >= h->nscen) return set_error(STORM_ERR_ARG, "storm_fvt_set_state: scenario out of range");
   CK(cudaSetDevice(h->device));
-  const int T = h->L.T;
-  std::vector<double> buf(3 * (size_t)T);
-  for (int c = 0; c < T; c++) {
-    int o = h->L.cell_old[c];
+  const HostLayout& P = h->parts[sid];
+  const ScenarioInfo& I = h->info[sid];
+  const int Ts = P.T;
+  std::vector<double> buf(3 * (size_t)Ts);
+  for (int c = 0; c < Ts; c++) {
+    int o = P.cell_old[c];
     buf[c] = hh[o];
-    buf[T + c] = u[o];
-    buf[2 * (size_t)T + c] = v[o];
+    buf[Ts + c] = u[o];
+    buf[2 * (size_t)Ts + c] = v[o];
   }
   const Dev& d = h->d;
-  CK(cudaMemcpyAsync(d.rkh, buf.data(), 8 * (size_t)T, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(d.u_a, buf.data() + T, 8 * (size_t)T, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(d.v_a, buf.data() + 2 * (size_t)T, 8 * (size_t)T, cudaMemcpyHostToDevice, h->stream));
-  const int nblk = (T + kRed - 1) / kRed;
-  k_init<<<nblk, kRed, 0, h->stream>>>(d);
-  k_init_final<<<1, kRed, 0, h->stream>>>(d, nblk);
+  CK(cudaMemcpyAsync(d.rkh + I.cell_off, buf.data(), 8 * (size_t)Ts, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(d.u_a + I.cell_off, buf.data() + Ts, 8 * (size_t)Ts, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(d.v_a + I.cell_off, buf.data() + 2 * (size_t)Ts, 8 * (size_t)Ts, cudaMemcpyHostToDevice,
+                     h->stream));
+  k_init<<<I.blk_cnt, kRed, 0, h->stream>>>(d, I.cell_off);
+  k_init_final<<<1, kRed, 0, h->stream>>>(d, sid);
   CK(cudaGetLastError());
   h->launches += 2;
   CK(cudaStreamSynchronize(h->stream));
+  h->have_scen_state[sid] = 1;
   h->have_state = true;
+  for (uint8_t f : h->have_scen_state) h->have_state = h->have_state && f;
   return STORM_OK;
+}
+
+int storm_fvt_set_state(StormFvtHandle* h, const double* hh, const double* u, const double* v) {
+  if (h && h->nscen != 1)
+    return set_error(STORM_ERR_ARG, "storm_fvt_set_state: batched handle, use storm_fvt_set_scenario_state");
+  return storm_fvt_set_scenario_state(h, 0, hh, u, v);
+}
+
+static void fill_stats(const StormFvtHandle* h, const Scalars& s, StormFvtStepStats* stats) {
+  std::memset(stats, 0, sizeof *stats);
+  stats->iter = s.iter;
+  stats->converged = s.converged;
+  stats->ttime = s.ttime;
+  stats->stime = s.stime;
+  stats->delt = h->opt.steady ? s.delt_fric : s.delt;
+  stats->rmax = s.rmax;
+  stats->rms_dh = s.rms;
+  stats->tmass = s.tmass;
+  for (int b = 0; b < STORM_MAX_BDR; b++) {
+    stats->cqin3[b] = s.cqin3[b];
+    stats->cqout3[b] = s.cqout3[b];
+  }
+  stats->device_status = s.status;
 }
 
 int storm_fvt_step(StormFvtHandle* h, int32_t nsteps, StormFvtStepStats* stats) {
@@ -539,8 +611,8 @@ int storm_fvt_step(StormFvtHandle* h, int32_t nsteps, StormFvtStepStats* stats) 
   if (!h->have_state) return set_error(STORM_ERR_ARG, "storm_fvt_step: state not set");
   if (nsteps < 0) return set_error(STORM_ERR_ARG, "storm_fvt_step: negative step count");
   CK(cudaSetDevice(h->device));
-  const int K = h->opt.rkorder;
   const int poll = h->opt.steady ? 16 : (1 << 30);
+  const size_t scb = sizeof(Scalars) * (size_t)h->nscen;
   h->last_flux_ms = 0.0;
   h->last_flux_launches = 0;
   CK(cudaEventRecord(h->ev0, h->stream));
@@ -578,47 +650,45 @@ int storm_fvt_step(StormFvtHandle* h, int32_t nsteps, StormFvtStepStats* stats) 
       CK(cudaGraphLaunch(h->exec, h->stream));
       h->launches += h->kernels_per_step;
       if ((i + 1) % poll == 0 && i + 1 < nsteps) {
-        CK(cudaMemcpyAsync(h->sc_host, h->d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(h->sc_host, h->d.sc, scb, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        if (h->sc_host->converged) break;
+        bool all = true;
+        for (int sI = 0; sI < h->nscen; sI++) all = all && h->sc_host[sI].converged;
+        if (all) break;
       }
     }
     CK(cudaEventRecord(h->ev1, h->stream));
   }
-  CK(cudaMemcpyAsync(h->sc_host, h->d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(h->sc_host, h->d.sc, scb, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->last_step_ms = ms;
-  const Scalars& s = *h->sc_host;
-  if (stats) {
-    std::memset(stats, 0, sizeof *stats);
-    stats->iter = s.iter;
-    stats->converged = s.converged;
-    stats->ttime = s.ttime;
-    stats->stime = s.stime;
-    stats->delt = h->opt.steady ? s.delt_fric : s.delt;
-    stats->rmax = s.rmax;
-    stats->rms_dh = s.rms;
-    stats->tmass = s.tmass;
-    for (int b = 0; b < STORM_MAX_BDR; b++) {
-      stats->cqin3[b] = s.cqin3[b];
-      stats->cqout3[b] = s.cqout3[b];
-    }
-    stats->device_status = s.status;
-  }
-  if (s.status & 1)
-    return set_error(STORM_ERR_DEVICE, "storm_fvt_step: non-finite depth or velocity in the state");
+  if (stats) fill_stats(h, h->sc_host[0], stats);
+  for (int sI = 0; sI < h->nscen; sI++)
+    if (h->sc_host[sI].status & 1)
+      return set_error(STORM_ERR_DEVICE, "storm_fvt_step: non-finite depth or velocity in scenario " +
+                                             std::to_string(sI));
   return STORM_OK;
 }
 
-int storm_fvt_get_state(StormFvtHandle* h, double* hh, double* u, double* v, double* rkh, double* rku, double* rkv,
-                        double* hvtx) {
+int storm_fvt_scenario_stats(const StormFvtHandle* h, int32_t sid, StormFvtStepStats* stats) {
+  if (!h || !stats) return set_error(STORM_ERR_ARG, "storm_fvt_scenario_stats: null argument");
+  if (sid < 0 || sid >= h->nscen) return set_error(STORM_ERR_ARG, "storm_fvt_scenario_stats: scenario out of range");
+  fill_stats(h, h->sc_host[sid], stats);
+  return STORM_OK;
+}
+
+int storm_fvt_get_scenario_state(StormFvtHandle* h, int32_t sid, double* hh, double* u, double* v, double* rkh,
+                                 double* rku, double* rkv, double* hvtx) {
   clear_error();
   if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_get_state: null handle");
+  if (sid < 0 || sid >= h->nscen) return set_error(STORM_ERR_ARG, "storm_fvt_get_state: scenario out of range");
   CK(cudaSetDevice(h->device));
-  const int T = h->L.T, N = h->L.N;
-  std::vector<double> buf(std::max(T, N));
+  const HostLayout& P = h->parts[sid];
+  const ScenarioInfo& I = h->info[sid];
+  const int Ts = P.T, Ns = P.N;
+  std::vector<double> buf(std::max(Ts, Ns));
   auto pull = [&](const double* dev, double* dst, int n, const std::vector<int32_t>& perm) -> int {
     if (!dst) return 0;
     CK(cudaMemcpyAsync(buf.data(), dev, 8 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
@@ -627,26 +697,36 @@ int storm_fvt_get_state(StormFvtHandle* h, double* hh, double* u, double* v, dou
     return 0;
   };
   const Dev& d = h->d;
+  const int co = I.cell_off, no = I.node_off;
   int rc;
-  if ((rc = pull(d.rkh, hh, T, h->L.cell_old))) return rc;
-  if ((rc = pull(d.u_a, u, T, h->L.cell_old))) return rc;
-  if ((rc = pull(d.v_a, v, T, h->L.cell_old))) return rc;
-  if ((rc = pull(d.rkh, rkh, T, h->L.cell_old))) return rc;
-  if ((rc = pull(d.rku, rku, T, h->L.cell_old))) return rc;
-  if ((rc = pull(d.rkv, rkv, T, h->L.cell_old))) return rc;
-  if ((rc = pull(d.hvtx, hvtx, N, h->L.node_old))) return rc;
+  if ((rc = pull(d.rkh + co, hh, Ts, P.cell_old))) return rc;
+  if ((rc = pull(d.u_a + co, u, Ts, P.cell_old))) return rc;
+  if ((rc = pull(d.v_a + co, v, Ts, P.cell_old))) return rc;
+  if ((rc = pull(d.rkh + co, rkh, Ts, P.cell_old))) return rc;
+  if ((rc = pull(d.rku + co, rku, Ts, P.cell_old))) return rc;
+  if ((rc = pull(d.rkv + co, rkv, Ts, P.cell_old))) return rc;
+  if ((rc = pull(d.hvtx + no, hvtx, Ns, P.node_old))) return rc;
   return STORM_OK;
+}
+
+int storm_fvt_get_state(StormFvtHandle* h, double* hh, double* u, double* v, double* rkh, double* rku, double* rkv,
+                        double* hvtx) {
+  if (h && h->nscen != 1)
+    return set_error(STORM_ERR_ARG, "storm_fvt_get_state: batched handle, use storm_fvt_get_scenario_state");
+  return storm_fvt_get_scenario_state(h, 0, hh, u, v, rkh, rku, rkv, hvtx);
 }
 
 int storm_fvt_get_drycell(StormFvtHandle* h, int32_t* dry) {
   clear_error();
   if (!h || !dry) return set_error(STORM_ERR_ARG, "storm_fvt_get_drycell: null argument");
+  if (h->nscen != 1) return set_error(STORM_ERR_ARG, "storm_fvt_get_drycell: batched handle");
   CK(cudaSetDevice(h->device));
-  const int T = h->L.T;
-  std::vector<uint8_t> b(T);
-  CK(cudaMemcpyAsync(b.data(), h->d.dry_a, T, cudaMemcpyDeviceToHost, h->stream));
+  const HostLayout& P = h->parts[0];
+  const int Ts = P.T;
+  std::vector<uint8_t> b(Ts);
+  CK(cudaMemcpyAsync(b.data(), h->d.dry_a, Ts, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  for (int c = 0; c < T; c++) dry[h->L.cell_old[c]] = b[c] ? 1 : 0;
+  for (int c = 0; c < Ts; c++) dry[P.cell_old[c]] = b[c] ? 1 : 0;
   return STORM_OK;
 }
 

@@ -15,7 +15,8 @@ namespace storm {
 
 constexpr int kMaxBdrDev = 16;
 
-// Per-handle scalars that live on the device (one struct, written by the kernels).
+// Per-scenario scalars that live on the device (one struct per scenario of the
+// handle, written by the kernels), followed by the scenario's static description.
 struct Scalars {
   int32_t iter;       // iterations completed
   int32_t converged;  // steady: rmax < rstop reached (solverFVT.f90:431)
@@ -27,14 +28,24 @@ struct Scalars {
   double ttime, stime, rmax, rms, tmass;
   double qin[kMaxBdrDev], hbc[kMaxBdrDev];
   double cqin3[kMaxBdrDev], cqout3[kMaxBdrDev];
+  double bch_max;               // dataprepFVT.f90:278-286
+  // static: boundary series and the scenario's ranges in the merged arrays
+  int32_t n_in, n_out;
+  int32_t last_cell;            // merged id of element n_elems (steady friction dt)
+  int32_t blk_off, blk_cnt;     // reduction blocks of the scenario's cell range
+  int32_t pad2;
+  int32_t out_type[kMaxBdrDev];
+  int32_t ts_off[2 * kMaxBdrDev], ts_cnt[2 * kMaxBdrDev];  // inflows, then outflows
 };
 
 // Kernel parameters: options, the device layout and the state buffers.
 struct Dev {
-  int32_t T, N, K, kst, nbdr, nbce;
-  int32_t steady, dt_op, lim, btype, hvalve, vclip, fric, stop_cr, flux, last_cell;
-  int32_t n_in, n_out;
-  double h_dry, h_wet, cfl, vceiling, visc, rstop, bch_max;
+  int32_t T, N, K, kst, nbdr, nbce;  // T counts the padded cell slots of all scenarios
+  int32_t steady, dt_op, lim, btype, hvalve, vclip, fric, stop_cr, flux;
+  int32_t nscen;
+  // scenario of each cell slot (-1: padding), node, interior edge and open boundary
+  const int32_t *cell_sid, *node_sid, *edge_sid, *bdr_sid;
+  double h_dry, h_wet, cfl, vceiling, visc, rstop;
   double alpha[4][4], beta[4];
   // cells
   const double *area, *perim, *xc, *yc, *z, *delz_x, *delz_y, *zmax, *cd;
@@ -57,7 +68,6 @@ struct Dev {
   // open boundaries
   const int32_t *bdr_kind, *bdr_slot, *bdr_off, *bdr_cnt, *bce_cell, *bce_slot;
   const double *bce_nx, *bce_ny, *bce_tx, *bce_ty, *bce_len, *bce_zmid;
-  const int32_t *ts_off, *ts_cnt, *out_type;
   const double *ts_t, *ts_v;
   // state
   double *rkh, *rku, *rkv;  // [K+1][T]
@@ -70,11 +80,11 @@ struct Dev {
   double* phimax;           // MAX(|phi|) of the last stage (stop criterion)
   double* bc_c;             // [3][nbce] boundary contributions to phi
   double* bc_rec;           // [3][nbce] reconstructed boundary-edge h, u, v
-  double* part;             // [nblk][8] reduction partials
+  double* part;             // [nblk][8] reduction partials (blocks never span scenarios)
   int32_t nbc_cells;        // cells with an open-boundary face (finished after k_bc)
   const int32_t* bc_cells;
   int32_t nblk_red;
-  Scalars* sc;
+  Scalars* sc;              // [nscen]
 };
 
 // Geometry and per-stage arrays read or written in the flux/gradient arithmetic type R:

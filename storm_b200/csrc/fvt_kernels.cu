@@ -260,15 +260,15 @@ __device__ __forceinline__ double block_min(double x, double* sm) {
   return r;
 }
 
-// get_time_bcs.f90:31-77 (one thread)
-__device__ void time_bcs(const Dev& d, double time) {
-  Scalars* sc = d.sc;
-  for (int k = 0; k < d.n_out; k++) {
-    if (d.out_type[k] != 1) continue;
-    int n = d.ts_cnt[d.n_in + k];
+// get_time_bcs.f90:31-77 for scenario `sid` (one thread)
+__device__ void time_bcs(const Dev& d, int sid, double time) {
+  Scalars* sc = &d.sc[sid];
+  for (int k = 0; k < sc->n_out; k++) {
+    if (sc->out_type[k] != 1) continue;
+    int n = sc->ts_cnt[kMaxBdrDev + k];
     if (n <= 0) continue;
-    const double* tl = d.ts_t + d.ts_off[d.n_in + k];
-    const double* ts = d.ts_v + d.ts_off[d.n_in + k];
+    const double* tl = d.ts_t + sc->ts_off[kMaxBdrDev + k];
+    const double* ts = d.ts_v + sc->ts_off[kMaxBdrDev + k];
     if (time < tl[0]) sc->hbc[k] = ts[0];
     else if (time >= tl[n - 1]) sc->hbc[k] = ts[n - 1];
     else
@@ -279,11 +279,11 @@ __device__ void time_bcs(const Dev& d, double time) {
           break;
         }
   }
-  for (int k = 0; k < d.n_in; k++) {
-    int n = d.ts_cnt[k];
+  for (int k = 0; k < sc->n_in; k++) {
+    int n = sc->ts_cnt[k];
     if (n <= 0) continue;
-    const double* tl = d.ts_t + d.ts_off[k];
-    const double* ts = d.ts_v + d.ts_off[k];
+    const double* tl = d.ts_t + sc->ts_off[k];
+    const double* ts = d.ts_v + sc->ts_off[k];
     if (time < tl[0]) sc->qin[k] = ts[0];
     else if (time >= tl[n - 1]) sc->qin[k] = ts[n - 1];
     else
@@ -303,11 +303,11 @@ constexpr int kRedThreads = 256;
 // ---------------------------------------------------------------------------
 // Initial state: rk(:,0) = (h, h*u, h*v) (solverFVT.f90:122-126 then :138-142),
 // first-stage dry flags and the CFL dt partials of the initial state.
-__global__ void __launch_bounds__(kRedThreads) k_init(Dev d) {
+__global__ void __launch_bounds__(kRedThreads) k_init(Dev d, int c0) {
   __shared__ double sm[kRedThreads / 32];
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
   double dtc = kVlarge;
-  if (c < d.T) {
+  if (c < d.T && d.cell_sid[c] >= 0) {
     double h = d.rkh[c], u = d.u_a[c], v = d.v_a[c];
     d.rku[c] = h * u;
     d.rkv[c] = h * v;
@@ -319,16 +319,17 @@ __global__ void __launch_bounds__(kRedThreads) k_init(Dev d) {
     dtc = d.cfl * d.area[c] / (dl * d.perim[c]);
   }
   double r = block_min<kRedThreads>(dtc, sm);
-  if (threadIdx.x == 0) d.part[8 * blockIdx.x + 4] = r;
+  if (threadIdx.x == 0) d.part[8 * (c0 / kRedThreads + blockIdx.x) + 4] = r;
 }
 
-__global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int nblk) {
+// One block per listed scenario: initial scalars and the first dt.
+__global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int sid) {
   __shared__ double sm[kRedThreads / 32];
+  Scalars* sc = &d.sc[sid];
   double m = kVlarge;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) m = fmin2(m, d.part[8 * b + 4]);
+  for (int b = threadIdx.x; b < sc->blk_cnt; b += blockDim.x) m = fmin2(m, d.part[8 * (sc->blk_off + b) + 4]);
   double dtmin = block_min<kRedThreads>(m, sm);
   if (threadIdx.x == 0) {
-    Scalars* sc = d.sc;
     sc->iter = 0;
     sc->converged = 0;
     sc->status = 0;
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int nblk) {
       sc->cqin3[b] = kZero;
       sc->cqout3[b] = kZero;
     }
-    time_bcs(d, kZero);
+    time_bcs(d, sid, kZero);
     if (d.steady) sc->delt = kZero;  // delt is first set inside the RK loop
     else sc->delt = (d.dt_op == 0) ? d.cfl : dtmin;
   }
@@ -352,7 +353,9 @@ __global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int nblk) {
 // Vertex water surface and depth of one stage.
 __global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= d.N || d.sc->converged) return;
+  if (n >= d.N) return;
+  const int sid = d.node_sid[n];
+  if (d.sc[sid].converged) return;
   const int b0 = d.n2t_off[n], b1 = d.n2t_off[n + 1];
   const double zv0 = d.zvtx[n];
   double id = kZero, a = kZero, zetaref = zv0;
@@ -373,7 +376,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ 
   if (hv < kZero) hv = kZero;
   d.vwet[n] = hv > d.h_dry;
   const int b = d.node_hbc[n];
-  if (b >= 0) hv = fmax2(kZero, d.sc->hbc[b] - zv0);
+  if (b >= 0) hv = fmax2(kZero, d.sc[sid].hbc[b] - zv0);
   d.hvtx[n] = hv;
 }
 
@@ -423,7 +426,9 @@ __global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* 
                                               const uint8_t* __restrict__ dry, double* __restrict__ rku_prev,
                                               double* __restrict__ rkv_prev) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.T || d.sc->converged) return;
+  if (c >= d.T) return;
+  const int sid = d.cell_sid[c];
+  if (sid < 0 || d.sc[sid].converged) return;
   const int T = d.T;
   const double zeta_c = hs[c] + d.z[c];
   const double u_c = d.u_a[c], v_c = d.v_a[c];
@@ -550,9 +555,10 @@ constexpr int kBcThreads = 128;
 template <class R>
 __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double* __restrict__ hs,
                                                    const uint8_t* __restrict__ dry) {
-  if (d.sc->converged) return;
-  extern __shared__ double smb[];
   const int b = blockIdx.x;
+  Scalars* const sc = &d.sc[d.bdr_sid[b]];
+  if (sc->converged) return;
+  extern __shared__ double smb[];
   const int kind = d.bdr_kind[b], slot = d.bdr_slot[b];
   const int off = d.bdr_off[b], cnt = d.bdr_cnt[b];
   const int T = d.T, NB = d.nbce;
@@ -578,10 +584,10 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
   };
   if (kind == BC_QBYH || kind == BC_QBYH_WET) {  // inflowQbyH.f90:31-212 / :221-402
     const bool wet_only = kind == BC_QBYH_WET;
-    const double qin = d.sc->qin[slot];
+    const double qin = sc->qin[slot];
     if (qin < kVsmall) {
       for (int e = threadIdx.x; e < cnt; e += blockDim.x) put(e, kZero, kZero, kZero);
-      if (threadIdx.x == 0) d.sc->cqin3[slot] = kZero;
+      if (threadIdx.x == 0) sc->cqin3[slot] = kZero;
       return;
     }
     for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
@@ -609,7 +615,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
       for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
         const int i = d.bce_cell[off + e];
         bool valid = !(wet_only && dry[i]);
-        double hleft = null_area ? d.bch_max : d.bc_rec[off + e], uedg, vedg;
+        double hleft = null_area ? sc->bch_max : d.bc_rec[off + e], uedg, vedg;
         if (hleft < h_dry) {
           hleft = fmax2(hleft, kZero);
           uedg = kZero;
@@ -655,7 +661,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
     for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
       const int i = d.bce_cell[off + e];
       bool valid = !(wet_only && dry[i]);
-      double hleft = null_area ? d.bch_max : d.bc_rec[off + e], uedg, vedg;
+      double hleft = null_area ? sc->bch_max : d.bc_rec[off + e], uedg, vedg;
       if (hleft < h_dry) {
         hleft = fmax2(hleft, kZero);
         uedg = kZero;
@@ -690,7 +696,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
       double cq = kZero;
       for (int e = 0; e < cnt; e++)
         if (ok[e]) cq = cq + tA[e];
-      d.sc->cqin3[slot] = cq;
+      sc->cqin3[slot] = cq;
     }
     return;
   }
@@ -710,7 +716,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
       hleft = fmax2(hleft, kZero);
       if (hs[i] < h_dry) { uedg = kZero; vedg = kZero; }
       else { uedg = ur0; vedg = vr0; }
-      const double hright = fmax2(kZero, d.sc->qin[slot] - zmid);
+      const double hright = fmax2(kZero, sc->qin[slot] - zmid);
       double uleft = uedg * nx + vedg * ny;
       const double sl = sqrt(kG * hleft), sr = sqrt(kG * hright);
       double uright = uleft + (sl - sr);
@@ -725,7 +731,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
       double uedg, vedg;
       if (dr || hleft < h_dry) { uedg = kZero; vedg = kZero; hleft = fmax2(hleft, kZero); }
       else { uedg = ur0; vedg = vr0; }
-      double hright = fmax2(kZero, d.sc->hbc[slot] - zmid);
+      double hright = fmax2(kZero, sc->hbc[slot] - zmid);
       if (hleft < h_dry && hright < h_dry) valid = false;
       else {
         double uleft, vleft, uright, vright;
@@ -806,8 +812,8 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
     double cq = kZero;
     for (int e = 0; e < cnt; e++)
       if (ok[e]) cq = cq + tA[e];
-    if (kind == BC_HIN) d.sc->cqin3[slot] = cq;
-    else d.sc->cqout3[slot] = cq;
+    if (kind == BC_HIN) sc->cqin3[slot] = cq;
+    else sc->cqout3[slot] = cq;
   }
 }
 
@@ -883,7 +889,9 @@ template <class R>
 __global__ void __launch_bounds__(128, 8) k_eflux(Dev d, Geo<R> G, const double* __restrict__ hs,
                                                const uint8_t* __restrict__ dry) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= d.ne || d.sc->converged) return;
+  if (e >= d.ne) return;
+  const int sid = d.edge_sid[e];
+  if (d.sc[sid].converged) return;
   const int L = d.eL[e], Rc = d.eR[e];
   const uint8_t sl = d.eslot[e];
   R f[3];
@@ -897,7 +905,7 @@ __global__ void __launch_bounds__(128, 8) k_eflux(Dev d, Geo<R> G, const double*
     G.efx[d.ne + e] = f[1] * len;
     G.efx[2 * d.ne + e] = f[2] * len;
   }
-  if (bad) atomicOr(&d.sc->status, 2);
+  if (bad) atomicOr(&d.sc[sid].status, 2);
 }
 
 // bed_slope_STD.f90:23-70 with adjustZb.f90:41-70: the amounts g*h*gradzb*area that
@@ -1054,9 +1062,9 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
     delt = um + wc;
     if (delt < SMALL_F) delt = 1.044;
     delt = d.cfl * d.area[c] / (delt * d.perim[c]);
-    if (s == d.K && c == d.last_cell) d.sc->delt_fric = delt;
+    if (s == d.K && c == d.sc[d.cell_sid[c]].last_cell) d.sc[d.cell_sid[c]].delt_fric = delt;
   } else {
-    delt = d.sc->delt;
+    delt = d.sc[d.cell_sid[c]].delt;
   }
   const double dt = delt / d.area[c];
   double rh = kZero, ru = kZero, rv = kZero;
@@ -1105,7 +1113,9 @@ template <class R>
 __global__ void __launch_bounds__(128, 10) k_flux(Dev d, Geo<R> G, int s, const double* __restrict__ hs,
                                               const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.T || d.sc->converged) return;
+  if (c >= d.T) return;
+  const int sid = d.cell_sid[c];
+  if (sid < 0 || d.sc[sid].converged) return;
   if (d.forder[c] & kOrderHasBc) return;
   flux_cell<R>(d, G, s, c, hs, dry, dry_next);
 }
@@ -1115,8 +1125,10 @@ template <class R>
 __global__ void __launch_bounds__(128) k_flux_bc(Dev d, Geo<R> G, int s, const double* __restrict__ hs,
                                                  const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.nbc_cells || d.sc->converged) return;
-  flux_cell<R>(d, G, s, d.bc_cells[i], hs, dry, dry_next);
+  if (i >= d.nbc_cells) return;
+  const int c = d.bc_cells[i];
+  if (d.sc[d.cell_sid[c]].converged) return;
+  flux_cell<R>(d, G, s, c, hs, dry, dry_next);
 }
 
 // ---------------------------------------------------------------------------
@@ -1124,11 +1136,13 @@ __global__ void __launch_bounds__(128) k_flux_bc(Dev d, Geo<R> G, int s, const d
 // block partials of the iteration's reductions (solverFVT.f90:335-386, 407-445).
 __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
   __shared__ double sm[kRedThreads / 32];
-  if (d.sc->converged) return;  // uniform over the grid
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int T = d.T, K = d.K;
+  const int sid = c < T ? d.cell_sid[c] : -1;
+  // a block never spans two scenarios, so this test is uniform over the block
+  if (d.sc[d.cell_sid[blockIdx.x * blockDim.x] < 0 ? 0 : d.cell_sid[blockIdx.x * blockDim.x]].converged) return;
   double st = kZero, sb = kZero, tm = kZero, rm = kZero, dtc = kVlarge;
-  if (c < T) {
+  if (sid >= 0) {
     const size_t qk = (size_t)K * T + c;
     const double h = d.rkh[qk];
     double u = d.u_a[c], v = d.v_a[c];
@@ -1166,7 +1180,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
         }
         break;
     }
-    const double dtf = d.steady ? d.sc->delt_fric : d.sc->delt;
+    const double dtf = d.steady ? d.sc[sid].delt_fric : d.sc[sid].delt;
     if (!dry2) rough = h / (h + dtf * rough * um);
     u = u * rough;
     v = v * rough;
@@ -1204,7 +1218,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
     rm = dry2 ? kZero : d.phimax[c];
     const double wc1 = dry1 ? kZero : sqrt(kG * h);
     dtc = d.cfl * d.area[c] / ((um1 + wc1 + SMALL_F) * d.perim[c]);
-    if (!isfinite(h) || !isfinite(u) || !isfinite(v)) atomicOr(&d.sc->status, 1);
+    if (!isfinite(h) || !isfinite(u) || !isfinite(v)) atomicOr(&d.sc[sid].status, 1);
   }
   double* pb = d.part + 8 * blockIdx.x;
   double r0 = block_sum<kRedThreads>(st, sm);
@@ -1219,12 +1233,14 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
   if (threadIdx.x == 0) pb[4] = r4;
 }
 
-__global__ void __launch_bounds__(kRedThreads) k_final(Dev d, int nblk) {
+__global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
   __shared__ double sm[kRedThreads / 32];
-  if (d.sc->converged) return;
+  const int sid = blockIdx.x;
+  Scalars* sc = &d.sc[sid];
+  if (sc->converged) return;
   double a0 = kZero, a1 = kZero, a2 = kZero, a3 = kZero, a4 = kVlarge;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-    const double* pb = d.part + 8 * b;
+  for (int b = threadIdx.x; b < sc->blk_cnt; b += blockDim.x) {
+    const double* pb = d.part + 8 * (sc->blk_off + b);
     a0 = a0 + pb[0];
     a1 = a1 + pb[1];
     a2 = a2 + pb[2];
@@ -1237,7 +1253,6 @@ __global__ void __launch_bounds__(kRedThreads) k_final(Dev d, int nblk) {
   const double rmax_phi = block_max<kRedThreads>(a3, sm);
   const double dtmin = block_min<kRedThreads>(a4, sm);
   if (threadIdx.x == 0) {
-    Scalars* sc = d.sc;
     sc->iter = sc->iter + 1;
     sc->ttime = sc->ttime + sc->delt;
     double sbot = sumbot;
@@ -1252,7 +1267,7 @@ __global__ void __launch_bounds__(kRedThreads) k_final(Dev d, int nblk) {
     } else {
       sc->stime = sc->stime + sc->delt;
       sc->rmax = rmax_phi;
-      time_bcs(d, sc->stime);
+      time_bcs(d, sid, sc->stime);
       sc->delt = (d.dt_op == 0) ? d.cfl : dtmin;
     }
   }

@@ -412,4 +412,124 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
   return 0;
 }
 
+void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& M, std::vector<ScenarioInfo>& info) {
+  const size_t S = parts.size();
+  info.assign(S, ScenarioInfo{});
+  int32_t T = 0, N = 0, ne = 0, nwall = 0, nbce = 0, nnz = 0, kst = 1;
+  for (size_t s = 0; s < S; s++) {
+    const HostLayout& P = parts[s];
+    ScenarioInfo& I = info[s];
+    I.cell_off = T;
+    I.cell_cnt = P.T;
+    I.node_off = N;
+    I.node_cnt = P.N;
+    I.blk_off = T / block;
+    I.blk_cnt = (P.T + block - 1) / block;
+    I.last_cell = T + P.last_cell_new;
+    T += I.blk_cnt * block;
+    N += P.N;
+    ne += P.ne;
+    nwall += P.nwall;
+    nbce += P.nbce;
+    nnz += P.n2t_nnz;
+    kst = std::max(kst, P.kst);
+  }
+  M = HostLayout();
+  M.T = T;
+  M.N = N;
+  M.kst = kst;
+  M.ne = ne;
+  M.nwall = nwall;
+  M.nbce = nbce;
+  M.n2t_nnz = nnz;
+  const size_t T3 = 3 * (size_t)T;
+  // per cell slot
+  M.cell_sid.assign(T, -1);
+  M.area.assign(T, 1.0); M.perim.assign(T, 1.0); M.xc.assign(T, 0.0); M.yc.assign(T, 0.0);
+  M.z.assign(T, 0.0); M.delz_x.assign(T, 0.0); M.delz_y.assign(T, 0.0); M.zmax.assign(T, 0.0);
+  M.cd.assign(T, 0.0); M.lsq_a.assign(T, 1.0); M.lsq_b.assign(T, 0.0); M.lsq_c.assign(T, 1.0);
+  M.lsq_det.assign(T, 1.0); M.nst.assign(T, 0); M.forder.assign(T, 0); M.hvmask.assign(T, 0);
+  M.vert.assign(T3, 0); M.t2t3.assign(T3, -1); M.fref.assign(T3, 0); M.fkind.assign(T3, FACE_NONE);
+  M.rc_x.assign(T3, 0.0); M.rc_y.assign(T3, 0.0); M.fnx.assign(T3, 0.0); M.fny.assign(T3, 0.0);
+  M.flen.assign(T3, 0.0); M.fz0.assign(T3, 0.0);
+  M.st_id.assign((size_t)kst * T, 0); M.st_w.assign((size_t)kst * T, 0.0);
+  M.st_dx.assign((size_t)kst * T, 0.0); M.st_dy.assign((size_t)kst * T, 0.0);
+  M.node_sid.reserve(N); M.edge_sid.reserve(ne);
+  int32_t eoff = 0, woff = 0, boff = 0, noff_nnz = 0, tsoff = 0;
+  M.n2t_off.assign(1, 0);
+  for (size_t s = 0; s < S; s++) {
+    const HostLayout& P = parts[s];
+    const ScenarioInfo& I = info[s];
+    const int32_t co = I.cell_off, no = I.node_off;
+    for (int32_t c = 0; c < P.T; c++) {
+      const int32_t g = co + c;
+      M.cell_sid[g] = (int32_t)s;
+      M.area[g] = P.area[c]; M.perim[g] = P.perim[c]; M.xc[g] = P.xc[c]; M.yc[g] = P.yc[c];
+      M.z[g] = P.z[c]; M.delz_x[g] = P.delz_x[c]; M.delz_y[g] = P.delz_y[c]; M.zmax[g] = P.zmax[c];
+      M.cd[g] = P.cd[c]; M.lsq_a[g] = P.lsq_a[c]; M.lsq_b[g] = P.lsq_b[c]; M.lsq_c[g] = P.lsq_c[c];
+      M.lsq_det[g] = P.lsq_det[c]; M.nst[g] = P.nst[c]; M.forder[g] = P.forder[c]; M.hvmask[g] = P.hvmask[c];
+      for (int j = 0; j < 3; j++) {
+        const size_t q = (size_t)j * P.T + c, qg = (size_t)j * T + g;
+        M.vert[qg] = P.vert[q] + no;
+        M.t2t3[qg] = P.t2t3[q] < 0 ? -1 : P.t2t3[q] + co;
+        const uint8_t kind = P.fkind[q] & 7;
+        int32_t r = P.fref[q];
+        if (kind == FACE_LEFT || kind == FACE_RIGHT) r += eoff;
+        else if (kind == FACE_WALL) r += woff;
+        else if (kind == FACE_BC) r += boff;
+        M.fref[qg] = r;
+        M.fkind[qg] = P.fkind[q];
+        M.rc_x[qg] = P.rc_x[q]; M.rc_y[qg] = P.rc_y[q]; M.fnx[qg] = P.fnx[q]; M.fny[qg] = P.fny[q];
+        M.flen[qg] = P.flen[q]; M.fz0[qg] = P.fz0[q];
+      }
+      for (int k = 0; k < P.kst; k++) {
+        const size_t q = (size_t)k * P.T + c, qg = (size_t)k * T + g;
+        M.st_id[qg] = P.st_id[q] + co;
+        M.st_w[qg] = P.st_w[q]; M.st_dx[qg] = P.st_dx[q]; M.st_dy[qg] = P.st_dy[q];
+      }
+    }
+    for (int32_t n = 0; n < P.N; n++) {
+      M.node_sid.push_back((int32_t)s);
+      M.zvtx.push_back(P.zvtx[n]); M.node_x.push_back(P.node_x[n]); M.node_y.push_back(P.node_y[n]);
+      M.node_hbc.push_back(P.node_hbc[n]);
+      M.n2t_off.push_back(P.n2t_off[n + 1] + noff_nnz);
+    }
+    for (int32_t q = 0; q < P.n2t_nnz; q++) {
+      M.n2t_cell.push_back(P.n2t_cell[q] + co);
+      M.n2t_w.push_back(P.n2t_w[q]);
+    }
+    for (int32_t e = 0; e < P.ne; e++) {
+      M.edge_sid.push_back((int32_t)s);
+      M.eL.push_back(P.eL[e] + co); M.eR.push_back(P.eR[e] + co); M.eslot.push_back(P.eslot[e]);
+      M.enx.push_back(P.enx[e]); M.eny.push_back(P.eny[e]); M.elen.push_back(P.elen[e]); M.ez0.push_back(P.ez0[e]);
+    }
+    for (int32_t w = 0; w < P.nwall; w++) {
+      M.wall_p1.push_back(P.wall_p1[w] + no);
+      M.wall_p2.push_back(P.wall_p2[w] + no);
+    }
+    for (int32_t b = 0; b < P.nbdr; b++) {
+      M.bdr_sid.push_back((int32_t)s);
+      M.bdr_kind.push_back(P.bdr_kind[b]); M.bdr_slot.push_back(P.bdr_slot[b]);
+      M.bdr_off.push_back(P.bdr_off[b] + boff); M.bdr_cnt.push_back(P.bdr_cnt[b]);
+    }
+    for (int32_t e = 0; e < P.nbce; e++) {
+      M.bce_cell.push_back(P.bce_cell[e] + co); M.bce_slot.push_back(P.bce_slot[e]);
+      M.bce_nx.push_back(P.bce_nx[e]); M.bce_ny.push_back(P.bce_ny[e]);
+      M.bce_tx.push_back(P.bce_tx[e]); M.bce_ty.push_back(P.bce_ty[e]);
+      M.bce_len.push_back(P.bce_len[e]); M.bce_zmid.push_back(P.bce_zmid[e]);
+    }
+    for (int32_t c : P.bc_cells) M.bc_cells.push_back(c + co);
+    for (size_t i = 0; i < P.ts_t.size(); i++) {
+      M.ts_t.push_back(P.ts_t[i]);
+      M.ts_v.push_back(P.ts_v[i]);
+    }
+    (void)tsoff;
+    eoff += P.ne;
+    woff += P.nwall;
+    boff += P.nbce;
+    noff_nnz += P.n2t_nnz;
+  }
+  M.nbdr = (int32_t)M.bdr_kind.size();
+}
+
 }  // namespace storm

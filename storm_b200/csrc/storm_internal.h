@@ -80,9 +80,26 @@ struct HostLayout {
   std::vector<double> ts_t, ts_v;
   double bch_max = 0.0;
   int32_t last_cell_new = 0;  // new id of element n_elems (steady friction dt)
+  // merged layouts only
+  std::vector<int32_t> cell_sid, node_sid, edge_sid, bdr_sid;
 };
 
-// Build the device layout from the prepared (Fortran-layout) mesh.
+// Placement of one scenario inside a merged (batched) layout.
+struct ScenarioInfo {
+  int32_t cell_off = 0, cell_cnt = 0;  // cell slots [cell_off, cell_off + cell_cnt)
+  int32_t node_off = 0, node_cnt = 0;
+  int32_t blk_off = 0, blk_cnt = 0;    // reduction blocks covering the padded range
+  int32_t last_cell = 0;               // merged id of element n_elems
+};
+
+// Build the device layout of one prepared (Fortran-layout) mesh.
 int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& L);
+
+// Concatenate per-scenario layouts into one: every scenario's cell range starts on
+// a multiple of `block` (reduction blocks never span two scenarios); ids are shifted
+// by the scenario's offsets; cell_sid/node_sid/edge_sid/bdr_sid name the scenario
+// of every cell slot (-1 for padding), node, interior edge and open boundary.
+void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& M,
+                   std::vector<ScenarioInfo>& info);
 
 }  // namespace storm

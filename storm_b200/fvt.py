@@ -27,7 +27,8 @@ EXPORTS = (
     "storm_fvt_create", "storm_fvt_set_state", "storm_fvt_step", "storm_fvt_get_state",
     "storm_fvt_get_drycell", "storm_fvt_kernel_launches", "storm_fvt_set_kernel_timing",
     "storm_fvt_last_timing", "storm_fvt_kernel_times", "storm_fvt_destroy",
-    "storm_fvt_cfl_dt_noalloc",
+    "storm_fvt_cfl_dt_noalloc", "storm_fvt_create_batch", "storm_fvt_num_scenarios",
+    "storm_fvt_set_scenario_state", "storm_fvt_get_scenario_state", "storm_fvt_scenario_stats",
 )
 
 KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux")
@@ -72,6 +73,13 @@ def lib():
     L.storm_fvt_destroy.argtypes = [C.c_void_p]
     L.storm_fvt_cfl_dt_noalloc.argtypes = [C.c_void_p] * 5 + [C.c_int32, C.c_double, C.c_double, C.c_double,
                                                                 C.c_void_p, C.c_void_p]
+    L.storm_fvt_create_batch.argtypes = [C.POINTER(C.POINTER(abi.Mesh)), C.c_int32, C.POINTER(abi.Options),
+                                         C.POINTER(C.c_void_p)]
+    L.storm_fvt_num_scenarios.argtypes = [C.c_void_p]
+    L.storm_fvt_num_scenarios.restype = C.c_int32
+    L.storm_fvt_set_scenario_state.argtypes = [C.c_void_p, C.c_int32, dp, dp, dp]
+    L.storm_fvt_get_scenario_state.argtypes = [C.c_void_p, C.c_int32] + [dp] * 7
+    L.storm_fvt_scenario_stats.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.StepStats)]
     _lib = L
     return L
 
@@ -195,3 +203,45 @@ class Solver:
         n = (C.c_int64 * 8)()
         _chk(lib().storm_fvt_kernel_times(self._h, ms, n))
         return {k: (ms[i], n[i]) for i, k in enumerate(KERNEL_CLASSES)}
+
+
+class BatchSolver(Solver):
+    """Many independent scenarios advanced together (``storm_fvt_create_batch``): one
+    launch per kernel covers every mesh; each scenario has its own dt, clocks, stop
+    test and statistics."""
+
+    def __init__(self, meshes, options: abi.Options, *, keep=None):
+        self._keep = keep
+        ms = [m.mesh if isinstance(m, PreparedMesh) else m for m in meshes]
+        self.sizes = [(m.n_elems, m.n_pts) for m in ms]
+        self.T = sum(t for t, _ in self.sizes)
+        self.N = sum(n for _, n in self.sizes)
+        self.options = options
+        arr = (C.POINTER(abi.Mesh) * len(ms))(*[C.pointer(m) for m in ms])
+        h = C.c_void_p()
+        _chk(lib().storm_fvt_create_batch(arr, len(ms), C.byref(options), C.byref(h)))
+        self._h = h
+
+    @property
+    def n(self) -> int:
+        return int(lib().storm_fvt_num_scenarios(self._h))
+
+    def set_scenario_state(self, i: int, h, u, v):
+        T = self.sizes[i][0]
+        h, u, v = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, u, v))
+        if not (len(h) == len(u) == len(v) == T):
+            raise ValueError("state arrays must have n_elems entries of the scenario")
+        _chk(lib().storm_fvt_set_scenario_state(self._h, i, abi.dptr(h), abi.dptr(u), abi.dptr(v)))
+
+    def scenario_stats(self, i: int) -> dict:
+        st = abi.StepStats()
+        _chk(lib().storm_fvt_scenario_stats(self._h, i, C.byref(st)))
+        return st.as_dict()
+
+    def scenario_state(self, i: int) -> dict:
+        T, N = self.sizes[i]
+        out = {k: np.empty(T) for k in ("h", "u", "v", "rkh", "rku", "rkv")}
+        out["hvtx"] = np.empty(N)
+        _chk(lib().storm_fvt_get_scenario_state(self._h, i, *(abi.dptr(out[k]) for k in
+                                                              ("h", "u", "v", "rkh", "rku", "rkv", "hvtx"))))
+        return out
