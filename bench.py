@@ -145,6 +145,65 @@ def run_cpu(sc, steps, threads, warmup=0):
     return sc.n_elems * sc.options.rkorder * steps / dt, dt
 
 
+def run_batch(args, rank, world, local):
+    """Batched steady ensemble (one handle, one launch per kernel for all members):
+    mixed precision, autotuned block shapes, run to RMS dh < 1e-6 or --istop; reports
+    the cell-stage rate over the whole run and the iterations/time to steady of each
+    member (cold start from still water)."""
+    import torch
+    from storm_b200 import abi, build, fvt
+    build.build()
+    torch.cuda.set_device(local)
+    scs = scenarios.batch_channels(args.batch_n, args.batch_lo, args.batch_hi, seed=4 + rank,
+                                   opt_limiter=args.batch_limiter, precision=abi.PREC_MIXED, device=local)
+    pms = [fvt.build_mesh(sc.problem) for sc in scs]
+    b = fvt.BatchSolver(pms, scs[0].options, keep=pms)
+    for i, sc in enumerate(scs):
+        b.set_scenario_state(i, sc.h0, sc.u0, sc.v0)
+    tuned = b.autotune(iters=2)
+    torch.cuda.synchronize()
+    chunk, done, t_ms = 64, 0, 0.0
+    conv_at = [None] * len(scs)
+    launches0 = b.kernel_launches()
+    with ClockSampler(local) as clk:
+        while done < args.istop:
+            n = min(chunk, args.istop - done)
+            b.step(n)
+            t_ms += b.last_timing()["step_ms"]
+            done += n
+            stats = [b.scenario_stats(i) for i in range(len(scs))]
+            for i, st in enumerate(stats):
+                if st["converged"] and conv_at[i] is None:
+                    conv_at[i] = t_ms
+            if all(st["converged"] for st in stats):
+                break
+    iters = np.array([st["iter"] for st in stats])
+    cells = np.array([sc.n_elems for sc in scs])
+    cell_stages = float(np.sum(iters * cells) * 3)
+    conv = np.array([c is not None for c in conv_at])
+    tts = np.array([c if c is not None else np.nan for c in conv_at])
+    out = {
+        "metric": "cell-stage updates/s (batched steady ensemble) and time-to-steady per scenario",
+        "value": cell_stages / (t_ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": int(iters.max()),
+        "warmup": 0, "ms_per_step": t_ms / max(1, int(iters.max())), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic (seeded generator)",
+        "config": {"workload": f"batch-{len(scs)}x[{args.batch_lo},{args.batch_hi}]", "cells": int(cells.sum()),
+                   "scenarios": len(scs), "rstop": 1e-6, "istop": args.istop,
+                   "limiter": {0: "first order (opt 0)", 1: "LSQ (opt 1)", 2: "LSQ + BJ (opt 2)"}[args.batch_limiter],
+                   "block_sizes": tuned},
+        "time_to_steady": {"converged": int(conv.sum()), "of": len(scs),
+                           "iterations_median": float(np.median(iters[conv])) if conv.any() else None,
+                           "iterations_max": int(iters[conv].max()) if conv.any() else None,
+                           "ms_median": float(np.nanmedian(tts)) if conv.any() else None,
+                           "ms_all": float(t_ms), "cold_start": "still water, flat at the outlet level (raised to give the inlet h_n)"},
+        "gpu_launches": b.kernel_launches() - launches0,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -158,7 +217,14 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["meander", "dambreak", "channel"], default="meander")
+    ap.add_argument("--config", choices=["meander", "dambreak", "channel", "batch"], default="meander")
+    ap.add_argument("--batch-n", type=int, default=256, help="scenarios of the batched steady ensemble")
+    ap.add_argument("--batch-lo", type=int, default=20_000)
+    ap.add_argument("--batch-hi", type=int, default=400_000)
+    ap.add_argument("--istop", type=int, default=20_000, help="iteration cap of the steady runs")
+    ap.add_argument("--batch-limiter", type=int, default=0, choices=(0, 1, 2),
+                    help="opt_limiter of the steady ensemble (0: the only option whose RMS residual "
+                         "reaches 1e-6 on these channels; BJ stalls near 3e-5)")
     ap.add_argument("--cells", type=int, default=2_000_000)
     ap.add_argument("--cpu-steps", type=int, default=3, help="oracle iterations timed for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -205,6 +271,9 @@ def main():
         }
         print(json.dumps(out))
         return 0
+
+    if args.config == "batch":
+        return run_batch(args, rank, world, local)
 
     import torch
     dist = None

@@ -309,6 +309,12 @@ STORM_FVT_API int storm_fvt_last_timing(const StormFvtHandle* hd, double* step_m
  * 6 eflux (interior-edge fluxes); 7 is zero. */
 STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, int64_t* launches);
 
+/* Project autotuner: times `iters` iterations per candidate block size of the node,
+ * gradient, edge-flux and cell kernels on this handle's meshes (per-kernel CUDA
+ * events), keeps the fastest of each, re-captures the iteration graph and restores
+ * the state it started from.  `chosen` (may be NULL) receives the four sizes. */
+STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t* chosen);
+
 STORM_FVT_API int storm_fvt_destroy(StormFvtHandle* hd);
 
 /*

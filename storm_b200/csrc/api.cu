@@ -69,6 +69,8 @@ struct StormFvtHandle {
   std::vector<int> fev_class;    // kernel class of each pair
   double kt_ms[8] = {0};         // per-class totals of the last timed call
   int64_t kt_n[8] = {0};
+  // block sizes of the stage kernels (storm_fvt_autotune picks them)
+  int bs_node = 256, bs_grad = 256, bs_eflux = 128, bs_flux = 128;
 };
 
 namespace {
@@ -124,10 +126,10 @@ enum { KT_NODE = 0, KT_GRAD, KT_BC, KT_FLUX, KT_FRIC, KT_FINAL, KT_EFLUX, KT_COU
 int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
   const Dev& d = h->d;
   const int T = d.T, N = d.N, K = d.K;
-  const int gT = (T + kCellThreads - 1) / kCellThreads;
-  const int gF = (T + kFluxThreads - 1) / kFluxThreads;
-  const int gN = (N + kNodeThreads - 1) / kNodeThreads;
-  const int gE = (d.ne + kFluxThreads - 1) / kFluxThreads;
+  const int gT = (T + h->bs_grad - 1) / h->bs_grad;
+  const int gF = (T + h->bs_flux - 1) / h->bs_flux;
+  const int gN = (N + h->bs_node - 1) / h->bs_node;
+  const int gE = (d.ne + h->bs_eflux - 1) / h->bs_eflux;
   // in timing mode every launch is bracketed by an event pair tagged with its class
   auto mark = [&](int cls) -> int {
     if (!timing) return 0;
@@ -163,9 +165,9 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     uint8_t* dry_next = (s & 1) ? d.dry_b : d.dry_a;
     const int gB = (d.nbc_cells + kFluxThreads - 1) / kFluxThreads;
     if (mark(KT_NODE)) return STORM_ERR_CUDA;
-    k_node<<<gN, kNodeThreads, 0, h->stream>>>(d, hs, dry);
+    k_node<<<gN, h->bs_node, 0, h->stream>>>(d, hs, dry);
     if (done() || mark(KT_GRAD)) return STORM_ERR_CUDA;
-    launch(STAGE_GRAD, gT, kCellThreads, 0, h->stream, s, hs, dry, dry_next);
+    launch(STAGE_GRAD, gT, h->bs_grad, 0, h->stream, s, hs, dry, dry_next);
     if (done()) return STORM_ERR_CUDA;
     if (d.nbdr > 0 && !timing) {
       // k_bc on the side stream overlaps k_eflux and k_flux of the cells without
@@ -174,8 +176,8 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
       CK(cudaStreamWaitEvent(h->side, h->fork_ev[s], 0));
       launch(STAGE_BC, d.nbdr, 128, h->bc_smem, h->side, s, hs, dry, dry_next);
       CK(cudaEventRecord(h->join_ev[s], h->side));
-      if (gE > 0) launch(STAGE_EFLUX, gE, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
-      launch(STAGE_FLUX, gF, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+      if (gE > 0) launch(STAGE_EFLUX, gE, h->bs_eflux, 0, h->stream, s, hs, dry, dry_next);
+      launch(STAGE_FLUX, gF, h->bs_flux, 0, h->stream, s, hs, dry, dry_next);
       CK(cudaStreamWaitEvent(h->stream, h->join_ev[s], 0));
       if (gB > 0) launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
     } else {
@@ -186,11 +188,11 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
       }
       if (gE > 0) {
         if (mark(KT_EFLUX)) return STORM_ERR_CUDA;
-        launch(STAGE_EFLUX, gE, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+        launch(STAGE_EFLUX, gE, h->bs_eflux, 0, h->stream, s, hs, dry, dry_next);
         if (done()) return STORM_ERR_CUDA;
       }
       if (mark(KT_FLUX)) return STORM_ERR_CUDA;
-      launch(STAGE_FLUX, gF, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+      launch(STAGE_FLUX, gF, h->bs_flux, 0, h->stream, s, hs, dry, dry_next);
       if (gB > 0) launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
       if (done()) return STORM_ERR_CUDA;
     }
@@ -753,6 +755,77 @@ int storm_fvt_kernel_times(const StormFvtHandle* h, double* ms, int64_t* launche
     launches[c] = h->kt_n[c];
   }
   return STORM_OK;
+}
+
+int storm_fvt_autotune(StormFvtHandle* h, int32_t iters, int32_t* chosen) {
+  clear_error();
+  if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_autotune: null handle");
+  if (!h->have_state) return set_error(STORM_ERR_ARG, "storm_fvt_autotune: state not set");
+  if (iters < 1) iters = 1;
+  CK(cudaSetDevice(h->device));
+  // snapshot of the mutable state (restored afterwards: tuning does not advance the run)
+  const Dev& d = h->d;
+  const size_t T = (size_t)d.T, L = (size_t)(d.K + 1) * T;
+  const size_t bytes = 8 * (3 * L + 2 * T) + 2 * T + sizeof(Scalars) * (size_t)h->nscen;
+  char* snap = nullptr;
+  CK(cudaMalloc(&snap, bytes));
+  struct Piece {
+    void* p;
+    size_t n;
+  } pieces[] = {{d.rkh, 8 * L}, {d.rku, 8 * L}, {d.rkv, 8 * L}, {d.u_a, 8 * T}, {d.v_a, 8 * T},
+                {d.dry_a, T}, {d.dry_b, T}, {d.sc, sizeof(Scalars) * (size_t)h->nscen}};
+  size_t off = 0;
+  for (auto& pc : pieces) {
+    CK(cudaMemcpyAsync(snap + off, pc.p, pc.n, cudaMemcpyDeviceToDevice, h->stream));
+    off += pc.n;
+  }
+  struct Knob {
+    int* bs;
+    int cls;
+    int cand[3];
+  } knobs[] = {{&h->bs_node, KT_NODE, {64, 128, 256}},
+               {&h->bs_grad, KT_GRAD, {64, 128, 256}},
+               {&h->bs_eflux, KT_EFLUX, {32, 64, 128}},
+               {&h->bs_flux, KT_FLUX, {32, 64, 128}}};
+  const bool was_timing = h->timing;
+  h->timing = true;
+  int rc = 0;
+  for (auto& kb : knobs) {
+    double best = 1e300;
+    int best_bs = *kb.bs;
+    for (int cand : kb.cand) {
+      *kb.bs = cand;
+      if ((rc = storm_fvt_step(h, iters, nullptr))) break;
+      const double t = h->kt_ms[kb.cls];
+      if (t < best) {
+        best = t;
+        best_bs = cand;
+      }
+    }
+    *kb.bs = best_bs;
+    if (rc) break;
+  }
+  h->timing = was_timing;
+  off = 0;
+  for (auto& pc : pieces) {
+    cudaMemcpyAsync(pc.p, snap + off, pc.n, cudaMemcpyDeviceToDevice, h->stream);
+    off += pc.n;
+  }
+  cudaStreamSynchronize(h->stream);
+  cudaFree(snap);
+  if (rc) return rc;
+  if (chosen) {
+    chosen[0] = h->bs_node;
+    chosen[1] = h->bs_grad;
+    chosen[2] = h->bs_eflux;
+    chosen[3] = h->bs_flux;
+  }
+  // re-capture the iteration graph with the chosen shapes
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->exec = nullptr;
+  h->graph = nullptr;
+  return capture_graph(h);
 }
 
 int storm_fvt_destroy(StormFvtHandle* h) {

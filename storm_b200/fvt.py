@@ -29,6 +29,7 @@ EXPORTS = (
     "storm_fvt_last_timing", "storm_fvt_kernel_times", "storm_fvt_destroy",
     "storm_fvt_cfl_dt_noalloc", "storm_fvt_create_batch", "storm_fvt_num_scenarios",
     "storm_fvt_set_scenario_state", "storm_fvt_get_scenario_state", "storm_fvt_scenario_stats",
+    "storm_fvt_autotune",
 )
 
 KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux")
@@ -80,6 +81,7 @@ def lib():
     L.storm_fvt_set_scenario_state.argtypes = [C.c_void_p, C.c_int32, dp, dp, dp]
     L.storm_fvt_get_scenario_state.argtypes = [C.c_void_p, C.c_int32] + [dp] * 7
     L.storm_fvt_scenario_stats.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.StepStats)]
+    L.storm_fvt_autotune.argtypes = [C.c_void_p, C.c_int32, ip]
     _lib = L
     return L
 
@@ -196,6 +198,12 @@ class Solver:
         n = C.c_int64()
         _chk(lib().storm_fvt_last_timing(self._h, C.byref(a), C.byref(b), C.byref(n)))
         return {"step_ms": a.value, "flux_ms": b.value, "flux_launches": n.value}
+
+    def autotune(self, iters: int = 2) -> dict:
+        """Pick block sizes by timing (state restored afterwards)."""
+        ch = np.zeros(4, dtype=np.int32)
+        _chk(lib().storm_fvt_autotune(self._h, int(iters), abi.iptr(ch)))
+        return dict(zip(("node", "grad", "eflux", "flux"), ch.tolist()))
 
     def kernel_times(self) -> dict:
         """Per-kernel device ms and launch counts of the last step in timing mode."""

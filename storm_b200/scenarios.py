@@ -274,3 +274,85 @@ def algorithmic_bytes_per_cell_stage(n_elems: int, n_edges: int, n_pts: int,
     T, E, N = float(n_elems), float(n_edges), float(n_pts)
     vbar = 3.0 * T / N if mean_valence is None else mean_valence
     return 232.0 + 42.0 * E / T + 20.0 * N / T + 12.0 * vbar * N / T
+
+
+def meander_channel(n_cells: int, width: float, q: float, manning: float, stage: float, seed: int,
+                    slope: float = 0.001, cells_across: int = 0, cover_inlet: bool = True,
+                    **opt) -> Scenario:
+    """One steady ensemble member: a sine-meandering channel with the proportions and
+    bed of the straight 100 m x 10 m channel (length 10 widths, square quads each split
+    along one diagonal, bed slope 0.001 plus seeded noise of +-1 cm), bent along a
+    sine centreline of seeded wavelength (8-15 widths) and amplitude (0.5-1.5 widths);
+    about `n_cells` triangles.  Manning n and inflow Q (vtype 1) as given.  The
+    downstream water surface (htype 1) stands `stage` m above the Manning normal depth
+    of the member, h_n = (n Q / (W sqrt(S)))^(3/5), so the outlet stays subcritical:
+    with the stage counted from the bed, members with a large unit discharge put a
+    stage boundary on supercritical outflow, where the reference scheme (and this
+    port, bit for bit) diverges.  Cold start: still water with a flat surface at the
+    outlet level, raised where needed so the inlet carries at least h_n."""
+    rng = np.random.default_rng(seed)
+    ny = cells_across or int(np.clip(round(np.sqrt(n_cells / 20.0)), 6, 200))
+    nx = max(4, int(round(n_cells / (2 * ny))))
+    ds = width / ny
+    length = nx * ds
+    lam = rng.uniform(8.0, 15.0) * width
+    amp = rng.uniform(0.5, 1.5) * width
+    # centreline by arc length: y = amp sin(2 pi x / lam), sampled finely then resampled
+    xf = np.linspace(0.0, length * 1.5, 20 * nx + 1)
+    yf = amp * np.sin(2 * np.pi * xf / lam)
+    sf = np.concatenate([[0.0], np.cumsum(np.hypot(np.diff(xf), np.diff(yf)))])
+    s = np.arange(nx + 1) * ds
+    cx = np.interp(s, sf, xf)
+    cy = np.interp(s, sf, yf)
+    tx = np.gradient(cx)
+    ty = np.gradient(cy)
+    tn = np.hypot(tx, ty)
+    nxv, nyv = -ty / tn, tx / tn
+    off = (np.arange(ny + 1) / ny - 0.5) * width
+    X = (cx[:, None] + off[None, :] * nxv[:, None]).reshape(-1)
+    Y = (cy[:, None] + off[None, :] * nyv[:, None]).reshape(-1)
+    S = np.repeat(s, ny + 1)
+    nid = lambda i, j: i * (ny + 1) + j  # noqa: E731
+    I, J = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    I, J = I.reshape(-1), J.reshape(-1)
+    p00, p10, p11, p01 = nid(I, J), nid(I + 1, J), nid(I + 1, J + 1), nid(I, J + 1)
+    tri = np.empty((2 * nx * ny, 3), dtype=np.int64)
+    tri[0::2] = np.stack([p00, p10, p11], axis=1)
+    tri[1::2] = np.stack([p00, p11, p01], axis=1)
+    tri1 = _orient_ccw(X, Y, tri)
+    zb = slope * (length - S) + rng.uniform(-0.01, 0.01, size=S.shape)
+    T = len(tri1)
+    h_normal = (manning * q / (width * np.sqrt(slope))) ** 0.6
+    hbc = h_normal + stage  # outlet bed plane is at 0
+    t0 = tri1.astype(np.int64) - 1
+    zc = (zb[t0[:, 0]] + zb[t0[:, 1]] + zb[t0[:, 2]]) / 3.0
+    wse0 = hbc
+    if cover_inlet:
+        wse0 = max(hbc, float(zb[: ny + 1].max()) + h_normal)
+    h0 = np.maximum(wse0 - zc, 0.0)
+    prob = abi.ProblemHolder(
+        X, Y, tri1, zb, np.full(T, manning), zb_at_vertices=True, cd_at_vertices=False,
+        inflow=[{"type": 1, "nodes": np.array([nid(0, j) + 1 for j in range(ny + 1)]), "value": q}],
+        outflow=[{"type": 1, "nodes": np.array([nid(nx, j) + 1 for j in range(ny + 1)]), "value": hbc}])
+    o = dict(rkorder=3, opt_limiter=2, flux=abi.FLUX_HLL, cfl=0.9, steady=1, stop_cr=1, rstop=1e-6,
+             btype=0, hvalve=1, h_dry=1e-3, h_wet=1e-3, opt_friction=0)
+    o.update(opt)
+    return Scenario("meander_channel", prob, h0, np.zeros(T), np.zeros(T), abi.default_options(**o),
+                    {"seed": seed, "width": width, "q": q, "manning": manning, "stage": stage,
+                     "h_normal": h_normal, "hbc": hbc, "wse0": wse0, "slope": slope, "nx": nx, "ny": ny,
+                     "wavelength": lam, "amplitude": amp})
+
+
+def batch_channels(n_scen: int = 256, lo: int = 20_000, hi: int = 400_000, seed: int = 4, **opt) -> list:
+    """The batched steady ensemble: `n_scen` meandering channels with sizes
+    log-uniform in [lo, hi] triangles, width U[20,80] m, Q U[20,500] m^3/s,
+    n U[0.02,0.06], downstream stage U[0.5,3] m above normal depth (one seed per
+    member)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scen):
+        n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        out.append(meander_channel(n, width=rng.uniform(20, 80), q=rng.uniform(20, 500),
+                                   manning=rng.uniform(0.02, 0.06), stage=rng.uniform(0.5, 3.0),
+                                   seed=int(rng.integers(1 << 30)), **opt))
+    return out

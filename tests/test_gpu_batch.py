@@ -73,3 +73,27 @@ def test_batch_rejects_single_scenario_calls(storm_lib):
     with pytest.raises(fvt.StormError) as e:
         b.set_state(z, z, z)  # the whole-handle call is for single-scenario handles
     assert e.value.code == abi.STORM_ERR_ARG
+
+
+def test_autotune_keeps_state_and_results(storm_lib, oracle_mod):
+    """The autotuner restores the state it timed from, and other block shapes give the
+    same bits (every per-cell result is independent of the launch shape)."""
+    sc = scenarios.meander(n_target=12000, seed=13)
+    sc.problem.cd[:] = 0.0
+    pm = fvt.build_mesh(sc.problem)
+    g = fvt.Solver(pm, sc.options, keep=pm)
+    g.set_state(sc.h0, sc.u0, sc.v0)
+    g.step(5)
+    before = g.state()
+    chosen = g.autotune(iters=2)
+    after = g.state()
+    for k in ("h", "u", "v", "rku", "rkv"):
+        assert np.array_equal(_bits(before[k]), _bits(after[k])), k
+    assert set(chosen) == {"node", "grad", "eflux", "flux"}
+    g.step(20)
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    o.set_state(sc.h0, sc.u0, sc.v0)
+    o.step(25)
+    a, b = o.state(), g.state()
+    for k in ("h", "u", "v", "rku", "rkv"):
+        assert np.array_equal(_bits(a[k]), _bits(b[k])), k
