@@ -13,8 +13,9 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libstorm_fvt.so")
-SOURCES = ["api.cu", "fvt_kernels.cu", "layout.cpp", "mesh_build.cpp", "noalloc.cu"]
-HEADERS = ["fvt_device.cuh", "storm_internal.h", os.path.join("..", "..", "include", "storm_fvt.h")]
+SOURCES = ["api.cu", "fvt_kernels.cu", "layout.cpp", "mesh_build.cpp", "noalloc.cu", "gnn_kernels.cu"]
+HEADERS = ["fvt_device.cuh", "storm_internal.h", "umma.cuh", os.path.join("..", "..", "include", "storm_fvt.h"),
+           os.path.join("..", "..", "include", "storm_gnn.h")]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

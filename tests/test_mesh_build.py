@@ -91,6 +91,18 @@ def test_library_exports_every_declared_symbol(storm_lib):
         assert hasattr(lib, name), name
 
 
+def test_library_exports_every_warm_start_symbol(storm_lib):
+    from storm_b200 import gnn
+    hdr = open(os.path.join(ROOT, "include", "storm_gnn.h")).read()
+    declared = set(re.findall(r"STORM_FVT_API\s+[\w\s\*]+?\b(storm_gnn_\w+)\s*\(", hdr))
+    assert declared == set(gnn.EXPORTS)
+    lib = C.CDLL(fvt.lib_path())
+    for name in declared:
+        assert hasattr(lib, name), name
+    L = gnn.lib()
+    assert L.storm_gnn_grad_size(384, 128) == 128 * 384 + 128 + 128 * 128 + 128
+
+
 def test_option_checks_run_before_device_use(storm_lib):
     """Invalid options are rejected on the host (STORM_ERR_ARG / UNSUPPORTED)."""
     sc = scenarios.channel(nx=10, ny=4)
