@@ -158,7 +158,7 @@ def init_params(specs, total, seed: int = 0, out_scale: float = 1.0) -> np.ndarr
         lim1 = math.sqrt(6.0 / s.k_in)
         w1[:] = rng.uniform(-lim1, lim1, size=w1.shape)
         lim2 = math.sqrt(6.0 / HID) * (0.25 if s.name.startswith(("edge", "node")) else 1.0) * (
-            out_scale if s.name == "dec" else 1.0)
+            0.1 * out_scale if s.name == "dec" else 1.0)
         w2v = rng.uniform(-lim2, lim2, size=(s.n_out, HID)).astype(np.float32)
         if s.name == "dec":
             w2v[N_TARGET:] = 0.0
