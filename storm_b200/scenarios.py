@@ -343,16 +343,24 @@ def meander_channel(n_cells: int, width: float, q: float, manning: float, stage:
                      "wavelength": lam, "amplitude": amp})
 
 
-def batch_channels(n_scen: int = 256, lo: int = 20_000, hi: int = 400_000, seed: int = 4, **opt) -> list:
-    """The batched steady ensemble: `n_scen` meandering channels with sizes
-    log-uniform in [lo, hi] triangles, width U[20,80] m, Q U[20,500] m^3/s,
-    n U[0.02,0.06], downstream stage U[0.5,3] m above normal depth (one seed per
-    member)."""
+def batch_channel_params(n_scen: int = 256, lo: int = 20_000, hi: int = 400_000, seed: int = 4) -> list:
+    """Parameters of the ensemble members (no meshes built): sizes log-uniform in
+    [lo, hi] triangles, width U[20,80] m, Q U[20,500] m^3/s, n U[0.02,0.06],
+    downstream stage U[0.5,3] m above normal depth, one mesh seed per member."""
     rng = np.random.default_rng(seed)
     out = []
-    for k in range(n_scen):
+    for _ in range(n_scen):
         n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
-        out.append(meander_channel(n, width=rng.uniform(20, 80), q=rng.uniform(20, 500),
-                                   manning=rng.uniform(0.02, 0.06), stage=rng.uniform(0.5, 3.0),
-                                   seed=int(rng.integers(1 << 30)), **opt))
+        out.append(dict(n_cells=n, width=rng.uniform(20, 80), q=rng.uniform(20, 500),
+                        manning=rng.uniform(0.02, 0.06), stage=rng.uniform(0.5, 3.0),
+                        seed=int(rng.integers(1 << 30))))
     return out
+
+
+def batch_channels(n_scen: int = 256, lo: int = 20_000, hi: int = 400_000, seed: int = 4, only=None,
+                   **opt) -> list:
+    """The batched steady ensemble: one :func:`meander_channel` per member of
+    :func:`batch_channel_params`; `only` (indices) builds a subset, in that order."""
+    params = batch_channel_params(n_scen, lo, hi, seed)
+    idx = range(n_scen) if only is None else only
+    return [meander_channel(**params[i], **opt) for i in idx]
