@@ -228,6 +228,58 @@ def run_batch(args, rank, world, local):
     return 0
 
 
+def run_steady_channel(args, rank, world, local):
+    """Time to steady state on the 8,000-cell channel (100 m x 10 m, HLL, LSQ + BJ,
+    SSP-RK3, CFL 0.9, RMS dh < 1e-8 or --istop iterations): the whole run on the GPU
+    in FP64 and in mixed precision (device time of the graph replays and wall time
+    through the C-ABI), against the oracle port on the host cores, timed on a bounded
+    sample of the same iterations and extrapolated per iteration."""
+    import torch
+    from storm_b200 import abi, build, fvt
+    build.build()
+    torch.cuda.set_device(local)
+    res = {}
+    h64 = None
+    for prec in ("fp64", "mixed"):
+        sc = scenarios.channel()
+        sc.options.device = local
+        sc.options.precision = abi.PREC_MIXED if prec == "mixed" else abi.PREC_FP64
+        pm = fvt.build_mesh(sc.problem)
+        solver = fvt.Solver(pm, sc.options, keep=pm)
+        solver.set_state(sc.h0, sc.u0, sc.v0)
+        solver.step(1)
+        solver.set_state(sc.h0, sc.u0, sc.v0)  # same start after the warm-up launch
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = solver.step(args.istop)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        dev_ms = solver.last_timing()["step_ms"]
+        res[prec] = {"iterations": st["iter"], "converged": bool(st["converged"]), "rms_dh": st["rms_dh"],
+                     "device_s": dev_ms / 1e3, "wall_s": wall, "ms_per_iteration": dev_ms / max(1, st["iter"]),
+                     "cqin": st["cqin3"][0], "cqout": st["cqout3"][0]}
+        if prec == "fp64":
+            h64 = solver.state()["h"]
+        else:
+            res[prec]["depth_max_abs_vs_fp64_m"] = float(np.abs(solver.state()["h"] - h64).max())
+        solver.close()
+    out = {"metric": "time to steady state (8,000-cell channel)", "value": res["fp64"]["wall_s"], "unit": "s",
+           "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic (seeded generator)",
+           "config": {"workload": "channel-8000", "rstop": 1e-8, "istop": args.istop, "flux": "HLL",
+                      "limiter": "LSQ + BJ", "rk": 3, "cfl": 0.9}, "gpu": res}
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sc = scenarios.channel()
+        n = max(1, min(args.istop, args.cpu_steps))
+        for th, key in ((1, "cpu_1_thread"), (threads, "cpu_all_threads")):
+            _, secs = run_cpu(sc, n, th)
+            per_it = secs / n
+            out[key] = {"cores": th, "kind": "port", "sample_iterations": n, "s_per_iteration": per_it,
+                        "extrapolated_s": per_it * res["fp64"]["iterations"]}
+    print(json.dumps(out))
+    return 0
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -241,7 +293,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["meander", "dambreak", "channel", "batch"], default="meander")
+    ap.add_argument("--config", choices=["meander", "dambreak", "channel", "batch", "steady-channel"], default="meander")
     ap.add_argument("--batch-n", type=int, default=256, help="scenarios of the batched steady ensemble")
     ap.add_argument("--batch-lo", type=int, default=20_000)
     ap.add_argument("--batch-hi", type=int, default=400_000)
@@ -298,6 +350,10 @@ def main():
 
     if args.config == "batch":
         return run_batch(args, rank, world, local)
+    if args.config == "steady-channel":
+        if rank != 0:
+            return 0
+        return run_steady_channel(args, rank, world, local)
 
     import torch
     dist = None
