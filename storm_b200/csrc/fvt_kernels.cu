@@ -993,16 +993,39 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
   const double h_c = hs[c];
   double p1 = kZero, p2 = kZero, p3 = kZero;
   const uint8_t ord = d.forder[c];
-#pragma unroll 1
+  // Issue the loads of all three faces before the (ordered) accumulation: face
+  // descriptors first, then the edge fluxes of the interior faces, so the gathers
+  // overlap instead of forming one dependent chain per face.
+  int fj[3], fkd[3], fre[3];
+#pragma unroll
   for (int t = 0; t < 3; t++) {
-    const int j = (ord >> (2 * t)) & 3;
+    fj[t] = (ord >> (2 * t)) & 3;
+    const size_t q = (size_t)fj[t] * T + c;
+    fkd[t] = d.fkind[q] & 7;
+    fre[t] = d.fref[q];
+  }
+  bool fok[3];
+  R fv[3][3];
+#pragma unroll
+  for (int t = 0; t < 3; t++) {
+    fok[t] = false;
+    fv[t][0] = fv[t][1] = fv[t][2] = R(0);
+    if (fkd[t] == FACE_LEFT || fkd[t] == FACE_RIGHT) {
+      const int e = fre[t];  // flux*length of the edge, evaluated once by k_eflux
+      fok[t] = d.eok[e];
+      fv[t][0] = G.efx[e];
+      fv[t][1] = G.efx[d.ne + e];
+      fv[t][2] = G.efx[2 * d.ne + e];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 3; t++) {
+    const int j = fj[t];
     const size_t q = (size_t)j * T + c;
-    const uint8_t fk = d.fkind[q];
-    const int kind = fk & 7;
+    const int kind = fkd[t];
     if (kind == FACE_LEFT || kind == FACE_RIGHT) {
-      const int e = d.fref[q];  // flux*length of the edge, evaluated once by k_eflux
-      if (d.eok[e]) {
-        const double f0 = G.efx[e], f1 = G.efx[d.ne + e], f2 = G.efx[2 * d.ne + e];
+      if (fok[t]) {
+        const double f0 = fv[t][0], f1 = fv[t][1], f2 = fv[t][2];
         if (kind == FACE_LEFT) {
           p1 = p1 - f0;
           p2 = p2 - f1;
@@ -1017,7 +1040,7 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
       if (dry_c) continue;
       const double nx = d.fnx[q], ny = d.fny[q], len = d.flen[q];
       if (d.btype == 0) {  // wenslp3_fluxes.f90:34-67
-        const int w = d.fref[q];
+        const int w = fre[t];
         const double h1 = d.hvtx[d.wall_p1[w]], h2 = d.hvtx[d.wall_p2[w]];
         double hedge = sqrt((h1 * h1 + h1 * h2 + h2 * h2) * kOneThird);
         if (hedge < kZero) hedge = kZero;
@@ -1041,7 +1064,7 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
         p3 = p3 - (f3 + dh * ny) * len;
       }
     } else if (kind == FACE_BC) {
-      const int e = d.fref[q];
+      const int e = fre[t];
       p1 = p1 - d.bc_c[e];
       p2 = p2 - d.bc_c[d.nbce + e];
       p3 = p3 - d.bc_c[2 * d.nbce + e];
@@ -1069,6 +1092,9 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
   const double dt = delt / d.area[c];
   double rh = kZero, ru = kZero, rv = kZero;
   for (int j = 0; j <= s - 1; j++) {
+    // a zero coefficient (SSP-RK3 stage 3, level 1) adds a signed zero to a sum that
+    // started at +0, which leaves its bits unchanged: skip the loads
+    if (d.alpha[s][j] == kZero) continue;
     const size_t q = (size_t)j * T + c;
     rh = rh + d.alpha[s][j] * d.rkh[q];
     ru = ru + d.alpha[s][j] * d.rku[q];
