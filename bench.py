@@ -41,6 +41,10 @@ import numpy as np  # noqa: E402
 from storm_b200 import scenarios  # noqa: E402
 
 METRIC = "cell-stage updates/s (FVT time step, 2M-triangle meander)"
+# DRAM bytes (read + write) per cell-stage of the stage kernels, from one ncu capture of
+# the same kernels on the 500k-cell meander (profiles/fvt_stage_kernels_meander.md);
+# traffic grows in proportion to the cells, so it is scaled to the workload's mesh.
+NCU_DRAM_BYTES_PER_CELL_STAGE = {}
 UNIT = "cell-stage updates/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 
@@ -280,6 +284,93 @@ def run_steady_channel(args, rank, world, local):
     return 0
 
 
+def run_gnn(args, rank, world, local):
+    """Throughput of the warm-start network's tcgen05 kernels on a synthetic union of
+    channel meshes of --cells cells: one inference forward pass and one training step
+    (forward, loss, backward, Adam), CUDA events on the stream, against the measured
+    dense bf16 tensor peak (the MLP products are the tensor-bound part)."""
+    import torch
+    from storm_b200 import build, fvt, gnn
+    build.build()
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    rng = np.random.default_rng(0)
+    nb, xn, xe, total = [], [], [], 0
+    while total < args.cells:
+        sc = scenarios.channel(nx=500, ny=50, seed=len(nb))
+        mn = fvt.build_mesh(sc.problem).numpy()
+        T = mn["n_elems"]
+        nb.append(gnn.neighbour_table(mn))
+        xn.append(rng.normal(size=(T, gnn.IN_NODE)).astype(np.float32))
+        xe.append(rng.normal(size=(3, T, gnn.IN_EDGE)).astype(np.float32))
+        total += T
+    g = gnn.build_graph_fast(nb, xn, xe)
+    dg = gnn.DeviceGraph(g, dev)
+    net = gnn.WarmStartNet(device=dev, seed=1)
+    target = torch.zeros((g.Tp, 3), dtype=torch.float32, device=dev)
+    w = torch.from_numpy((np.arange(g.Tp) < g.T).astype(np.float32)).to(dev)
+
+    def fwd_flops():
+        f = 0
+        for s in net.specs:
+            rows = 3 * g.Tp if s.name.startswith(("edge", "enc_edge")) else g.Tp
+            f += 2 * rows * (s.k_in * gnn.HID + gnn.HID * s.n_out)
+        return f
+
+    def train_flops():
+        f = 0
+        for s in net.specs:
+            rows = 3 * g.Tp if s.name.startswith(("edge", "enc_edge")) else g.Tp
+            f += 2 * rows * (s.k_in * gnn.HID + gnn.HID * s.n_out)          # forward
+            f += 2 * rows * gnn.HID * s.n_out                                # dy W2
+            if not s.name.startswith("enc"):
+                f += 2 * rows * gnn.HID * s.k_in                             # dz1 W1
+            f += 2 * rows * (s.k_in * gnn.HID + gnn.HID * s.n_out)          # dW1, dW2
+        return f
+
+    def timed(fn, n):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        net._check_err()
+        return e0.elapsed_time(e1) / n
+
+    def train_step():
+        y = net.forward(dg, save=True)
+        dy, _ = net.mse(y, target, w, 3.0 * g.T)
+        net.backward(dy)
+        net.adam_step(1e-4)
+
+    n = max(1, min(args.steps, 20))
+    l0 = gnn.kernel_launches()
+    ms_fwd = timed(lambda: net.forward(dg, save=False), n)
+    ms_train = timed(train_step, n)
+    launches = gnn.kernel_launches() - l0
+    pk = peaks()
+    peak = pk.get("bf16_tflops") or 1590.0
+    ff, tf = fwd_flops(), train_flops()
+    out = {"metric": "warm-start network throughput (cells/s)", "value": g.T / (ms_fwd / 1e3),
+           "unit": "cells/s (inference)", "higher_is_better": True, "n_gpus": 1, "dtype": "bf16 (fp32 accumulate)",
+           "data": "synthetic graph (channel meshes, random features)",
+           "config": {"workload": f"gnn-{g.T}", "cells": g.T, "layers": gnn.N_LAYERS, "hidden": gnn.HID},
+           "inference": {"ms": ms_fwd, "tflops": ff / (ms_fwd / 1e3) / 1e12},
+           "training_step": {"ms": ms_train, "tflops": tf / (ms_train / 1e3) / 1e12,
+                             "cells_per_s": g.T / (ms_train / 1e3)},
+           "roofline": {"bound": "tensor", "achieved": ff / (ms_fwd / 1e3) / 1e12, "peak": peak,
+                        "unit": "TFLOP/s", "frac": ff / (ms_fwd / 1e3) / 1e12 / peak, "traffic": None,
+                        "kernel": "forward pass (19 fused MLP launches)", "flops_per_launch": ff,
+                        "peak_source": pk["source"]},
+           "gpu_launches": launches}
+    print(json.dumps(out))
+    return 0
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -293,7 +384,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["meander", "dambreak", "channel", "batch", "steady-channel"], default="meander")
+    ap.add_argument("--config", choices=["meander", "dambreak", "channel", "batch", "steady-channel", "gnn"], default="meander")
     ap.add_argument("--batch-n", type=int, default=256, help="scenarios of the batched steady ensemble")
     ap.add_argument("--batch-lo", type=int, default=20_000)
     ap.add_argument("--batch-hi", type=int, default=400_000)
@@ -350,6 +441,10 @@ def main():
 
     if args.config == "batch":
         return run_batch(args, rank, world, local)
+    if args.config == "gnn":
+        if rank != 0:
+            return 0
+        return run_gnn(args, rank, world, local)
     if args.config == "steady-channel":
         if rank != 0:
             return 0
@@ -457,13 +552,25 @@ def main():
     stage_ms = sum(kt[k][0] for k in ("node", "grad", "bc", "eflux", "flux"))
     B = scenarios.algorithmic_bytes_per_cell_stage(T, E, N)
     pk = peaks()
-    achieved = B * T * K_rk * kt_steps / (stage_ms / 1e3) / 1e9
+    # The launch unit is one graph replay = one iteration (K stages of every kernel,
+    # friction and the reductions), timed with CUDA events on the library's stream over
+    # the timed region above; the per-kernel pass (serialised, one event pair per
+    # launch, the boundary kernel no longer overlapped) gives the shares.
+    ms_iter = ms_max / args.steps
+    achieved = B * T * K_rk / (ms_iter / 1e3) / 1e9
+    achieved_serial = B * T * K_rk * kt_steps / (stage_ms / 1e3) / 1e9
     iter_ms = sum(v[0] for v in kt.values())
+    traffic = None
+    if args.config in NCU_DRAM_BYTES_PER_CELL_STAGE:
+        traffic = NCU_DRAM_BYTES_PER_CELL_STAGE[args.config] * T * K_rk
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
-        "frac": achieved / pk["hbm_gbs"], "traffic": None,
-        "kernel": "one RK stage: k_node + k_grad + k_bc + k_eflux + k_flux",
-        "bytes_per_cell_stage": B, "peak_source": pk["source"],
+        "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+        "kernel": "one iteration (CUDA graph: K x [k_node, k_grad, k_bc || k_eflux, k_flux], k_fric, k_final)",
+        "algorithmic_bytes_per_launch": B * T * K_rk, "bytes_per_cell_stage": B, "peak_source": pk["source"],
+        "traffic_source": "ncu dram__bytes_read+write of the stage kernels on the 500k-cell meander, "
+                          "per cell-stage, scaled to this mesh" if traffic else None,
+        "achieved_serialised_stage_chain": achieved_serial,
         "kernel_ms_share": {k: round(v[0] / iter_ms, 4) for k, v in kt.items()},
         "flux_kernel_avg_ms": kt["flux"][0] / max(1, kt["flux"][1]),
     }

@@ -93,36 +93,92 @@ __device__ __forceinline__ void set_err(int32_t* err, int code) {
 
 // ---- shared-memory staging -------------------------------------------------------
 
+// The staging helpers below give every thread up to eight 16-byte chunks of the tile
+// (chunk q = threadIdx.x + i*256) and issue all of a thread's global loads before any
+// of its shared-memory stores, so 32 KB per SM are in flight instead of one load per
+// thread at a time.
+constexpr int kChunksPerThread = 8;  // 128 rows x 16 chunks / 256 threads
+
+__device__ __forceinline__ void store_chunk(uint8_t* dst, int q, int cpr, uint4 v) {
+  const int r = q / cpr, c = q - r * cpr;
+  const int blk = c >> 3;
+  *reinterpret_cast<uint4*>(dst + blk * (kRows * 128) + umma::sw128_offset(r, (c & 7) * 8)) = v;
+}
+
 // Stage rows [row0, row0+128) of one segment into `dst` (blocks of 128 x 64, 16 KB each).
 __device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* dst) {
   const int cpr = s.width >> 3;  // 16-byte chunks per row
   const int total = kRows * cpr;
-  for (int q = threadIdx.x; q < total; q += kThreads) {
-    const int r = q / cpr, c = q - r * cpr;
-    const int row = row0 + r;
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (!s.agg) {
-      const int srow = s.idx ? s.idx[row] : row;
-      if (srow >= 0) v = *reinterpret_cast<const uint4*>(s.src + static_cast<size_t>(srow) * s.width + c * 8);
-    } else {
+  if (!s.agg) {
+    uint4 v[kChunksPerThread];
+    int srow[kChunksPerThread];
+#pragma unroll
+    for (int i = 0; i < kChunksPerThread; i++) {
+      const int q = threadIdx.x + i * kThreads;
+      const int row = row0 + q / cpr;
+      srow[i] = (q < total) ? (s.idx ? s.idx[row] : row) : -1;
+    }
+#pragma unroll
+    for (int i = 0; i < kChunksPerThread; i++) {
+      const int q = threadIdx.x + i * kThreads;
+      const int c = q % cpr;
+      v[i] = make_uint4(0, 0, 0, 0);
+      if (srow[i] >= 0)
+        v[i] = *reinterpret_cast<const uint4*>(s.src + static_cast<size_t>(srow[i]) * s.width + c * 8);
+    }
+#pragma unroll
+    for (int i = 0; i < kChunksPerThread; i++) {
+      const int q = threadIdx.x + i * kThreads;
+      if (q < total) store_chunk(dst, q, cpr, v[i]);
+    }
+    return;
+  }
+  // aggregation: sum of the three edge rows of each cell, in halves of four chunks
+#pragma unroll
+  for (int h = 0; h < kChunksPerThread; h += 4) {
+    uint4 w[4][3];
+    bool m[4][3];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int q = threadIdx.x + (h + i) * kThreads;
+      const int row = row0 + q / cpr;
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        m[i][k] = (q < total) && s.nbr[static_cast<size_t>(k) * s.agg_stride + row] >= 0;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int q = threadIdx.x + (h + i) * kThreads;
+      const int row = row0 + q / cpr, c = q % cpr;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        w[i][k] = make_uint4(0, 0, 0, 0);
+        if (m[i][k]) {
+          const size_t er = static_cast<size_t>(k) * s.agg_stride + row;
+          w[i][k] = *reinterpret_cast<const uint4*>(s.src + er * s.width + c * 8);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int q = threadIdx.x + (h + i) * kThreads;
+      if (q >= total) continue;
       float acc[8];
 #pragma unroll
       for (int j = 0; j < 8; j++) acc[j] = 0.f;
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        const size_t er = static_cast<size_t>(k) * s.agg_stride + row;
-        if (s.nbr[er] < 0) continue;
-        const uint4 w = *reinterpret_cast<const uint4*>(s.src + er * s.width + c * 8);
-        const bf16* b = reinterpret_cast<const bf16*>(&w);
+        if (!m[i][k]) continue;
+        const bf16* b = reinterpret_cast<const bf16*>(&w[i][k]);
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[j] += __bfloat162float(b[j]);
       }
+      uint4 v;
       bf16* o = reinterpret_cast<bf16*>(&v);
 #pragma unroll
       for (int j = 0; j < 8; j++) o[j] = __float2bfloat16(acc[j]);
+      store_chunk(dst, q, cpr, v);
     }
-    const int blk = c >> 3;
-    *reinterpret_cast<uint4*>(dst + blk * (kRows * 128) + umma::sw128_offset(r, (c & 7) * 8)) = v;
   }
 }
 
@@ -130,30 +186,59 @@ __device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* d
 __device__ __forceinline__ void stage_f32(const float* src, int width, int row0, uint8_t* dst) {
   const int cpr = width >> 3;
   const int total = kRows * cpr;
-  for (int q = threadIdx.x; q < total; q += kThreads) {
-    const int r = q / cpr, c = q - r * cpr;
-    const float4* p = reinterpret_cast<const float4*>(src + static_cast<size_t>(row0 + r) * width + c * 8);
-    const float4 a = p[0], b = p[1];
-    uint4 v;
-    bf16* o = reinterpret_cast<bf16*>(&v);
-    o[0] = __float2bfloat16(a.x); o[1] = __float2bfloat16(a.y); o[2] = __float2bfloat16(a.z);
-    o[3] = __float2bfloat16(a.w); o[4] = __float2bfloat16(b.x); o[5] = __float2bfloat16(b.y);
-    o[6] = __float2bfloat16(b.z); o[7] = __float2bfloat16(b.w);
-    const int blk = c >> 3;
-    *reinterpret_cast<uint4*>(dst + blk * (kRows * 128) + umma::sw128_offset(r, (c & 7) * 8)) = v;
+#pragma unroll
+  for (int h = 0; h < kChunksPerThread; h += 4) {
+    float4 a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int q = threadIdx.x + (h + i) * kThreads;
+      a[i] = b[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (q < total) {
+        const int r = q / cpr, c = q - r * cpr;
+        const float4* p = reinterpret_cast<const float4*>(src + static_cast<size_t>(row0 + r) * width + c * 8);
+        a[i] = p[0];
+        b[i] = p[1];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int q = threadIdx.x + (h + i) * kThreads;
+      if (q >= total) continue;
+      uint4 v;
+      bf16* o = reinterpret_cast<bf16*>(&v);
+      o[0] = __float2bfloat16(a[i].x); o[1] = __float2bfloat16(a[i].y); o[2] = __float2bfloat16(a[i].z);
+      o[3] = __float2bfloat16(a[i].w); o[4] = __float2bfloat16(b[i].x); o[5] = __float2bfloat16(b[i].y);
+      o[6] = __float2bfloat16(b[i].z); o[7] = __float2bfloat16(b[i].w);
+      store_chunk(dst, q, cpr, v);
+    }
   }
 }
 
 // Stage a bf16 row-major [nrows][ncols] matrix (ncols multiple of 64) as blocks of
-// nrows x 64 (block stride nrows*128 bytes).
+// nrows x 64 (block stride nrows*128 bytes); loads batched eight per thread.
 __device__ __forceinline__ void stage_matrix(const bf16* src, int nrows, int ncols, uint8_t* dst) {
   const int cpr = ncols >> 3;
   const int total = nrows * cpr;
-  for (int q = threadIdx.x; q < total; q += kThreads) {
-    const int r = q / cpr, c = q - r * cpr;
-    const uint4 v = *reinterpret_cast<const uint4*>(src + static_cast<size_t>(r) * ncols + c * 8);
-    const int blk = c >> 3;
-    *reinterpret_cast<uint4*>(dst + blk * (nrows * 128) + umma::sw128_offset(r, (c & 7) * 8)) = v;
+  for (int q0 = 0; q0 < total; q0 += kChunksPerThread * kThreads) {
+    uint4 v[kChunksPerThread];
+#pragma unroll
+    for (int i = 0; i < kChunksPerThread; i++) {
+      const int q = q0 + threadIdx.x + i * kThreads;
+      v[i] = make_uint4(0, 0, 0, 0);
+      if (q < total) {
+        const int r = q / cpr, c = q - r * cpr;
+        v[i] = *reinterpret_cast<const uint4*>(src + static_cast<size_t>(r) * ncols + c * 8);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kChunksPerThread; i++) {
+      const int q = q0 + threadIdx.x + i * kThreads;
+      if (q < total) {
+        const int r = q / cpr, c = q - r * cpr;
+        const int blk = c >> 3;
+        *reinterpret_cast<uint4*>(dst + blk * (nrows * 128) + umma::sw128_offset(r, (c & 7) * 8)) = v[i];
+      }
+    }
   }
 }
 

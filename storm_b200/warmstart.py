@@ -393,6 +393,19 @@ def pipeline(train_n=4096, eval_n=64, lo=2000, hi=8000, gen_batch=512, istop=400
         np.savez(weights_out, params=net.params_numpy(), **norm.arrays())
     del batches
     # 3. evaluation on held-out scenarios
+    res["eval"] = evaluate(net, norm, eval_n, lo, hi, istop, limiter, device, seed)
+    return res
+
+
+def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, device=0, seed=7,
+             plain_n=8) -> dict:
+    """Held-out scenarios (seeds disjoint from the training data) run to the stop test:
+    cold FP64 and cold mixed (batched), warm mixed (batched, from the network's
+    prediction), the plain FP64 solver on each scenario alone (the first `plain_n`),
+    and an FP64 continuation to RMS dh < 1e-10 as the steady state the depth errors
+    are measured against."""
+    import torch
+    dev = torch.device(f"cuda:{device}")
     ev = _member_list(eval_n, lo, hi, seed=seed * 100003 + 99_999_989, limiter=limiter)
     inps = []
     tf = time.perf_counter()
@@ -425,7 +438,7 @@ def pipeline(train_n=4096, eval_n=64, lo=2000, hi=8000, gen_batch=512, istop=400
                 "device_s_batch": r["device_ms"] / 1e3, "device_ms_per_scenario": r["device_ms"] / len(ev),
                 "wall_s_batch": r["wall_s"]}
 
-    res["eval"] = {"cold_fp64": summ(cold64), "cold_mixed": summ(cold_mx), "warm_mixed": summ(warm_mx),
+    out = {"cold_fp64": summ(cold64), "cold_mixed": summ(cold_mx), "warm_mixed": summ(warm_mx),
                    "inference_ms_batch": infer_ms, "inference_host_s_batch": tm["host_s"],
                    "features_host_s_batch": feat_s,
                    "speedup_per_scenario_vs_cold_fp64": (cold64["device_ms"]) / (warm_mx["device_ms"] + infer_ms),
@@ -440,7 +453,31 @@ def pipeline(train_n=4096, eval_n=64, lo=2000, hi=8000, gen_batch=512, istop=400
                                                     "cold_mixed": float(np.median(dh_cold)),
                                                     "cold_fp64": float(np.median(dh_cold64)),
                                                     "prediction": float(np.median(dh_pred))}}
-    return res
+    plain = []
+    for sc in ev[:plain_n]:
+        pm = fvt.build_mesh(sc.problem)
+        opt = abi.default_options(**{f: getattr(sc.options, f) for f, _ in abi.Options._fields_ if f != "reserved"})
+        opt.precision = abi.PREC_FP64
+        opt.device = device
+        with fvt.Solver(pm, opt, keep=pm) as s1:
+            s1.set_state(sc.h0, sc.u0, sc.v0)
+            s1.step(1)
+            s1.set_state(sc.h0, sc.u0, sc.v0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = s1.step(istop)
+            torch.cuda.synchronize()
+            plain.append({"cells": sc.n_elems, "iters": st["iter"], "converged": bool(st["converged"]),
+                          "wall_s": time.perf_counter() - t0, "device_s": s1.last_timing()["step_ms"] / 1e3})
+    if plain:
+        w_plain = float(np.mean([p["wall_s"] for p in plain]))
+        warm_wall = (warm_mx["wall_s"] + infer_ms / 1e3 + tm["host_s"] + feat_s) / len(ev)
+        out["plain_fp64_single"] = {"scenarios": len(plain), "wall_s_mean": w_plain,
+                                    "iters_mean": float(np.mean([p["iters"] for p in plain])),
+                                    "converged": int(sum(p["converged"] for p in plain))}
+        out["speedup_per_scenario_vs_plain_fp64_single_cold"] = w_plain / warm_wall
+        out["warm_batched_wall_s_per_scenario_incl_network"] = warm_wall
+    return out
 
 
 def main(argv=None):
@@ -458,9 +495,22 @@ def main(argv=None):
     ap.add_argument("--cells-per-batch", type=int, default=400_000)
     ap.add_argument("--weights-out", default=None)
     ap.add_argument("--json-out", default=None)
+    ap.add_argument("--model", default=None, help="evaluate this trained model (.npz) instead of training")
+    ap.add_argument("--plain-n", type=int, default=8)
     a = ap.parse_args(argv)
     from . import build
     build.build()
+    if a.model:
+        import torch
+        torch.cuda.set_device(0)
+        net, norm = load_model(a.model)
+        res = {"model": a.model, "eval": evaluate(net, norm, a.eval_n, a.lo, a.hi, a.istop, plain_n=a.plain_n)}
+        s = json.dumps(res)
+        print(s)
+        if a.json_out:
+            with open(a.json_out, "w") as f:
+                f.write(s + "\n")
+        return
     res = pipeline(a.train_n, a.eval_n, a.lo, a.hi, a.gen_batch, a.istop, a.epochs, a.cells_per_batch, a.lr,
                    weights_out=a.weights_out, log=lambda m: print(m, flush=True))
     s = json.dumps(res)

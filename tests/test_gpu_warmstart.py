@@ -1,0 +1,36 @@
+"""The trained warm start against the method without it: on held-out ensemble
+members (seeds disjoint from the training data) the solver, started from the
+network's prediction, reaches the same stop test (RMS dh < 1e-6) in fewer iterations
+than from the cold start, and its steady depth agrees with the cold run's."""
+import os
+
+import numpy as np
+import pytest
+
+from storm_b200 import abi, fvt, scenarios, warmstart
+
+pytestmark = pytest.mark.gpu
+
+MODEL = os.path.join(os.path.dirname(warmstart.__file__), "models", "warmstart_channels.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(MODEL), reason="no trained model in the package")
+def test_warm_start_needs_fewer_iterations(storm_lib):
+    net, norm = warmstart.load_model(MODEL)
+    scs = scenarios.batch_channels(6, 2000, 5000, seed=424_242, opt_limiter=0)
+    inps = []
+    for sc in scs:
+        pm = fvt.build_mesh(sc.problem)
+        q, hbc = warmstart.scenario_q_hbc(sc)
+        inps.append(warmstart.scenario_inputs(pm.numpy(), q, hbc, sc.options.h_dry))
+    preds = warmstart.predict(net, norm, inps, "cuda:0")
+    states = [warmstart.state_from_prediction(i, p) for i, p in zip(inps, preds)]
+    for h, u, v in states:
+        assert np.isfinite(h).all() and (h >= 0).all() and np.isfinite(u).all() and np.isfinite(v).all()
+    cold = warmstart.run_steady_batch(scs, istop=40000, precision=abi.PREC_MIXED)
+    warm = warmstart.run_steady_batch(scs, states=states, istop=40000, precision=abi.PREC_MIXED)
+    assert cold["converged"].all() and warm["converged"].all()
+    assert warm["iters"].mean() < 0.67 * cold["iters"].mean(), (warm["iters"], cold["iters"])
+    for a, b in zip(warm["states"], cold["states"]):
+        # both runs stop at RMS dh < 1e-6, a few cm short of the steady state
+        assert np.abs(a["h"] - b["h"]).max() < 0.25
