@@ -44,7 +44,7 @@ METRIC = "cell-stage updates/s (FVT time step, 2M-triangle meander)"
 # DRAM bytes (read + write) per cell-stage of the stage kernels, from one ncu capture of
 # the same kernels on the 500k-cell meander (profiles/fvt_stage_kernels_meander.md);
 # traffic grows in proportion to the cells, so it is scaled to the workload's mesh.
-NCU_DRAM_BYTES_PER_CELL_STAGE = {}
+NCU_DRAM_BYTES_PER_CELL_STAGE = {"meander": 714.6}
 UNIT = "cell-stage updates/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 
@@ -575,8 +575,9 @@ def main():
         "flux_kernel_avg_ms": kt["flux"][0] / max(1, kt["flux"][1]),
     }
 
+    metric = METRIC if args.config == "meander" else f"cell-stage updates/s (FVT time step, {args.config})"
     out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
         "data": "synthetic (seeded generator; no public dataset exists for this path)",

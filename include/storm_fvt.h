@@ -81,7 +81,8 @@ typedef struct StormFvtOptions {
   int32_t opt_friction;/* 0 Manning, 1 Chezy, 2 drag, 3 Colebrook, 4 Strickler     */
   int32_t stop_cr;     /* steady stop criterion: 0 max|phi|, 1 RMS relative dh     */
   int32_t flux;        /* interior-edge flux: STORM_FLUX_ROE|HLL|RUSANOV           */
-  int32_t precision;   /* STORM_PREC_FP64 (only value accepted by this version)    */
+  int32_t precision;   /* STORM_PREC_FP64, or STORM_PREC_MIXED (FP32 gradient, flux
+                          and source arithmetic; FP64 state, reconstruction, mass)  */
   int32_t device;      /* CUDA device ordinal                                      */
   int32_t reserved[6]; /* must be zero                                             */
 } StormFvtOptions;

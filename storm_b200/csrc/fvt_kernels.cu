@@ -1,25 +1,27 @@
 // fvt_kernels.cu -- sm_100a kernels of one SToRM FVT iteration (solverFVT.f90:129-476).
 //
-// One RK stage (solverFVT.f90:161-325) is four launches:
-//   k_node  per node : ctr2vtxWSE type 3 + cap + positivity_vtx + enforce_bcs stage
-//                      nodes (to_vertices.f90:26-41, enforce_bcs.f90:37-56)
-//   k_grad  per cell : find_dry_cells state, lsq_grad_array x3, limiterBJ x3, delh -= delz
-//                      (cell_grads.f90), hgradfix2.f90:48-98, zeroing of cells with a
-//                      vertex depth <= h_dry (to_vertices.f90:44-55)
-//   k_bc    per open boundary (one CTA): inflowQbyH / inflowH / outflowbyH /
-//                      crit_outflow / free_flow, including the inflow fixed-point
-//   k_flux  per cell : every face flux of the cell (Roe/HLL/Rusanov, I1 wet/dry wall,
-//                      wenslp3/weslp2 walls, boundary contributions) gathered in the
-//                      order invisc_fluxes.f90 scatters them, bed_slope_STD + adjustZb,
-//                      the SSP-RK combination, vclip, h >= 0 and wet/dry hysteresis
+// One RK stage (solverFVT.f90:161-325) is:
+//   k_node   per node : ctr2vtxWSE type 3 + cap + positivity_vtx + enforce_bcs stage
+//                       nodes (to_vertices.f90:26-41, enforce_bcs.f90:37-56)
+//   k_grad   per cell : find_dry_cells state, lsq_grad_array x3, limiterBJ x3, delh -= delz
+//                       (cell_grads.f90), hgradfix2.f90:48-98, zeroing of cells with a
+//                       vertex depth <= h_dry (to_vertices.f90:44-55)
+//   k_bc     per open boundary (one CTA): inflowQbyH / inflowH / outflowbyH /
+//                       crit_outflow / free_flow, including the inflow fixed point
+//   k_eflux  per interior edge: the Roe/HLL/Rusanov flux (with the I1 wet/dry wall test)
+//                       evaluated once, in the reference's orientation, times the length
+//   k_flux   per cell : the cell's face contributions (edge fluxes from k_eflux, the
+//                       wenslp3/weslp2 walls, boundary contributions) added in the order
+//                       invisc_fluxes.f90 scatters them, bed_slope_STD + adjustZb, the
+//                       SSP-RK combination, vclip, h >= 0 and wet/dry hysteresis
+//                       (k_flux_bc: the cells with an open-boundary face, after k_bc)
 // and one iteration ends with
 //   k_fric  per cell : find_dry_cells, fric_terms_impl, the numerical valve, the
 //                      RK level copy, block partials of sumtop/sumbot/tmass/max|phi|/dt
-//   k_final one CTA  : deterministic reduction of the partials, stop test, clocks,
-//                      get_time_bcs.
+//   k_final one CTA per scenario: deterministic reduction of the partials, stop test,
+//                      clocks, get_time_bcs.
 // No float atomics: every sum is a fixed-order tree or a serial loop, so the results
-// are reproducible run to run; every interior-edge flux is evaluated by both of its
-// cells with the same inputs in the same order, so both sides agree bit for bit.
+// are reproducible run to run.
 #include <cstdint>
 
 #include "fvt_device.cuh"
