@@ -105,42 +105,46 @@ __device__ __forceinline__ void store_chunk(uint8_t* dst, int q, int cpr, uint4 
   *reinterpret_cast<uint4*>(dst + blk * (kRows * 128) + umma::sw128_offset(r, (c & 7) * 8)) = v;
 }
 
-// Stage rows [row0, row0+128) of one segment into `dst` (blocks of 128 x 64, 16 KB each).
-__device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* dst) {
+// Stage rows [row0, row0+128) of one segment into `dst` (blocks of 128 x 64, 16 KB
+// each) with `nthr` threads (thread `tid` of them), in rounds of eight chunks per thread.
+__device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* dst, int tid = -1,
+                                              int nthr = kThreads) {
+  if (tid < 0) tid = threadIdx.x;
   const int cpr = s.width >> 3;  // 16-byte chunks per row
   const int total = kRows * cpr;
   if (!s.agg) {
-    uint4 v[kChunksPerThread];
-    int srow[kChunksPerThread];
+    for (int q0 = 0; q0 < total; q0 += kChunksPerThread * nthr) {
+      uint4 v[kChunksPerThread];
+      int srow[kChunksPerThread];
 #pragma unroll
-    for (int i = 0; i < kChunksPerThread; i++) {
-      const int q = threadIdx.x + i * kThreads;
-      const int row = row0 + q / cpr;
-      srow[i] = (q < total) ? (s.idx ? s.idx[row] : row) : -1;
-    }
+      for (int i = 0; i < kChunksPerThread; i++) {
+        const int q = q0 + tid + i * nthr;
+        const int row = row0 + q / cpr;
+        srow[i] = (q < total) ? (s.idx ? s.idx[row] : row) : -1;
+      }
 #pragma unroll
-    for (int i = 0; i < kChunksPerThread; i++) {
-      const int q = threadIdx.x + i * kThreads;
-      const int c = q % cpr;
-      v[i] = make_uint4(0, 0, 0, 0);
-      if (srow[i] >= 0)
-        v[i] = *reinterpret_cast<const uint4*>(s.src + static_cast<size_t>(srow[i]) * s.width + c * 8);
-    }
+      for (int i = 0; i < kChunksPerThread; i++) {
+        const int q = q0 + tid + i * nthr;
+        const int c = q % cpr;
+        v[i] = make_uint4(0, 0, 0, 0);
+        if (srow[i] >= 0)
+          v[i] = *reinterpret_cast<const uint4*>(s.src + static_cast<size_t>(srow[i]) * s.width + c * 8);
+      }
 #pragma unroll
-    for (int i = 0; i < kChunksPerThread; i++) {
-      const int q = threadIdx.x + i * kThreads;
-      if (q < total) store_chunk(dst, q, cpr, v[i]);
+      for (int i = 0; i < kChunksPerThread; i++) {
+        const int q = q0 + tid + i * nthr;
+        if (q < total) store_chunk(dst, q, cpr, v[i]);
+      }
     }
     return;
   }
-  // aggregation: sum of the three edge rows of each cell, in halves of four chunks
-#pragma unroll
-  for (int h = 0; h < kChunksPerThread; h += 4) {
+  // aggregation: sum of the three edge rows of each cell, in rounds of four chunks
+  for (int h = 0; h * nthr < total; h += 4) {
     uint4 w[4][3];
     bool m[4][3];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-      const int q = threadIdx.x + (h + i) * kThreads;
+      const int q = tid + (h + i) * nthr;
       const int row = row0 + q / cpr;
 #pragma unroll
       for (int k = 0; k < 3; k++)
@@ -148,7 +152,7 @@ __device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* d
     }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-      const int q = threadIdx.x + (h + i) * kThreads;
+      const int q = tid + (h + i) * nthr;
       const int row = row0 + q / cpr, c = q % cpr;
 #pragma unroll
       for (int k = 0; k < 3; k++) {
@@ -161,7 +165,7 @@ __device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* d
     }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-      const int q = threadIdx.x + (h + i) * kThreads;
+      const int q = tid + (h + i) * nthr;
       if (q >= total) continue;
       float acc[8];
 #pragma unroll
@@ -242,6 +246,45 @@ __device__ __forceinline__ void stage_matrix(const bf16* src, int nrows, int nco
   }
 }
 
+constexpr int kProducersAsync = 128;
+
+// Asynchronous copy of one 16-byte chunk global -> shared (zero-filled when `valid` is
+// false); the copies of a thread are grouped with commit / wait_group.
+__device__ __forceinline__ void cp_async16(uint8_t* dst, const void* src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(umma::smem_addr(dst)), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Issue (without waiting) the copies of one gathered, non-aggregated segment tile by
+// the 128 producer threads: every thread resolves the source rows of its (at most 16)
+// chunks first, all index loads in flight together, then issues its copies.
+constexpr int kMaxAsyncChunks = 16;  // 128 rows x 16 chunks / 128 threads
+__device__ __forceinline__ void stage_segment_async(const Seg& s, int row0, uint8_t* dst, int tid) {
+  const int cpr = s.width >> 3;
+  const int total = kRows * cpr;
+  int srow[kMaxAsyncChunks];
+#pragma unroll
+  for (int i = 0; i < kMaxAsyncChunks; i++) {
+    const int q = tid + i * kProducersAsync;
+    const int row = row0 + q / cpr;
+    srow[i] = (q < total) ? (s.idx ? s.idx[row] : row) : -1;
+  }
+#pragma unroll
+  for (int i = 0; i < kMaxAsyncChunks; i++) {
+    const int q = tid + i * kProducersAsync;
+    if (q >= total) continue;
+    const int r = q / cpr, c = q - r * cpr;
+    const bf16* src = s.src + static_cast<size_t>(srow[i] >= 0 ? srow[i] : 0) * s.width + c * 8;
+    cp_async16(dst + (c >> 3) * (kRows * 128) + umma::sw128_offset(r, (c & 7) * 8), src, srow[i] >= 0);
+  }
+}
+
 __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
   return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~static_cast<uintptr_t>(1023));
 }
@@ -261,86 +304,143 @@ __device__ __forceinline__ void mma_kmajor(uint32_t tmem_d, uint32_t a, uint32_t
 // ---- forward ----------------------------------------------------------------------
 
 // Shared memory: W1 (128 x k_in), W2 (n_out x 128), two A staging buffers (128 x 128),
-// the hidden tile (128 x 128), bias copies, barriers.
+// the hidden tile (128 x 128), barriers.
 __host__ __device__ constexpr size_t fwd_smem_bytes(int k_in, int n_out) {
   return 1024 + static_cast<size_t>(kHid) * k_in * 2 + static_cast<size_t>(n_out) * kHid * 2 +
          2 * (kRows * 128 * 2) + kRows * kHid * 2 + 256;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) k_mlp_fwd(MlpFwd p) {
+// Warp roles of the forward kernel (288 threads):
+//   warps 0-3  producers: gather each input segment of the CTA's tiles into the
+//              two-buffer staging ring (a buffer is refilled once the MMAs that read
+//              it have completed);
+//   warps 4-7  epilogue: TMEM -> bias + ReLU -> hidden tile, then TMEM -> bias
+//              (+ residual) -> output; warp 4+q reads TMEM lanes 32q..32q+31;
+//   warp 8     one thread issues the MMAs: D1[slot] = A W1^T over the segments, then
+//              D2[slot] = a1 W2^T once the epilogue has written the hidden tile.
+// D1 and D2 are double-buffered in TMEM (slot = tile parity), so the MMAs of tile t+1
+// proceed while the epilogue drains tile t.  Every wait is bounded; a wait that runs
+// out raises the abort flag, which every role polls.
+constexpr int kFwdThreads = 288;
+__device__ __forceinline__ bool aborted(const int* flag) { return *reinterpret_cast<const volatile int*>(flag) != 0; }
+constexpr int kProducers = 128;
+
+__global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(MlpFwd p) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
   uint8_t* w1s = base;
   uint8_t* w2s = w1s + kHid * p.k_in * 2;
   uint8_t* abuf = w2s + p.n_out * kHid * 2;  // 2 x 32 KB
   uint8_t* a1s = abuf + 2 * (kRows * 128 * 2);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(a1s + kRows * kHid * 2);  // [0,1] stage, [2] D1, [3] D2
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(a1s + kRows * kHid * 2);
+  uint64_t* full = bars;        // [2] staging buffer filled (128 producer arrivals)
+  uint64_t* empty = bars + 2;   // [2] MMAs reading the buffer done (commit)
+  uint64_t* d1full = bars + 4;  // [2] D1[slot] complete (commit)
+  uint64_t* a1full = bars + 6;  // hidden tile written (128 epilogue arrivals)
+  uint64_t* d2full = bars + 7;  // [2] D2[slot] complete (commit)
+  uint64_t* tfree = bars + 9;   // [2] epilogue done with D1/D2[slot] (128 arrivals)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 11);
   __shared__ int s_abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int i = 0; i < 4; i++) umma::mbar_init(&bars[i], 1);
+    umma::mbar_init(&full[0], kProducers);
+    umma::mbar_init(&full[1], kProducers);
+    umma::mbar_init(&empty[0], 1);
+    umma::mbar_init(&empty[1], 1);
+    umma::mbar_init(&d1full[0], 1);
+    umma::mbar_init(&d1full[1], 1);
+    umma::mbar_init(a1full, kRows);
+    umma::mbar_init(&d2full[0], 1);
+    umma::mbar_init(&d2full[1], 1);
+    umma::mbar_init(&tfree[0], kRows);
+    umma::mbar_init(&tfree[1], kRows);
     umma::mbar_fence_init();
     s_abort = 0;
   }
-  if (warp == 0) umma::tmem_alloc(tmem_slot, 256);
-  stage_matrix(p.w1, kHid, p.k_in, w1s);
-  stage_matrix(p.w2, p.n_out, kHid, w2s);
+  if (warp == 0) umma::tmem_alloc(tmem_slot, 512);
+  {  // weights, staged by all threads
+    const int cpr1 = p.k_in >> 3, tot1 = kHid * cpr1;
+    for (int q = threadIdx.x; q < tot1; q += kFwdThreads) {
+      const int r = q / cpr1, c = q - r * cpr1;
+      *reinterpret_cast<uint4*>(w1s + (c >> 3) * (kHid * 128) + umma::sw128_offset(r, (c & 7) * 8)) =
+          *reinterpret_cast<const uint4*>(p.w1 + static_cast<size_t>(r) * p.k_in + c * 8);
+    }
+    const int cpr2 = kHid >> 3, tot2 = p.n_out * cpr2;
+    for (int q = threadIdx.x; q < tot2; q += kFwdThreads) {
+      const int r = q / cpr2, c = q - r * cpr2;
+      *reinterpret_cast<uint4*>(w2s + (c >> 3) * (p.n_out * 128) + umma::sw128_offset(r, (c & 7) * 8)) =
+          *reinterpret_cast<const uint4*>(p.w2 + static_cast<size_t>(r) * kHid + c * 8);
+    }
+  }
   umma::fence_async_smem();
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t d1 = tmem, d2 = tmem + 128;
-  const uint32_t w1a = umma::smem_addr(w1s), w2a = umma::smem_addr(w2s);
-  const uint32_t a1a = umma::smem_addr(a1s);
-  const uint32_t idesc1 = umma::idesc_bf16(kRows, kHid, false, false);
-  const uint32_t idesc2 = umma::idesc_bf16(kRows, p.n_out, false, false);
-
-  uint32_t seg_count = 0, tiles_done = 0;
   const int ntiles = p.rows / kRows;
-  const int lane_base = (warp & 3) * 32;
-  const int row_in_tile = lane_base + lane;
-  const int half = warp >> 2;
 
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int row0 = tile * kRows;
-    int kcol = 0;
-    for (int s = 0; s < p.nseg; s++, seg_count++) {
-      const int b = seg_count & 1;
-      if (seg_count >= 2) {
-        if (!umma::mbar_wait(&bars[b], ((seg_count - 2) >> 1) & 1)) s_abort = 1;
+  if (warp < 4) {
+    // ---- producers
+    // Gathered segments are copied with cp.async, keeping the copies of two segments
+    // in flight (a segment is announced once the next one has been issued); the
+    // aggregation segment sums three rows in registers.
+    const int tid = threadIdx.x;
+    uint32_t g = 0;
+    int pending = -1;  // buffer whose cp.async copies are issued but not yet announced
+    for (int tile = blockIdx.x; tile < ntiles && !aborted(&s_abort); tile += gridDim.x) {
+      for (int s = 0; s < p.nseg; s++, g++) {
+        const int b = g & 1;
+        if (g >= 2 && !umma::mbar_wait(&empty[b], ((g >> 1) - 1) & 1)) {
+          s_abort = 1;
+          break;
+        }
+        uint8_t* dst = abuf + b * (kRows * 128 * 2);
+        if (p.seg[s].agg) {
+          if (pending >= 0) {
+            cp_async_wait<0>();
+            umma::fence_async_smem();
+            umma::mbar_arrive(&full[pending]);
+            pending = -1;
+          }
+          stage_segment(p.seg[s], tile * kRows, dst, tid, kProducers);
+          umma::fence_async_smem();
+          umma::mbar_arrive(&full[b]);
+        } else {
+          stage_segment_async(p.seg[s], tile * kRows, dst, tid);
+          cp_async_commit();
+          if (pending >= 0) {
+            cp_async_wait<1>();
+            umma::fence_async_smem();
+            umma::mbar_arrive(&full[pending]);
+          }
+          pending = b;
+        }
       }
-      __syncthreads();
-      if (s_abort) break;
-      uint8_t* dst = abuf + b * (kRows * 128 * 2);
-      stage_segment(p.seg[s], row0, dst);
-      umma::fence_async_smem();
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        umma::fence_after_sync();
-        const uint32_t aa = umma::smem_addr(dst);
-        // W1 columns [kcol, kcol + width): block kcol/64 of W1
-        mma_kmajor(d1, aa, kRows * 128, w1a + (kcol >> 6) * (kHid * 128), kHid * 128, p.seg[s].width,
-                   idesc1, s > 0);
-        umma::commit(&bars[b]);
-      }
-      kcol += p.seg[s].width;
     }
-    if (s_abort) break;
-    if (threadIdx.x == 0) umma::commit(&bars[2]);
-    if (!umma::mbar_wait(&bars[2], tiles_done & 1)) s_abort = 1;
-    __syncthreads();
-    if (s_abort) break;
-    umma::fence_after_sync();
-    // epilogue 1: bias + ReLU -> hidden tile (smem) and optional copy to global
-    {
-      const int r = row_in_tile;
-      for (int cc = 0; cc < 64; cc += 32) {
-        const int col0 = half * 64 + cc;
+    if (pending >= 0) {
+      cp_async_wait<0>();
+      umma::fence_async_smem();
+      umma::mbar_arrive(&full[pending]);
+    }
+  } else if (warp < 8) {
+    // ---- epilogue
+    const int q = warp & 3;
+    const int r = q * 32 + lane;  // row of the tile = TMEM lane
+    const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
+    uint32_t t = 0;
+    for (int tile = blockIdx.x; tile < ntiles && !aborted(&s_abort); tile += gridDim.x, t++) {
+      const int slot = t & 1;
+      const uint32_t d1 = tmem + slot * 128, d2 = tmem + 256 + slot * 128;
+      const size_t row = static_cast<size_t>(tile) * kRows + r;
+      if (!umma::mbar_wait(&d1full[slot], (t >> 1) & 1)) {
+        s_abort = 1;
+        break;
+      }
+      umma::fence_after_sync();
+      for (int col0 = 0; col0 < kHid; col0 += 32) {
         float v[32];
-        umma::tmem_ld32(d1 + (static_cast<uint32_t>(lane_base) << 16) + col0, v);
+        umma::tmem_ld32(d1 + lane_off + col0, v);
         uint4 pk[4];
         bf16* o = reinterpret_cast<bf16*>(pk);
 #pragma unroll
@@ -349,41 +449,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fwd(MlpFwd p) {
         for (int j = 0; j < 4; j++) {
           const int c = col0 + j * 8;
           *reinterpret_cast<uint4*>(a1s + (c >> 6) * (kRows * 128) + umma::sw128_offset(r, c & 63)) = pk[j];
-          if (p.a1_save)
-            *reinterpret_cast<uint4*>(p.a1_save + static_cast<size_t>(row0 + r) * kHid + c) = pk[j];
+          if (p.a1_save) *reinterpret_cast<uint4*>(p.a1_save + row * kHid + c) = pk[j];
         }
       }
-    }
-    umma::fence_async_smem();
-    umma::fence_before_sync();
-    __syncthreads();
-    if (threadIdx.x == 0) {
+      umma::fence_async_smem();
+      umma::fence_before_sync();
+      umma::mbar_arrive(a1full);
+      if (!umma::mbar_wait(&d2full[slot], (t >> 1) & 1)) {
+        s_abort = 1;
+        break;
+      }
       umma::fence_after_sync();
-      mma_kmajor(d2, a1a, kRows * 128, w2a, p.n_out * 128, kHid, idesc2, false);
-      umma::commit(&bars[3]);
-    }
-    if (!umma::mbar_wait(&bars[3], tiles_done & 1)) s_abort = 1;
-    __syncthreads();
-    if (s_abort) break;
-    umma::fence_after_sync();
-    // epilogue 2: bias (+ residual) -> output
-    {
-      const int r = row_in_tile;
-      const int per_half = p.n_out / 2;  // 32 or 64 columns per warp half
-      for (int cc = 0; cc < per_half; cc += 32) {
-        const int col0 = half * per_half + cc;
+      for (int col0 = 0; col0 < p.n_out; col0 += 32) {
         float v[32];
-        umma::tmem_ld32(d2 + (static_cast<uint32_t>(lane_base) << 16) + col0, v);
-        const size_t o0 = static_cast<size_t>(row0 + r) * p.n_out + col0;
+        const size_t o0 = row * p.n_out + col0;
         if (p.res) {
+          uint4 rr[4];
           const uint4* rp = reinterpret_cast<const uint4*>(p.res + o0);
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const uint4 w = rp[j];
-            const bf16* b = reinterpret_cast<const bf16*>(&w);
+          for (int j = 0; j < 4; j++) rr[j] = rp[j];
+          umma::tmem_ld32(d2 + lane_off + col0, v);
 #pragma unroll
-            for (int t = 0; t < 8; t++) v[j * 8 + t] += __bfloat162float(b[t]);
+          for (int j = 0; j < 4; j++) {
+            const bf16* b = reinterpret_cast<const bf16*>(&rr[j]);
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[j * 8 + u] += __bfloat162float(b[u]);
           }
+        } else {
+          umma::tmem_ld32(d2 + lane_off + col0, v);
         }
 #pragma unroll
         for (int j = 0; j < 32; j++) v[j] += p.b2[col0 + j];
@@ -400,21 +493,63 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_fwd(MlpFwd p) {
           for (int j = 0; j < 8; j++) fp[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
         }
       }
+      umma::fence_before_sync();
+      umma::mbar_arrive(&tfree[slot]);
     }
-    umma::fence_before_sync();
-    __syncthreads();
-    tiles_done++;
+  } else if (lane == 0) {
+    // ---- MMA issuer
+    const uint32_t w1a = umma::smem_addr(w1s), w2a = umma::smem_addr(w2s);
+    const uint32_t a1a = umma::smem_addr(a1s);
+    const uint32_t idesc1 = umma::idesc_bf16(kRows, kHid, false, false);
+    const uint32_t idesc2 = umma::idesc_bf16(kRows, p.n_out, false, false);
+    uint32_t g = 0, t = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, t++) {
+      const int slot = t & 1;
+      const uint32_t d1 = tmem + slot * 128, d2 = tmem + 256 + slot * 128;
+      if (t >= 2 && !umma::mbar_wait(&tfree[slot], ((t >> 1) - 1) & 1)) ok = false;
+      int kcol = 0;
+      for (int s = 0; s < p.nseg && ok; s++, g++) {
+        const int b = g & 1;
+        if (!umma::mbar_wait(&full[b], (g >> 1) & 1)) {
+          ok = false;
+          break;
+        }
+        umma::fence_after_sync();
+        mma_kmajor(d1, umma::smem_addr(abuf + b * (kRows * 128 * 2)), kRows * 128,
+                   w1a + (kcol >> 6) * (kHid * 128), kHid * 128, p.seg[s].width, idesc1, s > 0);
+        umma::commit(&empty[b]);
+        kcol += p.seg[s].width;
+      }
+      if (!ok) break;
+      umma::commit(&d1full[slot]);
+      if (!umma::mbar_wait(a1full, t & 1)) {
+        ok = false;
+        break;
+      }
+      umma::fence_after_sync();
+      mma_kmajor(d2, a1a, kRows * 128, w2a, p.n_out * 128, kHid, idesc2, false);
+      umma::commit(&d2full[slot]);
+    }
+    // drain: the last arrivals on the staging barriers before shared memory is released
+    if (ok && g > 0) {
+      const uint32_t uses0 = (g + 1) >> 1, uses1 = g >> 1;
+      if (uses0 > 0 && !umma::mbar_wait(&empty[0], (uses0 - 1) & 1)) ok = false;
+      if (uses1 > 0 && !umma::mbar_wait(&empty[1], (uses1 - 1) & 1)) ok = false;
+    }
+    if (t > 0 && ok) {  // the last D2 of each slot (the epilogue waited for them too)
+      const uint32_t last = t - 1;
+      if (!umma::mbar_wait(&d2full[last & 1], (last >> 1) & 1)) ok = false;
+    }
+    if (!ok) s_abort = 1;
   }
-  // drain: the last arrival of each staging barrier (their MMAs finished before the
-  // last D2 wait, the arrivals may trail it) before shared memory is released
-  if (!s_abort) {
-    const uint32_t uses0 = (seg_count + 1) >> 1, uses1 = seg_count >> 1;
-    if (uses0 > 0 && !umma::mbar_wait(&bars[0], (uses0 - 1) & 1)) s_abort = 1;
-    if (uses1 > 0 && !umma::mbar_wait(&bars[1], (uses1 - 1) & 1)) s_abort = 1;
-  }
-  if (s_abort && threadIdx.x == 0) set_err(p.err, 1);
+  umma::fence_before_sync();
   __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tmem, 256);
+  if (s_abort && threadIdx.x == 0) set_err(p.err, 1);
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, 512);
+  }
 }
 
 // ---- backward: data gradients -------------------------------------------------------
@@ -923,7 +1058,7 @@ int storm_gnn_mlp_forward(const StormGnnMlpFwd* a, int32_t* dev_err, void* strea
   p.out_f32 = a->out_f32; p.a1_save = static_cast<bf16*>(a->a1_save); p.err = dev_err;
   const size_t smem = fwd_smem_bytes(a->k_in, a->n_out);
   cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  k_mlp_fwd<<<grid_for(a->rows), kThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
+  k_mlp_fwd<<<grid_for(a->rows), kFwdThreads, smem, static_cast<cudaStream_t>(stream)>>>(p);
   g_launches++;
   return cuda_check("k_mlp_fwd");
 }
