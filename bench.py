@@ -371,6 +371,31 @@ def run_gnn(args, rank, world, local):
     return 0
 
 
+def warm_start_eval(args, local) -> dict:
+    """The second half of the headline metric: time to steady state per scenario of
+    held-out ensemble members (2k-8k cells, RMS dh < 1e-6), the packaged warm-start
+    network + batched mixed solver against the plain FP64 solver from a cold start
+    (one scenario at a time), plus the batched cold runs."""
+    from storm_b200 import warmstart
+    model = os.path.join(ROOT, "storm_b200", "models", "warmstart_channels.npz")
+    if not os.path.exists(model):
+        return {"unavailable": "no trained model in the package"}
+    net, norm = warmstart.load_model(model, device=f"cuda:{local}")
+    ev = warmstart.evaluate(net, norm, eval_n=args.warm_eval, plain_n=min(4, args.warm_eval), device=local,
+                            reference=False)
+    return {
+        "scenarios": args.warm_eval, "cells": "2000-8000 per scenario", "rstop": 1e-6,
+        "plain_fp64_cold_s_per_scenario": ev["plain_fp64_single"]["wall_s_mean"],
+        "warm_batched_mixed_s_per_scenario": ev["warm_batched_wall_s_per_scenario_incl_network"],
+        "speedup_vs_plain_fp64_cold": ev["speedup_per_scenario_vs_plain_fp64_single_cold"],
+        "iters_mean": {"cold": ev["cold_mixed"]["iters_mean"], "warm": ev["warm_mixed"]["iters_mean"]},
+        "batched_device_ms_per_scenario": {"cold_fp64": ev["cold_fp64"]["device_ms_per_scenario"],
+                                           "cold_mixed": ev["cold_mixed"]["device_ms_per_scenario"],
+                                           "warm_mixed": ev["warm_mixed"]["device_ms_per_scenario"]},
+        "depth_max_abs_warm_vs_cold_fp64_m": ev["depth_err_vs_steady_max_m"]["warm_mixed"],
+    }
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -399,6 +424,8 @@ def main():
                     help="arithmetic of the headline run")
     ap.add_argument("--no-mixed", action="store_true", help="skip the secondary mixed-precision run")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0, help="CPU seconds of the reference arm")
+    ap.add_argument("--warm-eval", type=int, default=16,
+                    help="held-out scenarios of the warm- vs cold-start time-to-steady (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=200, help="iterations of the end-to-end pass")
     ap.add_argument("--kt-steps", type=int, default=5, help="iterations of the per-kernel timing pass")
     args = ap.parse_args()
@@ -594,6 +621,8 @@ def main():
     }
     if other is not None:
         out["other_precision"] = other
+    if rank == 0 and world == 1 and args.warm_eval > 0 and args.config == "meander":
+        out["time_to_steady"] = warm_start_eval(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cv, secs = run_cpu(sc, args.cpu_steps, threads)
