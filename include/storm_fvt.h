@@ -316,6 +316,43 @@ STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, i
  * the state it started from.  `chosen` (may be NULL) receives the four sizes. */
 STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t* chosen);
 
+/*
+ * Boundary data of the output-time vertex pass (Fortran module arrays the host holds
+ * after read_data: walls.f90:170-195 and ibc_arrays.f90:56-135, 181-252, 266-345).
+ * Vectors (TYPE(vector) arrays) are x,y interleaved, 2-D arrays column-major.
+ */
+typedef struct StormFvtOutputBoundary {
+  int32_t n_wall;            /* nodes on solid walls, not on a boundary string        */
+  const int32_t* wall_pts;   /* [n_wall] 1-based                                      */
+  const double* wtangs;      /* [n_wall] unit wall tangents                           */
+  int32_t qin_ld;            /* SIZE(qin_nodes,1)                                     */
+  const int32_t* n_qin;      /* [n_inflowbdr] nodes per inflow string                 */
+  const int32_t* qin_nodes;  /* (qin_ld, n_inflowbdr) 1-based                         */
+  const double* pnormals;    /* (qin_ld, n_inflowbdr) inward unit normals at the nodes */
+  const double* l_inflow;    /* (qin_ld, n_inflowbdr) length of inflow edge i         */
+  const double* qin2;        /* [n_inflowbdr] second velocity component (vtype 3), or NULL */
+  int32_t hbc_ld;            /* SIZE(hbc_nodes,1)                                     */
+  const double* hnormals;    /* (hbc_ld, n_outflowbdr) unit normals at the outflow nodes */
+} StormFvtOutputBoundary;
+
+/*
+ * The output step of the loop (solverFVT.f90:389-405, and :483-487 at exit) on the
+ * device: to_vertices.f90:26-65 (ctr2vtxWSE type 3, the cap, positivity_vtx, the u,v
+ * zeroing of wet cells with a dry vertex, ctr2vtx type 3 of u and v, wetdryvfix,
+ * the dry-vertex zeroing, enforce_bcs.f90:37-171 with vbc_by_h.f90), ctr2vtx of cd
+ * and error_est(2) (error_est.f90).  As in the reference, the zeroing of u,v in the
+ * partially wet cells is applied to the solution, so a run that writes output
+ * continues exactly as the reference's does.  in_loop = 1 for the output at the
+ * select_out iterations inside the loop, which sees the boundary values the last
+ * iteration ran with (get_time_bcs follows it, solverFVT.f90:462); 0 for the output
+ * after the loop, which sees them after the last get_time_bcs.  Outputs (node /
+ * element order, any may be NULL): hvtx, uvtx, vvtx, cdvtx [n_pts], e_est [n_elems].
+ * Single-scenario handles with rkorder >= 2 (the pass reads the last stage's input
+ * depth).
+ */
+STORM_FVT_API int storm_fvt_output_vertices(StormFvtHandle* h, const StormFvtOutputBoundary* ob, int32_t in_loop,
+                                            double* hvtx, double* uvtx, double* vvtx, double* cdvtx, double* e_est);
+
 STORM_FVT_API int storm_fvt_destroy(StormFvtHandle* hd);
 
 /*

@@ -50,6 +50,8 @@ def lib():
         L.orc_get_drycell.argtypes = [C.c_void_p, C.POINTER(C.c_int32)]
         L.orc_stage_probe.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int32)] + \
             [C.POINTER(C.c_double)] * 4
+        L.orc_output_vertices.argtypes = [C.c_void_p, C.POINTER(abi.OutputBoundary), C.c_int] + \
+            [C.POINTER(C.c_double)] * 5
         _lib = L
     return _lib
 
@@ -114,6 +116,15 @@ class Oracle:
         out["hvtx"] = np.empty(N)
         _chk(lib().orc_get_state(self._h, *(abi.dptr(out[k]) for k in
                                            ("h", "u", "v", "rkh", "rku", "rkv", "hvtx"))))
+        return out
+
+    def output_vertices(self, ob: abi.OutputBoundaryHolder, in_loop: bool = True) -> dict:
+        """The reference's output step (orc_output_vertices); zeroes u,v of wet cells
+        with a dry vertex, as the reference does."""
+        out = {k: np.empty(self.N) for k in ("hvtx", "uvtx", "vvtx", "cdvtx")}
+        out["e_est"] = np.empty(self.T)
+        _chk(lib().orc_output_vertices(self._h, C.byref(ob.struct), int(bool(in_loop)),
+                                       *(abi.dptr(out[k]) for k in ("hvtx", "uvtx", "vvtx", "cdvtx", "e_est"))))
         return out
 
     def drycell(self) -> np.ndarray:

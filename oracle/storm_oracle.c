@@ -108,6 +108,7 @@ struct orc {
   double* fedge;           /* interior-edge flux buffer (3, flow_edges1) */
   int32_t* fedge_set;      /* flux computed for this interior edge */
   double cqin3[STORM_MAX_BDR], cqout3[STORM_MAX_BDR];
+  double qin_it[STORM_MAX_BDR], hbc_it[STORM_MAX_BDR]; /* the values the last iteration ran with */
   /* loop state (solverFVT.f90:53-62) */
   int32_t iter, converged, have_state;
   double ttime, stime, delt, rmax, rms, tmass;
@@ -958,6 +959,8 @@ int orc_set_state(orc_t* o, const double* h, const double* u, const double* v) {
   memset(o->delv_x, 0, sizeof(double) * T); memset(o->delv_y, 0, sizeof(double) * T);
   bed_slope_vtx(o);   /* :93 */
   get_time_bcs(o, o->stime); /* :103 */
+  for (int32_t b = 0; b < o->n_in; b++) o->qin_it[b] = o->qin[b];
+  for (int32_t b = 0; b < o->n_out; b++) o->hbc_it[b] = o->hbc[b];
   /* :122-126 */
   int K = o->opt.rkorder;
   for (int32_t i = 1; i <= T; i++) {
@@ -1815,6 +1818,194 @@ static int rk_stage(orc_t* o, int rkstep, int upto, double* delt_io) {
   return bad;
 }
 
+/* ---- output step (solverFVT.f90:389-405, :483-487) ----------------------------- */
+
+/* vbc_by_h.f90:1-98; v_inflow is written to `v_in` [n_qin] */
+static double vbc_by_h(const orc_t* o, const StormFvtOutputBoundary* ob, int32_t ib, const double* wdepth,
+                       double* v_in) {
+  const int32_t n = ob->n_qin[ib - 1];
+  const int32_t ld = ob->qin_ld;
+  double* h_in = (double*)xcalloc((size_t)n + 1, sizeof(double));
+  double* a_in = (double*)xcalloc((size_t)n + 1, sizeof(double));
+  double* u_in = (double*)xcalloc((size_t)n + 1, sizeof(double));
+  for (int32_t i = 1; i <= n; i++) h_in[i - 1] = wdepth[ob->qin_nodes[(ib - 1) * ld + i - 1] - 1];
+  double ht = zero, at = zero;
+  for (int32_t i = 1; i <= n - 1; i++) {
+    a_in[i - 1] = ob->l_inflow[(ib - 1) * ld + i - 1] * (h_in[i - 1] + h_in[i]) * half;
+    ht = ht + (h_in[i - 1] + h_in[i]) * half;
+    at = at + a_in[i - 1];
+  }
+  const double qin = o->qin[ib - 1];
+  for (int32_t i = 1; i <= n - 1; i++) u_in[i - 1] = half * (h_in[i - 1] + h_in[i]) * qin / ht / at;
+  for (int32_t i = 1; i <= n; i++) v_in[i - 1] = zero;
+  for (int32_t i = 2; i <= n - 1; i++)
+    if (h_in[i - 1] > o->opt.h_dry) v_in[i - 1] = half * (u_in[i - 2] + u_in[i - 1]);
+  for (int32_t i = 1; i <= n - 1; i++) u_in[i - 1] = half * (v_in[i - 1] + v_in[i]);
+  double q = zero;
+  for (int32_t i = 1; i <= n - 1; i++) q = q + u_in[i - 1] * a_in[i - 1];
+  for (int32_t i = 2; i <= n - 1; i++)
+    if (h_in[i - 1] > o->opt.h_dry) v_in[i - 1] = v_in[i - 1] * qin / q;
+  for (int32_t i = 1; i <= n - 1; i++) u_in[i - 1] = half * (v_in[i - 1] + v_in[i]);
+  q = zero;
+  for (int32_t i = 1; i <= n - 1; i++) q = q + u_in[i - 1] * a_in[i - 1];
+  free(h_in);
+  free(a_in);
+  free(u_in);
+  return q;
+}
+
+int orc_output_vertices(orc_t* o, const StormFvtOutputBoundary* ob, int in_loop, double* hvtx_out,
+                        double* uvtx_out, double* vvtx_out, double* cdvtx_out, double* e_est_out) {
+  if (!o->have_state) return set_err(STORM_ERR_ARG, "state not set");
+  const int32_t N = o->n_pts, T = o->n_elems;
+  const double h_dry = o->opt.h_dry;
+  double* hv = (double*)xcalloc((size_t)N, sizeof(double));
+  double* uv = (double*)xcalloc((size_t)N, sizeof(double));
+  double* vv = (double*)xcalloc((size_t)N, sizeof(double));
+  /* to_vertices.f90:26-41 with ctr2vtxWSE.f90:89-105 and positivity_vtx.f90:22-27 */
+  for (int32_t i = 1; i <= N; i++) {
+    double id = zero, a = zero;
+    int counter = 0;
+    for (int32_t j = 2; j <= N2T(i, 1) + 1; j++) {
+      int32_t k = N2T(i, j);
+      if (DRY(k)) continue;
+      counter++;
+      id = id + C2VW(i, j - 1);
+      a = a + C2VW(i, j - 1) * ZETA(k);
+    }
+    double zv = counter > 0 ? a / id : ZVTX(i);
+    double zetaref = ZVTX(i);
+    for (int32_t j = 2; j <= N2T(i, 1) + 1; j++) {
+      int32_t k = N2T(i, j);
+      if (DRY(k)) continue;
+      zetaref = fmax2(ZETA(k), zetaref);
+    }
+    zv = fmin2(zv, zetaref);
+    hv[i - 1] = zv - ZVTX(i);
+    if (hv[i - 1] < zero) hv[i - 1] = zero;
+  }
+  /* to_vertices.f90:44-55: applied to the solution */
+  for (int32_t i = 1; i <= T; i++) {
+    if (DRY(i)) continue;
+    int flag = 1;
+    for (int j = 1; j <= 3; j++) flag = flag && (hv[GV(i, j) - 1] > h_dry);
+    if (!flag) { U(i) = zero; V(i) = zero; }
+  }
+  /* :56-62 */
+  ctr2vtx3(o, o->u, uv);
+  ctr2vtx3(o, o->v, vv);
+  if (o->opt.btype == 0) /* wetdryvfix.f90:26-46 */
+    for (int32_t i = 1; i <= N; i++) {
+      int wett = 0, dryt = 0;
+      for (int32_t j = 2; j <= N2T(i, 1) + 1; j++) {
+        if (DRY(N2T(i, j))) dryt = 1;
+        else wett = 1;
+      }
+      if (wett && dryt) { uv[i - 1] = zero; vv[i - 1] = zero; }
+    }
+  for (int32_t i = 1; i <= N; i++)
+    if (hv[i - 1] < h_dry) { uv[i - 1] = zero; vv[i - 1] = zero; }
+  /* enforce_bcs.f90:37-171 */
+  for (int32_t b = 1; b <= o->n_out; b++) {
+    const int32_t ht = o->htype[b - 1];
+    const double* hn = ob->hnormals + 2 * (size_t)(b - 1) * ob->hbc_ld;
+    if (ht == 1) {
+      for (int32_t i = 1; i <= o->n_hbc[b - 1]; i++) {
+        int32_t j = HBC_NODES(i, b);
+        const double hbc = in_loop ? o->hbc_it[b - 1] : o->hbc[b - 1];
+        double hnot = fmax2(zero, hbc - ZVTX(j));
+        double incr = 0.100 * (hnot - hv[j - 1]);
+        if (fabs(incr) < 0.0100) incr = hnot - hv[j - 1];
+        hv[j - 1] = hv[j - 1] - incr;
+        hv[j - 1] = fmax2(zero, hbc - ZVTX(j));
+      }
+      if (o->opt.hvalve)
+        for (int32_t i = 1; i <= o->n_hbc[b - 1]; i++) {
+          int32_t j = HBC_NODES(i, b);
+          double dot = uv[j - 1] * hn[2 * (i - 1)] + vv[j - 1] * hn[2 * (i - 1) + 1];
+          if (dot < zero) { uv[j - 1] = zero; vv[j - 1] = zero; }
+        }
+    } else if (ht == 0) {
+      for (int32_t i = 1; i <= o->n_hbc[b - 1]; i++) {
+        int32_t j = HBC_NODES(i, b);
+        double dot = uv[j - 1] * hn[2 * (i - 1)] + vv[j - 1] * hn[2 * (i - 1) + 1];
+        if (dot < zero) { uv[j - 1] = zero; vv[j - 1] = zero; }
+      }
+    }
+  }
+  if (o->opt.btype == 0) {
+    for (int32_t i = 1; i <= ob->n_wall; i++) {
+      int32_t p = ob->wall_pts[i - 1];
+      uv[p - 1] = zero;
+      vv[p - 1] = zero;
+    }
+  } else {
+    for (int32_t i = 1; i <= ob->n_wall; i++) {
+      int32_t p = ob->wall_pts[i - 1];
+      double tx = ob->wtangs[2 * (i - 1)], ty = ob->wtangs[2 * (i - 1) + 1];
+      double dot = uv[p - 1] * tx + vv[p - 1] * ty;
+      uv[p - 1] = dot * tx;
+      vv[p - 1] = dot * ty;
+    }
+  }
+  for (int32_t i = 1; i <= N; i++)
+    if (hv[i - 1] < h_dry) { uv[i - 1] = zero; vv[i - 1] = zero; }
+  double qin_save[STORM_MAX_BDR];
+  for (int32_t b = 0; b < o->n_in; b++) {
+    qin_save[b] = o->qin[b];
+    if (in_loop) o->qin[b] = o->qin_it[b];
+  }
+  for (int32_t b = 1; b <= o->n_in; b++) {
+    const int32_t vt = o->vtype[b - 1], n = ob->n_qin[b - 1];
+    const int32_t* qn = ob->qin_nodes + (size_t)(b - 1) * ob->qin_ld;
+    const double* pn = ob->pnormals + 2 * (size_t)(b - 1) * ob->qin_ld;
+    if (vt == 0) {
+      for (int32_t i = 1; i <= n; i++)
+        if (hv[qn[i - 1] - 1] > h_dry) {
+          uv[qn[i - 1] - 1] = o->qin[b - 1] * pn[2 * (i - 1)];
+          vv[qn[i - 1] - 1] = o->qin[b - 1] * pn[2 * (i - 1) + 1];
+        }
+    } else if (vt == 1 || vt == 5) {
+      double* v_in = (double*)xcalloc((size_t)n + 1, sizeof(double));
+      (void)vbc_by_h(o, ob, b, hv, v_in);
+      for (int32_t i = 1; i <= n; i++)
+        if (hv[qn[i - 1] - 1] > h_dry) {
+          uv[qn[i - 1] - 1] = v_in[i - 1] * pn[2 * (i - 1)];
+          vv[qn[i - 1] - 1] = v_in[i - 1] * pn[2 * (i - 1) + 1];
+        }
+      free(v_in);
+    } else if (vt == 3) {
+      for (int32_t i = 1; i <= n; i++)
+        if (hv[qn[i - 1] - 1] > h_dry) {
+          uv[qn[i - 1] - 1] = o->qin[b - 1];
+          vv[qn[i - 1] - 1] = ob->qin2 ? ob->qin2[b - 1] : zero;
+        }
+    }
+  }
+  for (int32_t b = 0; b < o->n_in; b++) o->qin[b] = qin_save[b];
+  if (hvtx_out) memcpy(hvtx_out, hv, sizeof(double) * N);
+  if (uvtx_out) memcpy(uvtx_out, uv, sizeof(double) * N);
+  if (vvtx_out) memcpy(vvtx_out, vv, sizeof(double) * N);
+  if (cdvtx_out) ctr2vtx3(o, o->cd, cdvtx_out);
+  if (e_est_out) /* error_est.f90, etype 2 */
+    for (int32_t i = 1; i <= T; i++) {
+      e_est_out[i - 1] = zero;
+      if (H(i) < h_dry) continue;
+      int32_t n1 = GV(i, 1), n2 = GV(i, 2), n3 = GV(i, 3);
+      double gzx = (ZVTX(n1) * (NY(n2) - NY(n3)) + ZVTX(n2) * (NY(n3) - NY(n1)) + ZVTX(n3) * (NY(n1) - NY(n2))) *
+                   half / AREA(i);
+      double gzy = (ZVTX(n1) * (NX(n3) - NX(n2)) + ZVTX(n2) * (NX(n1) - NX(n3)) + ZVTX(n3) * (NX(n2) - NX(n1))) *
+                   half / AREA(i);
+      double l = PERIM(i) * ONE_THIRD;
+      double gx = gzx + o->delh_x[i - 1], gy = gzy + o->delh_y[i - 1];
+      e_est_out[i - 1] = sqrt(gx * gx + gy * gy) * l / (Z(i) + H(i));
+    }
+  free(hv);
+  free(uv);
+  free(vv);
+  return 0;
+}
+
 /* The main loop body, solverFVT.f90:129-476, `nsteps` times. */
 int orc_step(orc_t* o, int nsteps, StormFvtStepStats* st) {
   if (!o->have_state) return set_err(STORM_ERR_ARG, "state not set");
@@ -1875,6 +2066,8 @@ int orc_step(orc_t* o, int nsteps, StormFvtStepStats* st) {
     } else {
       o->stime = o->stime + o->delt;
       o->rmax = rmax_phi;
+      for (int32_t b = 0; b < o->n_in; b++) o->qin_it[b] = o->qin[b];
+      for (int32_t b = 0; b < o->n_out; b++) o->hbc_it[b] = o->hbc[b];
       get_time_bcs(o, o->stime);
     }
   }

@@ -44,6 +44,12 @@ int orc_get_state(const orc_t* o, double* h, double* u, double* v, double* rkh,
 /* drycell as find_dry_cells would set it for the next stage (int32 0/1). */
 int orc_get_drycell(orc_t* o, int32_t* dry);
 
+/* The output step of solverFVT (to_vertices, ctr2vtx(cd), error_est(2)) after the
+ * last completed iteration; zeroes u,v of wet cells with a dry vertex as the reference
+ * does.  Output pointers may be NULL. */
+int orc_output_vertices(orc_t* o, const StormFvtOutputBoundary* ob, int in_loop, double* hvtx, double* uvtx,
+                        double* vvtx, double* cdvtx, double* e_est);
+
 /* Debug hooks: run only the first `upto` phases of one RK stage (rkstep) from the
  * current state and copy out intermediates.  Phases: 1 = dry cells, 2 = gradients
  * + hgradfix2, 3 = to_vertices, 4 = fluxes + bed slope.  Pointers may be NULL.

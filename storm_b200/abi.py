@@ -255,3 +255,144 @@ def mesh_to_numpy(m: Mesh) -> dict:
                  "tsh_ld", "bch_max"):
         d[name] = getattr(m, name)
     return d
+
+
+class OutputBoundary(C.Structure):
+    """StormFvtOutputBoundary: boundary arrays of the output-time vertex pass."""
+    _fields_ = [
+        ("n_wall", C.c_int32), ("wall_pts", _i), ("wtangs", _d), ("qin_ld", C.c_int32),
+        ("n_qin", _i), ("qin_nodes", _i), ("pnormals", _d), ("l_inflow", _d), ("qin2", _d),
+        ("hbc_ld", C.c_int32), ("hnormals", _d),
+    ]
+
+
+class OutputBoundaryHolder:
+    """The arrays the reference builds after read_data for enforce_bcs at output time,
+    from a prepared mesh (``mesh_to_numpy``) and the problem's boundary strings:
+
+    * ``wall_pts`` -- walls.f90:170-195: the nodes of the wall edges, in walledg1
+      order, without repetitions and without nodes of any boundary string;
+    * ``pnormals``/``l_inflow`` -- ibc_arrays.f90:59-135: per inflow string, the
+      inward normal of edge i (between nodes i and i+1), moved to the nodes (node n
+      takes edge n-1; node i, 1 < i < n, the sum of edges i-1 and i), normalised;
+    * ``hnormals`` -- ibc_arrays.f90:181-252 and ``wtangs`` -- :266-345: the sum of
+      the outward normals of the two boundary edges at the node, normalised (for
+      walls then turned by 90 degrees into a tangent).
+
+    ibc_arrays runs before dataprepFVT normalises the edge normals, so the sums use
+    normals of edge-length magnitude; the prepared mesh stores unit normals, which
+    are scaled back by the edge length here."""
+
+    def __init__(self, problem: "ProblemHolder", mn: dict):
+        T, E = int(mn["n_elems"]), int(mn["n_edges"])
+        ep = mn["edge_p"].reshape(E, 2).astype(np.int64)
+        ee = mn["edge_e"].reshape(E, 2).astype(np.int64)
+        nrm = mn["edge_normal"].reshape(E, 2) * mn["edge_length"][:, None]
+        tedge = mn["tri_edge"].reshape(T, 3).astype(np.int64)
+        key = {}
+        for e in range(E):
+            a, b = int(ep[e, 0]), int(ep[e, 1])
+            key.setdefault((min(a, b), max(a, b)), e + 1)
+
+        def elem_of(e):
+            t = int(ee[e - 1, 0])
+            return t if t > 0 else int(ee[e - 1, 1])
+
+        def sign_in(e, t):
+            for k in tedge[t - 1]:
+                if abs(int(k)) == e:
+                    return 1 if k > 0 else -1
+            raise ValueError("edge not in its element")
+
+        def unit(v):
+            length = np.sqrt(v[0] * v[0] + v[1] * v[1])
+            return np.array([v[0] / length, v[1] / length])
+
+        # boundary edges and, per node, the first two of them (bpolygon order: edge id)
+        bnd = [e + 1 for e in range(E) if ee[e, 0] <= 0 or ee[e, 1] <= 0]
+        at_node = {}
+        for e in bnd:
+            for p in ep[e - 1]:
+                lst = at_node.setdefault(int(p), [])
+                if len(lst) < 2:
+                    lst.append(e)
+
+        def outward_sum(p):
+            es = at_node.get(int(p), [])
+            if len(es) < 2:
+                es = (es + es)[:2] if es else []
+            if not es:
+                return np.zeros(2)
+            s = np.zeros(2)
+            acc = []
+            for e in es:
+                sg = sign_in(e, elem_of(e))
+                acc.append(nrm[e - 1] * (1.0 if sg > 0 else -1.0))
+            s = np.array([acc[0][0] + acc[1][0], acc[0][1] + acc[1][1]])
+            return unit(s)
+
+        ins = problem.inflow_spec
+        qin_nodes_all = set(int(p) for b in ins for p in b["nodes"])
+        n_out = int(mn["n_outflowbdr"])
+        hld = max(int(mn["hbc_ld"]), 1)
+        hbc_nodes = mn["hbc_nodes"].reshape(max(n_out, 0), -1) if n_out else np.zeros((0, hld), np.int32)
+        n_hbc = mn["n_hbc"]
+        hbc_all = set(int(hbc_nodes[b, i]) for b in range(n_out) for i in range(int(n_hbc[b])))
+        # walls.f90:170-195
+        wall = []
+        seen = set()
+        for e in mn["walledg1"]:
+            for p in ep[int(e) - 1]:
+                p = int(p)
+                if p not in seen and p not in qin_nodes_all and p not in hbc_all:
+                    seen.add(p)
+                    wall.append(p)
+        self.wall_pts = np.array(wall, dtype=np.int32)
+        wt = np.zeros((len(wall), 2))
+        for i, p in enumerate(wall):
+            u = outward_sum(p)
+            wt[i] = [-u[1], u[0]]
+        self.wtangs = np.ascontiguousarray(wt.reshape(-1))
+        # ibc_arrays.f90:59-135
+        n_in = len(ins)
+        self.qin_ld = max([len(b["nodes"]) for b in ins] + [1])
+        self.n_qin = np.array([len(b["nodes"]) for b in ins] + [0], dtype=np.int32)[:max(n_in, 1)]
+        qn = np.zeros((max(n_in, 1), self.qin_ld), dtype=np.int32)
+        pn = np.zeros((max(n_in, 1), self.qin_ld, 2))
+        lin = np.zeros((max(n_in, 1), self.qin_ld))
+        for b, spec in enumerate(ins):
+            nodes = [int(p) for p in spec["nodes"]]
+            n = len(nodes)
+            qn[b, :n] = nodes
+            for i in range(n - 1):
+                a, c = nodes[i], nodes[i + 1]
+                e = key[(min(a, c), max(a, c))]
+                sg = sign_in(e, elem_of(e))
+                pn[b, i] = -nrm[e - 1] if sg > 0 else nrm[e - 1]
+                lin[b, i] = mn["edge_length"][e - 1]
+            if n > 1:
+                pn[b, n - 1] = pn[b, n - 2]
+            for i in range(n - 2, 0, -1):
+                pn[b, i] = [pn[b, i, 0] + pn[b, i - 1, 0], pn[b, i, 1] + pn[b, i - 1, 1]]
+            for i in range(n):
+                pn[b, i] = unit(pn[b, i])
+        self.qin_nodes = np.ascontiguousarray(qn.reshape(-1))
+        self.pnormals = np.ascontiguousarray(pn.reshape(-1))
+        self.l_inflow = np.ascontiguousarray(lin.reshape(-1))
+        self.qin2 = np.zeros(max(n_in, 1))
+        # ibc_arrays.f90:181-252
+        self.hbc_ld = hld
+        hn = np.zeros((max(n_out, 1), hld, 2))
+        for b in range(n_out):
+            for i in range(int(n_hbc[b])):
+                hn[b, i] = outward_sum(hbc_nodes[b, i])
+        self.hnormals = np.ascontiguousarray(hn.reshape(-1))
+        s = OutputBoundary()
+        s.n_wall = len(wall)
+        s.wall_pts = iptr(self.wall_pts) if len(wall) else None
+        s.wtangs = dptr(self.wtangs) if len(wall) else None
+        s.qin_ld = self.qin_ld
+        s.n_qin, s.qin_nodes = iptr(self.n_qin), iptr(self.qin_nodes)
+        s.pnormals, s.l_inflow, s.qin2 = dptr(self.pnormals), dptr(self.l_inflow), dptr(self.qin2)
+        s.hbc_ld, s.hnormals = self.hbc_ld, dptr(self.hnormals)
+        self.struct = s

@@ -71,6 +71,9 @@ struct StormFvtHandle {
   int64_t kt_n[8] = {0};
   // block sizes of the stage kernels (storm_fvt_autotune picks them)
   int bs_node = 256, bs_grad = 256, bs_eflux = 128, bs_flux = 128;
+  // output pass (storm_fvt_output_vertices): device buffers, allocated at first use
+  void* out_buf = nullptr;
+  size_t out_bytes = 0;
 };
 
 namespace {
@@ -242,6 +245,7 @@ void release(StormFvtHandle* h) {
   if (h->arena) cudaFree(h->arena);
   if (h->arena32) cudaFree(h->arena32);
   if (h->sc_host) cudaFreeHost(h->sc_host);
+  if (h->out_buf) cudaFree(h->out_buf);
   delete h;
 }
 
@@ -297,6 +301,7 @@ int upload(StormFvtHandle* h) {
   size_t o_g[6];
   for (int i = 0; i < 6; i++) o_g[i] = A.take(8 * (size_t)T);
   size_t o_dra = A.take(T), o_drb = A.take(T), o_hv = A.take(8 * (size_t)N), o_vw = A.take(N);
+  size_t o_dro = A.take(T);
   size_t o_pm = A.take(8 * (size_t)T), o_bcc3 = A.take(8 * 3 * nbce), o_rec = A.take(8 * 3 * nbce);
   size_t o_part = A.take(8 * 8 * (size_t)nblk), o_sc = A.take(sizeof(Scalars) * (size_t)h->nscen);
   size_t o_efx = A.take(8 * 3 * ne1), o_eok = A.take(ne1);
@@ -355,6 +360,7 @@ int upload(StormFvtHandle* h) {
   d.delh_x = at<double>(B, o_g[0]); d.delh_y = at<double>(B, o_g[1]); d.delu_x = at<double>(B, o_g[2]);
   d.delu_y = at<double>(B, o_g[3]); d.delv_x = at<double>(B, o_g[4]); d.delv_y = at<double>(B, o_g[5]);
   d.dry_a = at<uint8_t>(B, o_dra); d.dry_b = at<uint8_t>(B, o_drb); d.hvtx = at<double>(B, o_hv);
+  d.dry_out = at<uint8_t>(B, o_dro);
   d.vwet = at<uint8_t>(B, o_vw); d.phimax = at<double>(B, o_pm); d.bc_c = at<double>(B, o_bcc3);
   d.bc_rec = at<double>(B, o_rec); d.part = at<double>(B, o_part); d.nblk_red = nblk;
   d.sc = at<Scalars>(B, o_sc);
@@ -716,6 +722,140 @@ int storm_fvt_get_state(StormFvtHandle* h, double* hh, double* u, double* v, dou
   if (h && h->nscen != 1)
     return set_error(STORM_ERR_ARG, "storm_fvt_get_state: batched handle, use storm_fvt_get_scenario_state");
   return storm_fvt_get_scenario_state(h, 0, hh, u, v, rkh, rku, rkv, hvtx);
+}
+
+int storm_fvt_output_vertices(StormFvtHandle* h, const StormFvtOutputBoundary* ob, int32_t in_loop, double* hvtx,
+                              double* uvtx, double* vvtx, double* cdvtx, double* e_est) {
+  clear_error();
+  if (!h || !ob) return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: null argument");
+  if (h->nscen != 1) return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: batched handle");
+  if (!h->have_state) return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: state not set");
+  if (h->d.K < 2)
+    return set_error(STORM_ERR_UNSUPPORTED, "storm_fvt_output_vertices: needs rkorder >= 2 (the last stage's input)");
+  CK(cudaSetDevice(h->device));
+  const HostLayout& P = h->parts[0];
+  const int N = P.N, T = P.T;
+  const Scalars& sc = h->sc_host[0];  // boundary values of the last completed iteration
+  // boundary lists in the device numbering
+  std::vector<int32_t> iv;   // wall nodes | outflow nodes | out_off | out_type | inflow nodes | in_off | in_type
+  std::vector<double> dv;    // wtang | hn | hbc | pn | lin | qin | qin2
+  if (ob->n_wall < 0 || (ob->n_wall > 0 && (!ob->wall_pts || !ob->wtangs)))
+    return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: wall arrays missing");
+  auto node_of = [&](int32_t p, int32_t* out) -> bool {
+    if (p < 1 || p > N) return false;
+    *out = P.node_new[p - 1];
+    return true;
+  };
+  const size_t i_wall = iv.size();
+  for (int32_t i = 0; i < ob->n_wall; i++) {
+    int32_t q;
+    if (!node_of(ob->wall_pts[i], &q)) return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: wall node out of range");
+    iv.push_back(q);
+  }
+  const size_t d_wt = dv.size();
+  for (int32_t i = 0; i < 2 * ob->n_wall; i++) dv.push_back(ob->wtangs[i]);
+  const int n_out = P.n_out;
+  const size_t i_onode = iv.size();
+  iv.insert(iv.end(), P.out_node.begin(), P.out_node.end());
+  const size_t i_ooff = iv.size();
+  iv.insert(iv.end(), P.out_off.begin(), P.out_off.end());
+  const size_t i_otype = iv.size();
+  for (int b = 0; b < n_out; b++) iv.push_back(P.out_type[b]);
+  const size_t d_hn = dv.size();
+  if (n_out > 0 && (!ob->hnormals || ob->hbc_ld < 1))
+    return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: hnormals missing");
+  for (int b = 0; b < n_out; b++)
+    for (int i = 0; i < P.out_off[b + 1] - P.out_off[b]; i++) {
+      if (i >= ob->hbc_ld) return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: hbc_ld too small");
+      dv.push_back(ob->hnormals[2 * ((size_t)b * ob->hbc_ld + i)]);
+      dv.push_back(ob->hnormals[2 * ((size_t)b * ob->hbc_ld + i) + 1]);
+    }
+  const size_t d_hbc = dv.size();
+  for (int b = 0; b < n_out; b++) dv.push_back(in_loop ? sc.hbc_it[b] : sc.hbc[b]);
+  const int n_in = P.n_in;
+  if (n_in > 0 && (!ob->n_qin || !ob->qin_nodes || !ob->pnormals || !ob->l_inflow || ob->qin_ld < 1))
+    return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: inflow arrays missing");
+  const size_t i_inode = iv.size();
+  std::vector<int32_t> in_off(1, 0);
+  const size_t d_pn0 = dv.size();
+  std::vector<double> pn, lin;
+  for (int b = 0; b < n_in; b++) {
+    const int32_t n = ob->n_qin[b];
+    if (n < 0 || n > ob->qin_ld) return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: n_qin out of range");
+    for (int32_t i = 0; i < n; i++) {
+      int32_t q;
+      if (!node_of(ob->qin_nodes[(size_t)b * ob->qin_ld + i], &q))
+        return set_error(STORM_ERR_ARG, "storm_fvt_output_vertices: inflow node out of range");
+      iv.push_back(q);
+      pn.push_back(ob->pnormals[2 * ((size_t)b * ob->qin_ld + i)]);
+      pn.push_back(ob->pnormals[2 * ((size_t)b * ob->qin_ld + i) + 1]);
+      lin.push_back(ob->l_inflow[(size_t)b * ob->qin_ld + i]);
+    }
+    in_off.push_back(in_off.back() + n);
+  }
+  (void)d_pn0;
+  const size_t i_ioff = iv.size();
+  iv.insert(iv.end(), in_off.begin(), in_off.end());
+  const size_t i_itype = iv.size();
+  for (int b = 0; b < n_in; b++) iv.push_back(P.in_type[b]);
+  const size_t d_pn = dv.size();
+  dv.insert(dv.end(), pn.begin(), pn.end());
+  const size_t d_lin = dv.size();
+  dv.insert(dv.end(), lin.begin(), lin.end());
+  const size_t d_qin = dv.size();
+  for (int b = 0; b < n_in; b++) dv.push_back(in_loop ? sc.qin_it[b] : sc.qin[b]);
+  const size_t d_qin2 = dv.size();
+  for (int b = 0; b < n_in; b++) dv.push_back(ob->qin2 ? ob->qin2[b] : 0.0);
+  iv.push_back(0);
+  dv.push_back(0.0);
+  // device buffer: outputs (hv, uv, vv, cdv [N], e_est [T]) then the lists
+  const size_t out_d = 8 * (4 * (size_t)h->d.N + (size_t)h->d.T);
+  const size_t need = out_d + 8 * dv.size() + 4 * iv.size() + 256;
+  if (need > h->out_bytes) {
+    if (h->out_buf) cudaFree(h->out_buf);
+    h->out_buf = nullptr;
+    h->out_bytes = 0;
+    cudaError_t e = cudaMalloc(&h->out_buf, need);
+    if (e != cudaSuccess) return set_error(STORM_ERR_NOMEM, "storm_fvt_output_vertices: device allocation failed");
+    h->out_bytes = need;
+  }
+  char* base = static_cast<char*>(h->out_buf);
+  double* dd = reinterpret_cast<double*>(base + out_d);
+  int32_t* di = reinterpret_cast<int32_t*>(base + out_d + 8 * dv.size());
+  CK(cudaMemcpyAsync(dd, dv.data(), 8 * dv.size(), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(di, iv.data(), 4 * iv.size(), cudaMemcpyHostToDevice, h->stream));
+  OutputArgs a{};
+  a.hv = reinterpret_cast<double*>(base);
+  a.uv = a.hv + h->d.N;
+  a.vv = a.uv + h->d.N;
+  a.cdv = a.vv + h->d.N;
+  a.e_est = a.cdv + h->d.N;
+  a.n_out = n_out;
+  a.out_node = di + i_onode; a.out_off = di + i_ooff; a.out_type = di + i_otype;
+  a.hn = dd + d_hn; a.hbc = dd + d_hbc;
+  a.n_wall = ob->n_wall; a.wall_node = di + i_wall; a.wtang = dd + d_wt;
+  a.n_in = n_in;
+  a.in_node = di + i_inode; a.in_off = di + i_ioff; a.in_type = di + i_itype;
+  a.pn = dd + d_pn; a.lin = dd + d_lin; a.qin = dd + d_qin; a.qin2 = dd + d_qin2;
+  launch_output(h->d, h->gd, h->gf, h->mixed, a, h->stream);
+  h->launches += 4 + (n_out > 0) + (ob->n_wall > 0) + (n_in > 0) + ((!h->opt.steady && h->opt.dt_op == 1) ? 2 : 0);
+  CK(cudaGetLastError());
+  // results in element / node order
+  std::vector<double> buf(std::max(N, T));
+  auto pull = [&](const double* dev, double* dst, int n, const std::vector<int32_t>& perm) -> int {
+    if (!dst) return 0;
+    CK(cudaMemcpyAsync(buf.data(), dev, 8 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < n; k++) dst[perm[k]] = buf[k];
+    return 0;
+  };
+  int rc;
+  if ((rc = pull(a.hv, hvtx, N, P.node_old)) || (rc = pull(a.uv, uvtx, N, P.node_old)) ||
+      (rc = pull(a.vv, vvtx, N, P.node_old)) || (rc = pull(a.cdv, cdvtx, N, P.node_old)) ||
+      (rc = pull(a.e_est, e_est, T, P.cell_old)))
+    return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return STORM_OK;
 }
 
 int storm_fvt_get_drycell(StormFvtHandle* h, int32_t* dry) {

@@ -28,6 +28,7 @@ struct Scalars {
   double ttime, stime, rmax, rms, tmass;
   double qin[kMaxBdrDev], hbc[kMaxBdrDev];
   double cqin3[kMaxBdrDev], cqout3[kMaxBdrDev];
+  double qin_it[kMaxBdrDev], hbc_it[kMaxBdrDev];  // values the last iteration ran with
   double bch_max;               // dataprepFVT.f90:278-286
   // static: boundary series and the scenario's ranges in the merged arrays
   int32_t n_in, n_out;
@@ -75,6 +76,7 @@ struct Dev {
   double *u_b, *v_b;        // velocities after hgradfix2 / to_vertices zeroing (fluxes)
   double *delh_x, *delh_y, *delu_x, *delu_y, *delv_x, *delv_y;
   uint8_t *dry_a, *dry_b;   // stage dry flags (ping-pong)
+  uint8_t* dry_out;         // find_dry_cells before the friction step (the output pass)
   double* hvtx;             // vertex depth after enforce_bcs (wall fluxes, output)
   uint8_t* vwet;            // hvtx > h_dry before enforce_bcs (to_vertices.f90:44-55)
   double* phimax;           // MAX(|phi|) of the last stage (stop criterion)
@@ -112,5 +114,23 @@ struct StageLaunch {
 };
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed);
 void set_bc_smem_limit(int bytes);
+
+// The output pass (to_vertices, ctr2vtx of cd, error_est(2)) after an iteration.
+struct OutputArgs {
+  // outflow strings: nodes [out_off[b], out_off[b+1]) of out_node, unit normals hn[2*i]
+  int32_t n_out;
+  const int32_t *out_node, *out_off, *out_type;
+  const double *hn, *hbc;
+  int32_t n_wall;
+  const int32_t* wall_node;
+  const double* wtang;
+  // inflow strings: nodes [in_off[b], in_off[b+1]) of in_node, normals pn, lengths lin
+  int32_t n_in;
+  const int32_t *in_node, *in_off, *in_type;
+  const double *pn, *lin, *qin, *qin2;
+  double *hv, *uv, *vv, *cdv, *e_est;  // outputs (device, new numbering)
+};
+void launch_output(const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed, const OutputArgs& a,
+                   cudaStream_t st);
 
 }  // namespace storm

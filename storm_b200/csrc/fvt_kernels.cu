@@ -346,6 +346,10 @@ __global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int sid) {
       sc->cqout3[b] = kZero;
     }
     time_bcs(d, sid, kZero);
+    for (int b = 0; b < kMaxBdrDev; b++) {
+      sc->qin_it[b] = sc->qin[b];
+      sc->hbc_it[b] = sc->hbc[b];
+    }
     if (d.steady) sc->delt = kZero;  // delt is first set inside the RK loop
     else sc->delt = (d.dt_op == 0) ? d.cfl : dtmin;
   }
@@ -1178,6 +1182,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
     const double h0 = d.rkh[c];  // rkh(i,0), the iteration's starting depth
     double um;
     const bool dry2 = dry_flag(h, u, v, d.h_dry, d.h_wet, &um);
+    d.dry_out[c] = dry2;
     const double cd = d.cd[c];
     double rough = kZero;
     switch (d.fric) {
@@ -1295,9 +1300,254 @@ __global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
     } else {
       sc->stime = sc->stime + sc->delt;
       sc->rmax = rmax_phi;
+      for (int b = 0; b < kMaxBdrDev; b++) {
+        sc->qin_it[b] = sc->qin[b];
+        sc->hbc_it[b] = sc->hbc[b];
+      }
       time_bcs(d, sid, sc->stime);
       sc->delt = (d.dt_op == 0) ? d.cfl : dtmin;
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The output pass of solverFVT.f90:389-405 (to_vertices.f90:26-65, ctr2vtx.f90:69-80,
+// wetdryvfix.f90, enforce_bcs.f90:37-171, vbc_by_h.f90, error_est.f90 etype 2) after
+// an iteration.  The depths come from zeta of the last stage's start (solverFVT.f90:169
+// is the only assignment of zeta) and the dry flags of the find_dry_cells call before
+// the friction step (:335), as in the reference.
+
+// to_vertices.f90:26-41: ctr2vtxWSE type 3, cap, positivity_vtx
+__global__ void __launch_bounds__(256) k_out_depth(Dev d, OutputArgs a) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N) return;
+  const double* hs = d.rkh + (size_t)(d.K - 1) * d.T;
+  const int b0 = d.n2t_off[n], b1 = d.n2t_off[n + 1];
+  const double zv0 = d.zvtx[n];
+  double id = kZero, s = kZero, zetaref = zv0;
+  int counter = 0;
+  for (int q = b0; q < b1; q++) {
+    const int k = d.n2t_cell[q];
+    if (d.dry_out[k]) continue;
+    const double zeta = hs[k] + d.z[k];
+    counter++;
+    id = id + d.n2t_w[q];
+    s = s + d.n2t_w[q] * zeta;
+  }
+  double zv = counter > 0 ? s / id : zv0;
+  for (int q = b0; q < b1; q++) {
+    const int k = d.n2t_cell[q];
+    if (d.dry_out[k]) continue;
+    zetaref = fmax2(hs[k] + d.z[k], zetaref);
+  }
+  zv = fmin2(zv, zetaref);
+  double hv = zv - zv0;
+  if (hv < kZero) hv = kZero;
+  a.hv[n] = hv;
+}
+
+// to_vertices.f90:44-55 on the solution (and the next stage's dry flag of a cell whose
+// velocity it zeroes), error_est.f90 etype 2
+template <class R>
+__global__ void __launch_bounds__(256) k_out_cell(Dev d, Geo<R> G, OutputArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.T || d.cell_sid[c] < 0) return;
+  const int T = d.T;
+  const int n1 = d.vert[c], n2 = d.vert[(size_t)T + c], n3 = d.vert[2 * (size_t)T + c];
+  const double h = d.rkh[c];
+  if (!d.dry_out[c]) {
+    const bool flag = (a.hv[n1] > d.h_dry) && (a.hv[n2] > d.h_dry) && (a.hv[n3] > d.h_dry);
+    if (!flag) {
+      d.u_a[c] = kZero;
+      d.v_a[c] = kZero;
+      double um;
+      d.dry_a[c] = dry_flag(h, kZero, kZero, d.h_dry, d.h_wet, &um);
+    }
+  }
+  if (a.e_est) {
+    double e = kZero;
+    if (!(h < d.h_dry)) {
+      const double x1 = d.node_x[n1], x2 = d.node_x[n2], x3 = d.node_x[n3];
+      const double y1 = d.node_y[n1], y2 = d.node_y[n2], y3 = d.node_y[n3];
+      const double z1 = d.zvtx[n1], z2 = d.zvtx[n2], z3 = d.zvtx[n3];
+      const double gzx = (z1 * (y2 - y3) + z2 * (y3 - y1) + z3 * (y1 - y2)) * kHalf / d.area[c];
+      const double gzy = (z1 * (x3 - x2) + z2 * (x1 - x3) + z3 * (x2 - x1)) * kHalf / d.area[c];
+      const double l = d.perim[c] * kOneThird;
+      const double gx = gzx + (double)G.delh_x[c], gy = gzy + (double)G.delh_y[c];
+      e = sqrt(gx * gx + gy * gy) * l / (d.z[c] + h);
+    }
+    a.e_est[c] = e;
+  }
+}
+
+// ctr2vtx type 3 of u, v and cd with the normalised weights (c2v_setup.f90:113-117),
+// wetdryvfix (btype 0), the dry-vertex zeroing of to_vertices.f90:58-61
+__global__ void __launch_bounds__(256) k_out_vel(Dev d, OutputArgs a) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N) return;
+  const int b0 = d.n2t_off[n], b1 = d.n2t_off[n + 1];
+  double tdist = kZero;
+  for (int q = b0; q < b1; q++) tdist = tdist + d.n2t_w[q];
+  double su = kZero, sv = kZero, scd = kZero;
+  bool wett = false, dryt = false;
+  for (int q = b0; q < b1; q++) {
+    const int k = d.n2t_cell[q];
+    const double w = d.n2t_w[q] / tdist;
+    su = su + w * d.u_a[k];
+    sv = sv + w * d.v_a[k];
+    scd = scd + w * d.cd[k];
+    if (d.dry_out[k]) dryt = true;
+    else wett = true;
+  }
+  if (d.btype == 0 && wett && dryt) {
+    su = kZero;
+    sv = kZero;
+  }
+  if (a.hv[n] < d.h_dry) {
+    su = kZero;
+    sv = kZero;
+  }
+  a.uv[n] = su;
+  a.vv[n] = sv;
+  if (a.cdv) a.cdv[n] = scd;
+}
+
+// enforce_bcs.f90:37-94, the outflow strings in order (one thread: the strings may
+// share end nodes)
+__global__ void k_out_outflow(Dev d, OutputArgs a) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int b = 0; b < a.n_out; b++) {
+    const int ty = a.out_type[b];
+    if (ty == 1)  // :44-56: the relaxed update is overwritten by the instantaneous one
+      for (int i = a.out_off[b]; i < a.out_off[b + 1]; i++) {
+        const int j = a.out_node[i];
+        a.hv[j] = fmax2(kZero, a.hbc[b] - d.zvtx[j]);
+      }
+    if (!((ty == 1 && d.hvalve) || ty == 0)) continue;
+    for (int i = a.out_off[b]; i < a.out_off[b + 1]; i++) {
+      const int j = a.out_node[i];
+      const double dot = a.uv[j] * a.hn[2 * i] + a.vv[j] * a.hn[2 * i + 1];
+      if (dot < kZero) {
+        a.uv[j] = kZero;
+        a.vv[j] = kZero;
+      }
+    }
+  }
+}
+
+// enforce_bcs.f90:97-121, walls then dry nodes
+__global__ void __launch_bounds__(256) k_out_walls(Dev d, OutputArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_wall) return;
+  const int p = a.wall_node[i];
+  if (d.btype == 0) {
+    a.uv[p] = kZero;
+    a.vv[p] = kZero;
+  } else {
+    const double tx = a.wtang[2 * i], ty = a.wtang[2 * i + 1];
+    const double dot = a.uv[p] * tx + a.vv[p] * ty;
+    a.uv[p] = dot * tx;
+    a.vv[p] = dot * ty;
+  }
+}
+__global__ void __launch_bounds__(256) k_out_drynodes(Dev d, OutputArgs a) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= d.N) return;
+  if (a.hv[n] < d.h_dry) {
+    a.uv[n] = kZero;
+    a.vv[n] = kZero;
+  }
+}
+
+// enforce_bcs.f90:124-169 with vbc_by_h.f90 for one inflow string, serial in node order
+// as the reference (the sums of vbc_by_h keep their order)
+__device__ void out_inflow_string(const Dev& d, const OutputArgs& a, int b) {
+  const int o = a.in_off[b], n = a.in_off[b + 1] - o;
+  const int vt = a.in_type[b];
+  const double qin = a.qin[b];
+  if (vt == 0 || vt == 3) {
+    for (int i = 0; i < n; i++) {
+      const int p = a.in_node[o + i];
+      if (a.hv[p] > d.h_dry) {
+        a.uv[p] = vt == 0 ? qin * a.pn[2 * (o + i)] : qin;
+        a.vv[p] = vt == 0 ? qin * a.pn[2 * (o + i) + 1] : (a.qin2 ? a.qin2[b] : kZero);
+      }
+    }
+    return;
+  }
+  if (vt != 1 && vt != 5) return;
+  // vbc_by_h: v_inflow(i), two passes over the string, all sums in node order
+  double ht = kZero, at = kZero;
+  for (int i = 0; i + 1 < n; i++) {
+    const double h1 = a.hv[a.in_node[o + i]], h2 = a.hv[a.in_node[o + i + 1]];
+    const double ai = a.lin[o + i] * (h1 + h2) * kHalf;
+    ht = ht + (h1 + h2) * kHalf;
+    at = at + ai;
+  }
+  // u_inflow(i) = half*(h(i)+h(i+1))*qin/ht/at; v(i) = half*(u(i-1)+u(i)) for wet inner nodes
+  auto hin = [&](int i) { return a.hv[a.in_node[o + i]]; };
+  auto u1 = [&](int i) { return kHalf * (hin(i) + hin(i + 1)) * qin / ht / at; };
+  auto v1 = [&](int i) { return (i >= 1 && i <= n - 2 && hin(i) > d.h_dry) ? kHalf * (u1(i - 1) + u1(i)) : kZero; };
+  double q = kZero;
+  for (int i = 0; i + 1 < n; i++) {
+    const double ui = kHalf * (v1(i) + v1(i + 1));
+    q = q + ui * (a.lin[o + i] * (hin(i) + hin(i + 1)) * kHalf);
+  }
+  auto v2 = [&](int i) { return (i >= 1 && i <= n - 2 && hin(i) > d.h_dry) ? v1(i) * qin / q : v1(i); };
+  for (int i = 0; i < n; i++) {
+    const int p = a.in_node[o + i];
+    if (a.hv[p] > d.h_dry) {
+      const double vi = v2(i);
+      a.uv[p] = vi * a.pn[2 * (o + i)];
+      a.vv[p] = vi * a.pn[2 * (o + i) + 1];
+    }
+  }
+}
+__global__ void k_out_inflow(Dev d, OutputArgs a) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int b = 0; b < a.n_in; b++) out_inflow_string(d, a, b);
+}
+
+// The next iteration's CFL dt after the output pass zeroed velocities: the reference
+// computes it at the start of that iteration from the current u, v (deltatFVT), so
+// the partials of k_fric are recomputed (same expression) and reduced again.
+__global__ void __launch_bounds__(kRedThreads) k_out_dt(Dev d) {
+  __shared__ double sm[kRedThreads / 32];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double dtc = kVlarge;
+  if (c < d.T && d.cell_sid[c] >= 0) {
+    const double h = d.rkh[c];
+    double um1;
+    const bool dry1 = dry_flag(h, d.u_a[c], d.v_a[c], d.h_dry, d.h_wet, &um1);
+    const double wc1 = dry1 ? kZero : sqrt(kG * h);
+    dtc = d.cfl * d.area[c] / ((um1 + wc1 + SMALL_F) * d.perim[c]);
+  }
+  const double r = block_min<kRedThreads>(dtc, sm);
+  if (threadIdx.x == 0) d.part[8 * blockIdx.x + 4] = r;
+}
+__global__ void __launch_bounds__(kRedThreads) k_out_dtfinal(Dev d) {
+  __shared__ double sm[kRedThreads / 32];
+  Scalars* sc = &d.sc[blockIdx.x];
+  double a4 = kVlarge;
+  for (int b = threadIdx.x; b < sc->blk_cnt; b += blockDim.x) a4 = fmin2(a4, d.part[8 * (sc->blk_off + b) + 4]);
+  const double dtmin = block_min<kRedThreads>(a4, sm);
+  if (threadIdx.x == 0) sc->delt = dtmin;
+}
+
+void launch_output(const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed, const OutputArgs& a,
+                   cudaStream_t st) {
+  const int gN = (d.N + 255) / 256, gT = (d.T + 255) / 256;
+  k_out_depth<<<gN, 256, 0, st>>>(d, a);
+  if (mixed) k_out_cell<float><<<gT, 256, 0, st>>>(d, Gf, a);
+  else k_out_cell<double><<<gT, 256, 0, st>>>(d, Gd, a);
+  k_out_vel<<<gN, 256, 0, st>>>(d, a);
+  if (a.n_out > 0) k_out_outflow<<<1, 32, 0, st>>>(d, a);
+  if (a.n_wall > 0) k_out_walls<<<(a.n_wall + 255) / 256, 256, 0, st>>>(d, a);
+  k_out_drynodes<<<gN, 256, 0, st>>>(d, a);
+  if (a.n_in > 0) k_out_inflow<<<1, 32, 0, st>>>(d, a);
+  if (!d.steady && d.dt_op == 1) {
+    k_out_dt<<<d.nblk_red, kRedThreads, 0, st>>>(d);
+    k_out_dtfinal<<<d.nscen, kRedThreads, 0, st>>>(d);
   }
 }
 

@@ -133,6 +133,16 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
       L.n2t_w[L.n2t_off[n] + j] = m.c2v_w[(size_t)j * N + o];
     }
   }
+  L.out_node.clear();
+  L.out_off.assign(1, 0);
+  for (int32_t b = 0; b < m.n_outflowbdr; b++) {
+    for (int32_t i = 0; i < m.n_hbc[b]; i++) {
+      int32_t p = m.hbc_nodes[(size_t)b * m.hbc_ld + i];
+      if (p < 1 || p > N) return set_error(STORM_ERR_MESH, "storm_fvt_create: hbc node out of range");
+      L.out_node.push_back(NN(p));
+    }
+    L.out_off.push_back((int32_t)L.out_node.size());
+  }
   L.node_hbc.assign(N, -1);
   for (int32_t b = 0; b < m.n_outflowbdr; b++) {
     if (m.htype[b] != 1) continue;

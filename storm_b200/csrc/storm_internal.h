@@ -68,6 +68,7 @@ struct HostLayout {
   std::vector<int32_t> n2t_off, n2t_cell;  // CSR [N+1], [nnz]
   std::vector<double> n2t_w;               // c2v_weights_id [nnz]
   std::vector<int16_t> node_hbc;           // htype-1 boundary (slot in hbc[]) or -1
+  std::vector<int32_t> out_node, out_off;  // nodes of every outflow string (new ids), CSR [n_out+1]
   // open boundaries [nbdr], in call order; edges [nbce]
   std::vector<int32_t> bdr_kind, bdr_slot, bdr_off, bdr_cnt;
   std::vector<int32_t> bce_cell, bce_slot;

@@ -29,7 +29,7 @@ EXPORTS = (
     "storm_fvt_last_timing", "storm_fvt_kernel_times", "storm_fvt_destroy",
     "storm_fvt_cfl_dt_noalloc", "storm_fvt_create_batch", "storm_fvt_num_scenarios",
     "storm_fvt_set_scenario_state", "storm_fvt_get_scenario_state", "storm_fvt_scenario_stats",
-    "storm_fvt_autotune",
+    "storm_fvt_autotune", "storm_fvt_output_vertices",
 )
 
 KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux")
@@ -82,6 +82,7 @@ def lib():
     L.storm_fvt_get_scenario_state.argtypes = [C.c_void_p, C.c_int32] + [dp] * 7
     L.storm_fvt_scenario_stats.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.StepStats)]
     L.storm_fvt_autotune.argtypes = [C.c_void_p, C.c_int32, ip]
+    L.storm_fvt_output_vertices.argtypes = [C.c_void_p, C.POINTER(abi.OutputBoundary), C.c_int32] + [dp] * 5
     _lib = L
     return L
 
@@ -180,6 +181,16 @@ class Solver:
         out["hvtx"] = np.empty(self.N)
         _chk(lib().storm_fvt_get_state(self._h, *(abi.dptr(out[k]) for k in
                                                  ("h", "u", "v", "rkh", "rku", "rkv", "hvtx"))))
+        return out
+
+    def output_vertices(self, ob: "abi.OutputBoundaryHolder", in_loop: bool = True) -> dict:
+        """The reference's output step (to_vertices, ctr2vtx(cd), error_est(2)) on the
+        device; zeroes u,v of wet cells with a dry vertex in the solution, as the
+        reference does (``storm_fvt_output_vertices``)."""
+        out = {k: np.empty(self.N) for k in ("hvtx", "uvtx", "vvtx", "cdvtx")}
+        out["e_est"] = np.empty(self.T)
+        _chk(lib().storm_fvt_output_vertices(self._h, C.byref(ob.struct), int(bool(in_loop)),
+                                             *(abi.dptr(out[k]) for k in ("hvtx", "uvtx", "vvtx", "cdvtx", "e_est"))))
         return out
 
     def drycell(self) -> np.ndarray:

@@ -141,3 +141,25 @@ def test_hll_is_consistent(oracle_mod):
     assert np.abs(s["h"][cells] - 1.0).max() < 1e-12
     assert np.abs(s["u"][cells] - 0.3).max() < 1e-12
     assert np.abs(s["v"][cells] + 0.2).max() < 1e-12
+
+
+def test_output_step_lake_at_rest(oracle_mod):
+    """The output step on a lake at rest: vertex depth = WSE - zvtx, zero velocity,
+    zero error estimate gradient of the free surface (flat WSE)."""
+    from storm_b200 import abi
+    sc = scenarios.channel(nx=20, ny=4, q=1e-30)
+    prob = sc.problem
+    o = oracle_mod.Oracle(prob, sc.options)
+    mn = o.mesh_numpy()
+    wse = 1.0  # the outlet stage of the channel, so the stage nodes agree too
+    h0 = np.maximum(wse - mn["z"], 0.0)
+    o.set_state(h0, np.zeros_like(h0), np.zeros_like(h0))
+    o.step(1)  # the output step reads zeta of the last stage's start
+    ob = abi.OutputBoundaryHolder(prob, mn)
+    out = o.output_vertices(ob, in_loop=False)
+    # one iteration on the noisy bed moves the water by O(1e-6) (the scheme is not
+    # exactly well balanced), so the checks carry that tolerance
+    assert np.allclose(out["hvtx"], np.maximum(wse - mn["zvtx"], 0.0), atol=1e-6)
+    assert np.abs(out["uvtx"]).max() < 1e-4 and np.abs(out["vvtx"]).max() < 1e-4
+    assert np.allclose(out["cdvtx"], 0.03, rtol=1e-12)
+    assert np.abs(out["e_est"]).max() < 1e-3
