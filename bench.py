@@ -131,7 +131,9 @@ def build_workload(args):
 
 def mesh_ratios(sc):
     from storm_b200 import fvt
+    t0 = time.perf_counter()
     pm = fvt.build_mesh(sc.problem)
+    mesh_ratios.build_s = time.perf_counter() - t0
     m = pm.mesh
     return pm, m.n_elems, m.n_edges, m.n_pts
 
@@ -493,7 +495,11 @@ def main():
         sc.options.precision = 1
     pm, T, E, N = mesh_ratios(sc)
     K_rk = sc.options.rkorder
+    t0 = time.perf_counter()
     solver = fvt.Solver(pm, sc.options, keep=pm)
+    setup = {"mesh_build_s": mesh_ratios.build_s, "create_s": time.perf_counter() - t0,
+             "what": "storm_fvt_mesh_build (topology, edges, walls, boundary arrays, LSQ and IDW set-up: "
+                     "read_data + dataprepFVT, host C++) and storm_fvt_create (layout, upload, graph capture)"}
 
     def barrier():
         if dist is not None:
@@ -615,6 +621,7 @@ def main():
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "gpu_launches": gpu_launches,
+        "setup": setup,
         "roofline": roofline,
         "clocks": clk.summary(),
         "final": {"iter": stats["iter"], "tmass": stats["tmass"], "status": stats["device_status"]},
