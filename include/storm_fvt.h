@@ -84,7 +84,13 @@ typedef struct StormFvtOptions {
   int32_t precision;   /* STORM_PREC_FP64, or STORM_PREC_MIXED (FP32 gradient, flux
                           and source arithmetic; FP64 state, reconstruction, mass)  */
   int32_t device;      /* CUDA device ordinal                                      */
-  int32_t reserved[6]; /* must be zero                                             */
+  int32_t rsavg_passes;/* residual smoothing (activateRSAVG, solverFVT.f90:238-256):
+                          Gauss-Seidel passes nRSAVG, 0 = off (the default)        */
+  int32_t rsavg_order; /* 0: cells in index order, as the reference (oracle only);
+                          1: by colour of the smoothing stencil (a documented
+                          variant: same steady state, parallel on the GPU)         */
+  double rsavg_eps;    /* epsRSAVG, 0 < eps <= 1                                   */
+  int32_t reserved[2]; /* must be zero                                             */
 } StormFvtOptions;
 
 /* Fill `opt` with the defaults of initialize_options.f90:23-141 (+ ROE, FP64). */

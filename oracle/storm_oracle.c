@@ -109,6 +109,9 @@ struct orc {
   int32_t* fedge_set;      /* flux computed for this interior edge */
   double cqin3[STORM_MAX_BDR], cqout3[STORM_MAX_BDR];
   double qin_it[STORM_MAX_BDR], hbc_it[STORM_MAX_BDR]; /* the values the last iteration ran with */
+  /* residual smoothing: phi0 copy, and the cells ordered by colour (rsavg_order 1) */
+  double* phi0;
+  int32_t* rs_seq;
   /* loop state (solverFVT.f90:53-62) */
   int32_t iter, converged, have_state;
   double ttime, stime, delt, rmax, rms, tmass;
@@ -738,6 +741,10 @@ static int check_options(const StormFvtOptions* op) {
   if (op->opt_friction < 0 || op->opt_friction > 4) return set_err(STORM_ERR_UNSUPPORTED, "opt_friction %d is not supported", op->opt_friction);
   if (op->flux < 0 || op->flux > 2) return set_err(STORM_ERR_ARG, "invalid flux option");
   if (op->stop_cr != 0 && op->stop_cr != 1) return set_err(STORM_ERR_ARG, "invalid stop_cr");
+  if (op->rsavg_passes < 0 || op->rsavg_passes > 64) return set_err(STORM_ERR_ARG, "invalid rsavg_passes");
+  if (op->rsavg_passes > 0 && !(op->rsavg_eps > 0.0 && op->rsavg_eps <= 1.0))
+    return set_err(STORM_ERR_ARG, "invalid rsavg_eps");
+  if (op->rsavg_order != 0 && op->rsavg_order != 1) return set_err(STORM_ERR_ARG, "invalid rsavg_order");
   return 0;
 }
 
@@ -893,7 +900,7 @@ void orc_destroy(orc_t* o) {
                   o->bcedgesoutflow, o->n_timeserh, o->hbc, o->timeloch, o->timeserh, o->h, o->u, o->v,
                   o->zeta, o->u_mag, o->wavec, o->hvtx, o->zetavtx, o->rough, o->delh_x, o->delh_y, o->delu_x,
                   o->delu_y, o->delv_x, o->delv_y, o->delz_x, o->delz_y, o->phi, o->drycell, o->rkh, o->rku,
-                  o->rkv, o->fedge, o->fedge_set};
+                  o->rkv, o->fedge, o->fedge_set, o->phi0, o->rs_seq};
   for (size_t i = 0; i < sizeof ptrs / sizeof ptrs[0]; i++) free(ptrs[i]);
   free(o);
 }
@@ -1753,6 +1760,71 @@ static void fric_terms_impl(orc_t* o, double delta_t) {
   }
 }
 
+/* Greedy colouring of the smoothing stencil t2t (made symmetric), cells visited in
+ * index order, each taking the smallest colour none of its already coloured
+ * neighbours has; rs_seq lists the cells by colour, in index order within a colour.
+ * The CUDA library builds the same colouring from the same t2t. */
+static void rsavg_colour(orc_t* o) {
+  const int32_t T = o->n_elems;
+  int32_t* deg = (int32_t*)xcalloc((size_t)T + 1, sizeof(int32_t));
+  for (int32_t i = 1; i <= T; i++)
+    for (int32_t m = 2; m <= T2T(i, 1) + 1; m++) {
+      deg[i - 1]++;
+      deg[T2T(i, m) - 1]++;
+    }
+  int32_t* off = (int32_t*)xcalloc((size_t)T + 1, sizeof(int32_t));
+  for (int32_t i = 0; i < T; i++) off[i + 1] = off[i] + deg[i];
+  int32_t* adj = (int32_t*)xcalloc((size_t)off[T] + 1, sizeof(int32_t));
+  int32_t* fill = (int32_t*)xcalloc((size_t)T + 1, sizeof(int32_t));
+  for (int32_t i = 1; i <= T; i++)
+    for (int32_t m = 2; m <= T2T(i, 1) + 1; m++) {
+      int32_t j = T2T(i, m);
+      adj[off[i - 1] + fill[i - 1]++] = j;
+      adj[off[j - 1] + fill[j - 1]++] = i;
+    }
+  int32_t* col = (int32_t*)xcalloc((size_t)T + 1, sizeof(int32_t));
+  int32_t ncol = 0;
+  unsigned char used[256];
+  for (int32_t i = 1; i <= T; i++) {
+    memset(used, 0, sizeof used);
+    for (int32_t q = off[i - 1]; q < off[i]; q++) {
+      int32_t j = adj[q];
+      if (j < i && col[j - 1] < 256) used[col[j - 1]] = 1;
+    }
+    int32_t c = 0;
+    while (c < 255 && used[c]) c++;
+    col[i - 1] = c;
+    if (c + 1 > ncol) ncol = c + 1;
+  }
+  o->rs_seq = (int32_t*)xcalloc((size_t)T + 1, sizeof(int32_t));
+  int32_t k = 0;
+  for (int32_t c = 0; c < ncol; c++)
+    for (int32_t i = 1; i <= T; i++)
+      if (col[i - 1] == c) o->rs_seq[k++] = i;
+  free(deg); free(off); free(adj); free(fill); free(col);
+}
+
+/* solverFVT.f90:238-256: residual smoothing (Jameson and Mavriplis), Gauss-Seidel
+ * passes over t2t; rsavg_order 0 visits the cells in index order as the reference,
+ * 1 by colour (the order of the CUDA library) */
+static void rsavg(orc_t* o) {
+  const StormFvtOptions* op = &o->opt;
+  const int32_t T = o->n_elems;
+  const double fac1 = one / (one + op->rsavg_eps * 3.0);
+  const double fac2 = op->rsavg_eps / (one + op->rsavg_eps * 3.0);
+  if (!o->phi0) o->phi0 = (double*)xcalloc((size_t)3 * T, sizeof(double));
+  if (op->rsavg_order == 1 && !o->rs_seq) rsavg_colour(o);
+  memcpy(o->phi0, o->phi, sizeof(double) * 3 * (size_t)T);
+  for (int k = 1; k <= op->rsavg_passes; k++)
+    for (int32_t q = 0; q < T; q++) {
+      const int32_t i = op->rsavg_order == 1 ? o->rs_seq[q] : q + 1;
+      for (int n = 1; n <= 3; n++) {
+        PHI(i, n) = fac1 * o->phi0[(size_t)(n - 1) * T + i - 1];
+        for (int32_t m = 2; m <= T2T(i, 1) + 1; m++) PHI(i, n) = PHI(i, n) + fac2 * PHI(T2T(i, m), n);
+      }
+    }
+}
+
 /* One RK stage, solverFVT.f90:161-325.  `upto` < 5 stops after a phase (probe). */
 static int rk_stage(orc_t* o, int rkstep, int upto, double* delt_io) {
   const int32_t T = o->n_elems;
@@ -1769,6 +1841,7 @@ static int rk_stage(orc_t* o, int rkstep, int upto, double* delt_io) {
   memset(o->phi, 0, sizeof(double) * 3 * T);
   int bad = invisc_fluxes(o);
   bed_slope_std(o);
+  if (op->rsavg_passes > 0) rsavg(o);
   if (upto <= 4) return bad;
   /* :259-283 */
   double delt = *delt_io;

@@ -35,7 +35,8 @@ class Options(C.Structure):
         ("opt_limiter", C.c_int32), ("btype", C.c_int32), ("hvalve", C.c_int32),
         ("vclip", C.c_int32), ("opt_friction", C.c_int32), ("stop_cr", C.c_int32),
         ("flux", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("rsavg_passes", C.c_int32), ("rsavg_order", C.c_int32), ("rsavg_eps", C.c_double),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

@@ -102,7 +102,13 @@ int check_options(const StormFvtOptions& o) {
     return set_error(STORM_ERR_ARG, "precision must be STORM_PREC_FP64 or STORM_PREC_MIXED");
   if (!(o.h_dry > 0.0) || !(o.h_wet >= o.h_dry)) return set_error(STORM_ERR_ARG, "need 0 < h_dry <= h_wet");
   if (!(o.cfl > 0.0)) return set_error(STORM_ERR_ARG, "cfl must be positive");
-  for (int i = 0; i < 6; i++)
+  if (o.rsavg_passes < 0 || o.rsavg_passes > 64) return set_error(STORM_ERR_ARG, "rsavg_passes must be 0..64");
+  if (o.rsavg_passes > 0 && !(o.rsavg_eps > 0.0 && o.rsavg_eps <= 1.0))
+    return set_error(STORM_ERR_ARG, "rsavg_eps must be in (0, 1]");
+  if (o.rsavg_passes > 0 && o.rsavg_order != 1)
+    return set_error(STORM_ERR_UNSUPPORTED,
+                     "residual smoothing in cell index order is serial; the GPU runs rsavg_order 1 (by colour)");
+  for (int i = 0; i < 2; i++)
     if (o.reserved[i]) return set_error(STORM_ERR_ARG, "reserved option fields must be zero");
   return 0;
 }
@@ -172,6 +178,8 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     if (done() || mark(KT_GRAD)) return STORM_ERR_CUDA;
     launch(STAGE_GRAD, gT, h->bs_grad, 0, h->stream, s, hs, dry, dry_next);
     if (done()) return STORM_ERR_CUDA;
+    const bool rs = h->opt.rsavg_passes > 0;
+    const int sF = rs ? STAGE_PHI : STAGE_FLUX, sFB = rs ? STAGE_PHI_BC : STAGE_FLUX_BC;
     if (d.nbdr > 0 && !timing) {
       // k_bc on the side stream overlaps k_eflux and k_flux of the cells without
       // boundary faces; the boundary cells are finished once both are done
@@ -180,9 +188,9 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
       launch(STAGE_BC, d.nbdr, 128, h->bc_smem, h->side, s, hs, dry, dry_next);
       CK(cudaEventRecord(h->join_ev[s], h->side));
       if (gE > 0) launch(STAGE_EFLUX, gE, h->bs_eflux, 0, h->stream, s, hs, dry, dry_next);
-      launch(STAGE_FLUX, gF, h->bs_flux, 0, h->stream, s, hs, dry, dry_next);
+      launch(sF, gF, h->bs_flux, 0, h->stream, s, hs, dry, dry_next);
       CK(cudaStreamWaitEvent(h->stream, h->join_ev[s], 0));
-      if (gB > 0) launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+      if (gB > 0) launch(sFB, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
     } else {
       if (d.nbdr > 0) {
         if (mark(KT_BC)) return STORM_ERR_CUDA;
@@ -195,8 +203,17 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
         if (done()) return STORM_ERR_CUDA;
       }
       if (mark(KT_FLUX)) return STORM_ERR_CUDA;
-      launch(STAGE_FLUX, gF, h->bs_flux, 0, h->stream, s, hs, dry, dry_next);
-      if (gB > 0) launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+      launch(sF, gF, h->bs_flux, 0, h->stream, s, hs, dry, dry_next);
+      if (gB > 0) launch(sFB, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+      if (done()) return STORM_ERR_CUDA;
+    }
+    if (rs) {  // solverFVT.f90:238-256, then the update of every cell
+      if (mark(KT_FLUX)) return STORM_ERR_CUDA;
+      const HostLayout& Lm = h->L;
+      for (int k = 0; k < h->opt.rsavg_passes; k++)
+        for (size_t c = 0; c + 1 < Lm.rs_off.size(); c++)
+          launch_rsavg(d, Lm.rs_off[c], Lm.rs_off[c + 1] - Lm.rs_off[c], h->stream);
+      launch(STAGE_UPDATE, (T + 127) / 128, 128, 0, h->stream, s, hs, dry, dry_next);
       if (done()) return STORM_ERR_CUDA;
     }
   }
@@ -290,6 +307,9 @@ int upload(StormFvtHandle* h) {
   size_t o_csid = cpy(L.cell_sid, T), o_nsid = cpy(L.node_sid, N);
   size_t o_esid = cpy(L.edge_sid, std::max(L.ne, 1)), o_bsid = cpy(L.bdr_sid, nbdr);
   size_t o_bcl = cpy(L.bc_cells, std::max<size_t>(L.bc_cells.size(), 1));
+  const bool rsavg = h->opt.rsavg_passes > 0;
+  size_t o_rsc = cpy(L.rs_cells, std::max<size_t>(L.rs_cells.size(), 1));
+  size_t o_phi = A.take(rsavg ? 8 * 3 * (size_t)T : 8), o_phi0 = A.take(rsavg ? 8 * 3 * (size_t)T : 8);
   const size_t ne1 = std::max(L.ne, 1);
   size_t o_eL = cpy(L.eL, ne1), o_eR = cpy(L.eR, ne1), o_es = cpy(L.eslot, ne1);
   size_t o_enx = cpy(L.enx, ne1), o_eny = cpy(L.eny, ne1), o_el = cpy(L.elen, ne1), o_ez0 = cpy(L.ez0, ne1);
@@ -361,6 +381,9 @@ int upload(StormFvtHandle* h) {
   d.delu_y = at<double>(B, o_g[3]); d.delv_x = at<double>(B, o_g[4]); d.delv_y = at<double>(B, o_g[5]);
   d.dry_a = at<uint8_t>(B, o_dra); d.dry_b = at<uint8_t>(B, o_drb); d.hvtx = at<double>(B, o_hv);
   d.dry_out = at<uint8_t>(B, o_dro);
+  d.rs_cells = at<int32_t>(B, o_rsc); d.phi = at<double>(B, o_phi); d.phi0 = at<double>(B, o_phi0);
+  d.rs_fac1 = 1.0 / (1.0 + o.rsavg_eps * 3.0);  // solverFVT.f90:59-60
+  d.rs_fac2 = o.rsavg_eps / (1.0 + o.rsavg_eps * 3.0);
   d.vwet = at<uint8_t>(B, o_vw); d.phimax = at<double>(B, o_pm); d.bc_c = at<double>(B, o_bcc3);
   d.bc_rec = at<double>(B, o_rec); d.part = at<double>(B, o_part); d.nblk_red = nblk;
   d.sc = at<Scalars>(B, o_sc);

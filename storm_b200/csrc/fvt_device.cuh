@@ -80,6 +80,10 @@ struct Dev {
   double* hvtx;             // vertex depth after enforce_bcs (wall fluxes, output)
   uint8_t* vwet;            // hvtx > h_dry before enforce_bcs (to_vertices.f90:44-55)
   double* phimax;           // MAX(|phi|) of the last stage (stop criterion)
+  // residual smoothing: phi and its copy [3][T], cells by colour of the t2t stencil
+  double *phi, *phi0;
+  const int32_t* rs_cells;
+  double rs_fac1, rs_fac2;
   double* bc_c;             // [3][nbce] boundary contributions to phi
   double* bc_rec;           // [3][nbce] reconstructed boundary-edge h, u, v
   double* part;             // [nblk][8] reduction partials (blocks never span scenarios)
@@ -100,7 +104,8 @@ struct Geo {
 };
 
 // One launch of a templated stage kernel (see launch_stage in fvt_kernels.cu).
-enum StageKernel { STAGE_GRAD, STAGE_BC, STAGE_EFLUX, STAGE_FLUX, STAGE_FLUX_BC };
+enum StageKernel { STAGE_GRAD, STAGE_BC, STAGE_EFLUX, STAGE_FLUX, STAGE_FLUX_BC, STAGE_PHI, STAGE_PHI_BC,
+                   STAGE_UPDATE };
 struct StageLaunch {
   int which;
   dim3 grid, block;
@@ -114,6 +119,7 @@ struct StageLaunch {
 };
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed);
 void set_bc_smem_limit(int bytes);
+void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st);
 
 // The output pass (to_vertices, ctr2vtx of cd, error_est(2)) after an iteration.
 struct OutputArgs {

@@ -992,8 +992,8 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<float>& G, in
 // solverFVT.f90:194), then the bed slope, then the RK update.  phi and the RK
 // combination are FP64 on both paths.
 template <class R>
-__device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, int c, const double* __restrict__ hs,
-                                          const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+__device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int c, const double* __restrict__ hs,
+                                             const uint8_t* __restrict__ dry, double* p1o, double* p2o, double* p3o) {
   const int T = d.T;
   const bool dry_c = dry[c];
   const double h_c = hs[c];
@@ -1082,6 +1082,15 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
     p2 = p2 - s2;
     p3 = p3 - s3;
   }
+  *p1o = p1;
+  *p2o = p2;
+  *p3o = p3;
+}
+
+// The RK update of stage s (1-based) for cell c from its phi (solverFVT.f90:259-325).
+__device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c, bool dry_c, double p1, double p2,
+                                          double p3, uint8_t* __restrict__ dry_next) {
+  const int T = d.T;
   // RK update (solverFVT.f90:259-283)
   const double u_c = d.u_a[c], v_c = d.v_a[c];
   double delt;
@@ -1138,6 +1147,70 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
   } else {
     d.phimax[c] = fmax2(fmax2(fmax2(kZero, fabs(p1)), fabs(p2)), fabs(p3));
   }
+}
+
+template <class R>
+__device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, int c, const double* __restrict__ hs,
+                                          const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+  double p1, p2, p3;
+  assemble_phi<R>(d, G, c, hs, dry, &p1, &p2, &p3);
+  rk_update(d, s, c, hs[c], dry[c] != 0, p1, p2, p3, dry_next);
+}
+
+// Residual smoothing (solverFVT.f90:238-256, activateRSAVG): the stage's phi is
+// assembled into d.phi (and its copy phi0), smoothed by Gauss-Seidel passes over the
+// cells of one colour of the t2t stencil at a time (cells of a colour share no
+// stencil edge, so each reads its neighbours' latest values exactly as a serial sweep
+// in colour order does), then every cell is updated.
+template <class R>
+__global__ void __launch_bounds__(128) k_flux_phi(Dev d, Geo<R> G, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, int bc_cells) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int c;
+  if (bc_cells) {
+    if (i >= d.nbc_cells) return;
+    c = d.bc_cells[i];
+  } else {
+    if (i >= d.T) return;
+    c = i;
+    if (d.forder[c] & kOrderHasBc) return;
+  }
+  const int sid = d.cell_sid[c];
+  if (sid < 0 || d.sc[sid].converged) return;
+  double p1, p2, p3;
+  assemble_phi<R>(d, G, c, hs, dry, &p1, &p2, &p3);
+  const size_t T = d.T;
+  d.phi[c] = p1;
+  d.phi[T + c] = p2;
+  d.phi[2 * T + c] = p3;
+  d.phi0[c] = p1;
+  d.phi0[T + c] = p2;
+  d.phi0[2 * T + c] = p3;
+}
+
+__global__ void __launch_bounds__(256) k_rsavg(Dev d, int off, int cnt) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= cnt) return;
+  const int c = d.rs_cells[off + q];
+  const int sid = d.cell_sid[c];
+  if (sid < 0 || d.sc[sid].converged) return;
+  const size_t T = d.T;
+  const int n = d.nst[c];
+  for (int k = 0; k < 3; k++) {
+    double p = d.rs_fac1 * d.phi0[k * T + c];
+    for (int m = 0; m < n; m++) p = p + d.rs_fac2 * d.phi[k * T + d.st_id[(size_t)m * T + c]];
+    d.phi[k * T + c] = p;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_update(Dev d, int s, const double* __restrict__ hs,
+                                            const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.T) return;
+  const int sid = d.cell_sid[c];
+  if (sid < 0 || d.sc[sid].converged) return;
+  const size_t T = d.T;
+  rk_update(d, s, c, hs[c], dry[c] != 0, d.phi[c], d.phi[T + c], d.phi[2 * T + c], dry_next);
 }
 
 // All cells without an open-boundary face (those wait for k_bc in k_flux_bc).
@@ -1571,12 +1644,25 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
     case STAGE_FLUX_BC:
       k_flux_bc<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.s, L.hs, L.dry, L.dry_next);
       break;
+    case STAGE_PHI:
+      k_flux_phi<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, 0);
+      break;
+    case STAGE_PHI_BC:
+      k_flux_phi<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, 1);
+      break;
+    case STAGE_UPDATE:
+      k_update<<<L.grid, L.block, 0, L.stream>>>(d, L.s, L.hs, L.dry, L.dry_next);
+      break;
   }
 }
 
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed) {
   if (mixed) launch_stage_t<float>(L, d, Gf);
   else launch_stage_t<double>(L, d, Gd);
+}
+
+void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st) {
+  if (cnt > 0) k_rsavg<<<(cnt + 255) / 256, 256, 0, st>>>(d, off, cnt);
 }
 
 void set_bc_smem_limit(int bytes) {

@@ -408,6 +408,48 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
       if (L.fkind[(size_t)j * T + c] == FACE_BC) L.forder[c] |= kOrderHasBc;
     if (L.forder[c] & kOrderHasBc) L.bc_cells.push_back(c);
   }
+  // Greedy colouring of the t2t stencil made symmetric, cells in reference index order,
+  // each taking the smallest colour none of its already coloured neighbours has (the
+  // order residual smoothing visits them; the oracle builds the same colouring).
+  {
+    std::vector<int32_t> deg((size_t)T + 1, 0);
+    for (int32_t o = 0; o < T; o++) {
+      const int32_t n = m.t2t[o];
+      for (int32_t k = 0; k < n; k++) {
+        deg[o]++;
+        deg[m.t2t[(size_t)(k + 1) * T + o] - 1]++;
+      }
+    }
+    std::vector<int32_t> off((size_t)T + 1, 0);
+    for (int32_t o = 0; o < T; o++) off[o + 1] = off[o] + deg[o];
+    std::vector<int32_t> adj(off[T]), fill(T, 0);
+    for (int32_t o = 0; o < T; o++) {
+      const int32_t n = m.t2t[o];
+      for (int32_t k = 0; k < n; k++) {
+        const int32_t j = m.t2t[(size_t)(k + 1) * T + o] - 1;
+        adj[off[o] + fill[o]++] = j;
+        adj[off[j] + fill[j]++] = o;
+      }
+    }
+    std::vector<int32_t> col(T, 0);
+    int32_t ncol = 0;
+    for (int32_t o = 0; o < T; o++) {
+      bool used[256] = {false};
+      for (int32_t q = off[o]; q < off[o + 1]; q++)
+        if (adj[q] < o && col[adj[q]] < 256) used[col[adj[q]]] = true;
+      int32_t c = 0;
+      while (c < 255 && used[c]) c++;
+      col[o] = c;
+      ncol = std::max(ncol, c + 1);
+    }
+    L.rs_off.assign(1, 0);
+    L.rs_cells.clear();
+    for (int32_t c = 0; c < ncol; c++) {
+      for (int32_t o = 0; o < T; o++)
+        if (col[o] == c) L.rs_cells.push_back(CN(o + 1));
+      L.rs_off.push_back((int32_t)L.rs_cells.size());
+    }
+  }
   // numerical valve targets (solverFVT.f90:357-370)
   for (int32_t j = 0; j < m.n_bcedges; j++) {
     if (!m.hbar[j]) continue;
@@ -540,6 +582,19 @@ void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& 
     noff_nnz += P.n2t_nnz;
   }
   M.nbdr = (int32_t)M.bdr_kind.size();
+  // residual-smoothing colours: colour c of every scenario together (scenarios share no cell)
+  size_t ncol = 0;
+  for (const HostLayout& P : parts) ncol = std::max(ncol, P.rs_off.empty() ? 0 : P.rs_off.size() - 1);
+  M.rs_off.assign(1, 0);
+  M.rs_cells.clear();
+  for (size_t c = 0; c < ncol; c++) {
+    for (size_t s = 0; s < S; s++) {
+      const HostLayout& P = parts[s];
+      if (c + 1 >= P.rs_off.size()) continue;
+      for (int32_t q = P.rs_off[c]; q < P.rs_off[c + 1]; q++) M.rs_cells.push_back(P.rs_cells[q] + info[s].cell_off);
+    }
+    M.rs_off.push_back((int32_t)M.rs_cells.size());
+  }
 }
 
 }  // namespace storm

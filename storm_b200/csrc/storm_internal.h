@@ -49,6 +49,7 @@ struct HostLayout {
   std::vector<double> lsq_a, lsq_b, lsq_c, lsq_det;
   std::vector<uint8_t> nst, forder, hvmask;
   std::vector<int32_t> bc_cells;  // cells with an open-boundary face, increasing
+  std::vector<int32_t> rs_cells, rs_off;  // cells by colour of the t2t stencil (new ids), CSR
   // [3][T]
   std::vector<int32_t> vert, t2t3, fref;
   std::vector<double> rc_x, rc_y, fnx, fny, flen, fz0;

@@ -163,3 +163,40 @@ def test_output_step_lake_at_rest(oracle_mod):
     assert np.abs(out["uvtx"]).max() < 1e-4 and np.abs(out["vvtx"]).max() < 1e-4
     assert np.allclose(out["cdvtx"], 0.03, rtol=1e-12)
     assert np.abs(out["e_est"]).max() < 1e-3
+
+
+def test_residual_smoothing_keeps_the_steady_state(oracle_mod):
+    """The reference's index-order sweep and the colour-order variant the GPU runs
+    reach the same smoothed steady state, in fewer iterations than plain iteration on
+    this channel.  (The smoothed steady state is not the plain one: the implicit
+    friction step is applied outside phi, so at steady state phi is not zero and
+    smoothing it moves the fixed point -- a property of the reference scheme.)"""
+    from storm_b200 import abi
+    sc = scenarios.batch_channels(1, 1600, 1700, seed=11, opt_limiter=0)[0]
+    res = {}
+    for name, kw in (("plain", {}), ("ref", dict(rsavg_passes=4, rsavg_order=0, rsavg_eps=0.8)),
+                     ("colour", dict(rsavg_passes=4, rsavg_order=1, rsavg_eps=0.8))):
+        o2 = abi.Options.from_buffer_copy(sc.options)
+        o2.rstop = 1e-8
+        for k, v in kw.items():
+            setattr(o2, k, v)
+        o = oracle_mod.Oracle(sc.problem, o2, threads=4)
+        o.set_state(sc.h0, sc.u0, sc.v0)
+        st = o.step(60000)
+        assert st["converged"]
+        res[name] = (st["iter"], o.state()["h"])
+    assert res["ref"][0] < res["plain"][0] and res["colour"][0] < res["plain"][0]
+    assert np.abs(res["colour"][1] - res["ref"][1]).max() < 2e-3
+    assert np.abs(res["ref"][1] - res["plain"][1]).max() < 0.1
+
+
+def test_residual_smoothing_options_checked(oracle_mod):
+    from storm_b200 import abi
+    sc = scenarios.channel(nx=10, ny=4)
+    for kw in (dict(rsavg_passes=2, rsavg_eps=0.0), dict(rsavg_passes=-1), dict(rsavg_passes=2, rsavg_eps=0.5,
+                                                                                   rsavg_order=3)):
+        o2 = abi.Options.from_buffer_copy(sc.options)
+        for k, v in kw.items():
+            setattr(o2, k, v)
+        with pytest.raises(oracle_mod.OracleError):
+            oracle_mod.Oracle(sc.problem, o2)
