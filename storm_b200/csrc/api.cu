@@ -78,9 +78,7 @@ struct StormFvtHandle {
 
 namespace {
 
-constexpr int kCellThreads = 256;
 constexpr int kFluxThreads = 128;
-constexpr int kNodeThreads = 256;
 constexpr int kRed = 256;
 
 #define CK(call)                                                                                     \

@@ -122,3 +122,15 @@ def test_default_options_match_reference_defaults(storm_lib):
         if name == "reserved":
             continue
         assert getattr(lo, name) == getattr(po, name), name
+
+
+def test_fewer_than_four_triangles_rejected(storm_lib, oracle_mod):
+    """read_data stops on a domain of fewer than 4 triangles; both builders do too."""
+    x = np.array([0.0, 1.0, 1.0, 0.0])
+    y = np.array([0.0, 0.0, 1.0, 1.0])
+    p = abi.ProblemHolder(x, y, np.array([[1, 2, 3], [1, 3, 4]], dtype=np.int32), np.zeros(4), np.zeros(2))
+    with pytest.raises(fvt.StormError) as e:
+        fvt.build_mesh(p)
+    assert e.value.code == abi.STORM_ERR_MESH
+    with pytest.raises(oracle_mod.OracleError):
+        oracle_mod.Oracle(p, abi.default_options())
