@@ -438,6 +438,15 @@ __global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* 
   const int T = d.T;
   const double zeta_c = hs[c] + d.z[c];
   const double u_c = d.u_a[c], v_c = d.v_a[c];
+  // face neighbours and vertices first: their loads (and the flags read through them
+  // below) are in flight while the stencil is gathered
+  int t3[3], vt[3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    t3[j] = d.t2t3[(size_t)j * T + c];
+    vt[j] = d.vert[(size_t)j * T + c];
+  }
+  const bool dry_c = dry[c];
   R hx = R(0), hy = R(0), ux = R(0), uy = R(0), vx = R(0), vy = R(0);
   if (d.lim == 1 || d.lim == 2) {
     R dz = R(0), ez = R(0), du = R(0), eu = R(0), dv = R(0), ev = R(0);
@@ -498,7 +507,7 @@ __global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* 
 #pragma unroll
     for (int j = 0; j < 3; j++) {
       const size_t q = (size_t)j * T + c;
-      const int k = d.t2t3[q];
+      const int k = t3[j];
       const R rx = G.rc_x[q], ry = G.rc_y[q];
       const double qz = k < 0 ? zeta_c : hs[k] + d.z[k];
       const double qu = k < 0 ? u_c : d.u_a[k];
@@ -517,12 +526,12 @@ __global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* 
   hx = hx - G.delz_x[c];
   hy = hy - G.delz_y[c];
   double ub = u_c, vb = v_c;
-  if (!dry[c]) {
+  if (!dry_c) {
     // hgradfix2.f90:48-98
     bool setgrad = zeta_c < d.zmax[c];
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-      const int l = d.t2t3[(size_t)j * T + c];
+      const int l = t3[j];
       if (l < 0) continue;
       if (dry[l] && d.z[l] < zeta_c) setgrad = false;
     }
@@ -538,7 +547,7 @@ __global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* 
     // to_vertices.f90:44-55
     bool flag = true;
 #pragma unroll
-    for (int j = 0; j < 3; j++) flag = flag && d.vwet[d.vert[(size_t)j * T + c]];
+    for (int j = 0; j < 3; j++) flag = flag && d.vwet[vt[j]];
     if (!flag) {
       ub = kZero;
       vb = kZero;

@@ -105,6 +105,56 @@ __device__ __forceinline__ void store_chunk(uint8_t* dst, int q, int cpr, uint4 
   *reinterpret_cast<uint4*>(dst + blk * (kRows * 128) + umma::sw128_offset(r, (c & 7) * 8)) = v;
 }
 
+template <int R>
+__device__ __forceinline__ void stage_agg_rounds(const Seg& s, int row0, uint8_t* dst, int tid, int nthr, int cpr,
+                                                 int total) {
+  for (int h = 0; h * nthr < total; h += R) {
+    uint4 w[R][3];
+    bool m[R][3];
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+      const int q = tid + (h + i) * nthr;
+      const int row = row0 + q / cpr;
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        m[i][k] = (q < total) && s.nbr[static_cast<size_t>(k) * s.agg_stride + row] >= 0;
+    }
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+      const int q = tid + (h + i) * nthr;
+      const int row = row0 + q / cpr, c = q % cpr;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        w[i][k] = make_uint4(0, 0, 0, 0);
+        if (m[i][k]) {
+          const size_t er = static_cast<size_t>(k) * s.agg_stride + row;
+          w[i][k] = *reinterpret_cast<const uint4*>(s.src + er * s.width + c * 8);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+      const int q = tid + (h + i) * nthr;
+      if (q >= total) continue;
+      float acc[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) acc[j] = 0.f;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        if (!m[i][k]) continue;
+        const bf16* b = reinterpret_cast<const bf16*>(&w[i][k]);
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[j] += __bfloat162float(b[j]);
+      }
+      uint4 v;
+      bf16* o = reinterpret_cast<bf16*>(&v);
+#pragma unroll
+      for (int j = 0; j < 8; j++) o[j] = __float2bfloat16(acc[j]);
+      store_chunk(dst, q, cpr, v);
+    }
+  }
+}
+
 // Stage rows [row0, row0+128) of one segment into `dst` (blocks of 128 x 64, 16 KB
 // each) with `nthr` threads (thread `tid` of them), in rounds of eight chunks per thread.
 __device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* dst, int tid = -1,
@@ -138,52 +188,10 @@ __device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* d
     }
     return;
   }
-  // aggregation: sum of the three edge rows of each cell, in rounds of four chunks
-  for (int h = 0; h * nthr < total; h += 4) {
-    uint4 w[4][3];
-    bool m[4][3];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int q = tid + (h + i) * nthr;
-      const int row = row0 + q / cpr;
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-        m[i][k] = (q < total) && s.nbr[static_cast<size_t>(k) * s.agg_stride + row] >= 0;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int q = tid + (h + i) * nthr;
-      const int row = row0 + q / cpr, c = q % cpr;
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        w[i][k] = make_uint4(0, 0, 0, 0);
-        if (m[i][k]) {
-          const size_t er = static_cast<size_t>(k) * s.agg_stride + row;
-          w[i][k] = *reinterpret_cast<const uint4*>(s.src + er * s.width + c * 8);
-        }
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int q = tid + (h + i) * nthr;
-      if (q >= total) continue;
-      float acc[8];
-#pragma unroll
-      for (int j = 0; j < 8; j++) acc[j] = 0.f;
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        if (!m[i][k]) continue;
-        const bf16* b = reinterpret_cast<const bf16*>(&w[i][k]);
-#pragma unroll
-        for (int j = 0; j < 8; j++) acc[j] += __bfloat162float(b[j]);
-      }
-      uint4 v;
-      bf16* o = reinterpret_cast<bf16*>(&v);
-#pragma unroll
-      for (int j = 0; j < 8; j++) o[j] = __float2bfloat16(acc[j]);
-      store_chunk(dst, q, cpr, v);
-    }
-  }
+  // aggregation: sum of the three edge rows of each cell, in rounds of eight chunks
+  // per thread (24 loads in flight) for the 128 producer threads, four otherwise
+  if (nthr <= 128) stage_agg_rounds<8>(s, row0, dst, tid, nthr, cpr, total);
+  else stage_agg_rounds<4>(s, row0, dst, tid, nthr, cpr, total);
 }
 
 // Stage an fp32 [rows][width] tile as bf16 (width 64 or 128).
