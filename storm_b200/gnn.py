@@ -6,7 +6,7 @@ SToRM has no such component: a steady run (solverFVT.f90:129-478 with ``steady``
 starts from the initial condition the user supplies.  Here the network predicts an
 initial h, hu, hv from the bed, roughness, cell geometry and the boundary discharge
 and stage; the solver then runs from that field to its own stop test, so the solver
-remains both the fallback and the judge of the result.
+remains both the fallback and the arbiter of the result.
 
 Architecture (encode / process / decode):
 
