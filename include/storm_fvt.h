@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define STORM_FVT_ABI_VERSION 1
+#define STORM_FVT_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define STORM_FVT_API __attribute__((visibility("default")))
@@ -136,6 +136,12 @@ typedef struct StormFvtProblem {
   const StormFvtBoundary* inflow;
   int32_t n_outflow;
   const StormFvtBoundary* outflow;
+  /* wind forcing (the text input of windforcing.f90: drag coefficient and wind
+     velocity components), NULL = no wind terms */
+  const double* wind_c0;
+  const double* wind_x;
+  const double* wind_y;
+  int32_t wind_at_vertices;  /*  1: the three arrays are [n_pts]; 0: [n_elems]     */
 } StormFvtProblem;
 
 /*
@@ -211,6 +217,8 @@ typedef struct StormFvtMesh {
   const double* timeloch;        /* (tsh_ld,n_outflowbdr)                           */
   const double* timeserh;        /* (tsh_ld,n_outflowbdr)                           */
   double bch_max;                /* dataprepFVT.f90:278-286                         */
+  const double* wcoef1;          /* [n_elems] wind terms added to phi(:,2:3) of wet */
+  const double* wcoef2;          /*  cells (dep_vars.f90:33), NULL: no wind terms   */
 } StormFvtMesh;
 
 /* Per-call statistics, the scalars solverFVT prints per iteration

@@ -90,6 +90,7 @@ struct orc {
   int32_t flow_edges1, wall_edges1, n_bcedges;
   int32_t *flowedg1, *walledg1, *bcedges, *hbar, *qbar;
   double *z, *zvtx, *cd;
+  double *wcoef1, *wcoef2; /* dep_vars.f90:33, NULL: no wind terms */
   /* boundaries */
   int32_t n_in, qin_ld, bcin_ld, tsq_ld;
   int32_t *vtype, *n_qin, *qin_nodes, *bcedgesinflow, *n_timeserq;
@@ -810,6 +811,32 @@ int orc_create(const StormFvtProblem* p, const StormFvtOptions* opt, orc_t** out
   }
   if (p->cd_at_vertices) vtx2ctr(o, p->cd, o->cd); /* :132-134 */
   else memcpy(o->cd, p->cd, sizeof(double) * T);
+  /* windforcing.f90:80-104 (text input, centred finite-volume solvers) */
+  if (p->wind_c0 && p->wind_x && p->wind_y) {
+    double* c0 = (double*)xcalloc((size_t)T, sizeof(double));
+    double* wx = (double*)xcalloc((size_t)T, sizeof(double));
+    double* wy = (double*)xcalloc((size_t)T, sizeof(double));
+    if (p->wind_at_vertices) {
+      vtx2ctr(o, p->wind_c0, c0);
+      vtx2ctr(o, p->wind_x, wx);
+      vtx2ctr(o, p->wind_y, wy);
+    } else {
+      memcpy(c0, p->wind_c0, sizeof(double) * T);
+      memcpy(wx, p->wind_x, sizeof(double) * T);
+      memcpy(wy, p->wind_y, sizeof(double) * T);
+    }
+    const double rho = 998.60; /* constants.f90:29 */
+    o->wcoef1 = (double*)xcalloc((size_t)T, sizeof(double));
+    o->wcoef2 = (double*)xcalloc((size_t)T, sizeof(double));
+    for (int32_t i = 1; i <= T; i++) {
+      double windmag = sqrt(wx[i - 1] * wx[i - 1] + wy[i - 1] * wy[i - 1]);
+      o->wcoef1[i - 1] = c0[i - 1] * wx[i - 1] * windmag / rho;
+      o->wcoef2[i - 1] = c0[i - 1] * wy[i - 1] * windmag / rho;
+    }
+    free(c0);
+    free(wx);
+    free(wy);
+  }
   /* :161-173 rc (before the normals are normalised) */
   o->rc_x = (double*)xcalloc((size_t)3 * T, sizeof(double));
   o->rc_y = (double*)xcalloc((size_t)3 * T, sizeof(double));
@@ -900,7 +927,7 @@ void orc_destroy(orc_t* o) {
                   o->bcedgesoutflow, o->n_timeserh, o->hbc, o->timeloch, o->timeserh, o->h, o->u, o->v,
                   o->zeta, o->u_mag, o->wavec, o->hvtx, o->zetavtx, o->rough, o->delh_x, o->delh_y, o->delu_x,
                   o->delu_y, o->delv_x, o->delv_y, o->delz_x, o->delz_y, o->phi, o->drycell, o->rkh, o->rku,
-                  o->rkv, o->fedge, o->fedge_set, o->phi0, o->rs_seq};
+                  o->rkv, o->fedge, o->fedge_set, o->phi0, o->rs_seq, o->wcoef1, o->wcoef2};
   for (size_t i = 0; i < sizeof ptrs / sizeof ptrs[0]; i++) free(ptrs[i]);
   free(o);
 }
@@ -933,6 +960,8 @@ int orc_export_mesh(const orc_t* o, StormFvtMesh* m) {
   m->hbc_ld = o->hbc_ld; m->n_hbc = o->n_hbc; m->hbc_nodes = o->hbc_nodes;
   m->tsh_ld = o->tsh_ld; m->n_timeserh = o->n_timeserh; m->timeloch = o->timeloch; m->timeserh = o->timeserh;
   m->bch_max = o->bch_max;
+  m->wcoef1 = o->wcoef1;
+  m->wcoef2 = o->wcoef2;
   return 0;
 }
 
@@ -1841,6 +1870,12 @@ static int rk_stage(orc_t* o, int rkstep, int upto, double* delt_io) {
   memset(o->phi, 0, sizeof(double) * 3 * T);
   int bad = invisc_fluxes(o);
   bed_slope_std(o);
+  if (o->wcoef1) /* solverFVT.f90:218-224 */
+    for (int32_t i = 1; i <= T; i++) {
+      if (DRY(i)) continue;
+      PHI(i, 2) = PHI(i, 2) + o->wcoef1[i - 1];
+      PHI(i, 3) = PHI(i, 3) + o->wcoef2[i - 1];
+    }
   if (op->rsavg_passes > 0) rsavg(o);
   if (upto <= 4) return bad;
   /* :259-283 */

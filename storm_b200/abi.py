@@ -87,6 +87,7 @@ class Problem(C.Structure):
         ("cd", _d), ("cd_at_vertices", C.c_int32),
         ("n_inflow", C.c_int32), ("inflow", C.POINTER(Boundary)),
         ("n_outflow", C.c_int32), ("outflow", C.POINTER(Boundary)),
+        ("wind_c0", _d), ("wind_x", _d), ("wind_y", _d), ("wind_at_vertices", C.c_int32),
     ]
 
 
@@ -118,6 +119,7 @@ class Mesh(C.Structure):
         ("hbc_ld", C.c_int32), ("n_hbc", _i), ("hbc_nodes", _i),
         ("tsh_ld", C.c_int32), ("n_timeserh", _i), ("timeloch", _d), ("timeserh", _d),
         ("bch_max", C.c_double),
+        ("wcoef1", _d), ("wcoef2", _d),
     ]
 
 
@@ -160,7 +162,7 @@ class ProblemHolder:
     """
 
     def __init__(self, x, y, tri, zb, cd, *, zb_at_vertices=True, cd_at_vertices=False,
-                 inflow=(), outflow=(), edge_p=None, edge_e=None):
+                 inflow=(), outflow=(), edge_p=None, edge_e=None, wind=None):
         self._keep = []
         self.x = np.ascontiguousarray(x, dtype=np.float64)
         self.y = np.ascontiguousarray(y, dtype=np.float64)
@@ -184,6 +186,14 @@ class ProblemHolder:
         p.cd, p.cd_at_vertices = dptr(self.cd), int(cd_at_vertices)
         p.n_inflow, p.inflow = self._bdr(self.inflow_spec)
         p.n_outflow, p.outflow = self._bdr(self.outflow_spec)
+        # wind: dict(c0=..., x=..., y=..., at_vertices=bool), the windforcing.f90 input
+        self.wind = wind
+        if wind is not None:
+            self.wind_c0 = np.ascontiguousarray(wind["c0"], dtype=np.float64)
+            self.wind_x = np.ascontiguousarray(wind["x"], dtype=np.float64)
+            self.wind_y = np.ascontiguousarray(wind["y"], dtype=np.float64)
+            p.wind_c0, p.wind_x, p.wind_y = dptr(self.wind_c0), dptr(self.wind_x), dptr(self.wind_y)
+            p.wind_at_vertices = int(bool(wind.get("at_vertices", False)))
         self.problem = p
 
     def _bdr(self, specs):
@@ -251,6 +261,8 @@ def mesh_to_numpy(m: Mesh) -> dict:
     ]
     for name, n, dt in spec:
         d[name] = _arr(getattr(m, name), n, dt)
+    for name in ("wcoef1", "wcoef2"):
+        d[name] = _arr(getattr(m, name), T, f64) if getattr(m, name) else None
     for name in ("t2t_ncol", "n2t_ncol", "c2v_ncol", "flow_edges1", "wall_edges1", "n_bcedges",
                  "n_inflowbdr", "n_outflowbdr", "bcin_ld", "bcout_ld", "hbc_ld", "tsq_ld",
                  "tsh_ld", "bch_max"):

@@ -289,6 +289,8 @@ int upload(StormFvtHandle* h) {
   size_t o_z = cpy(L.z, T), o_dzx = cpy(L.delz_x, T), o_dzy = cpy(L.delz_y, T), o_zmax = cpy(L.zmax, T);
   size_t o_cd = cpy(L.cd, T), o_la = cpy(L.lsq_a, T), o_lb = cpy(L.lsq_b, T), o_lc = cpy(L.lsq_c, T);
   size_t o_ld = cpy(L.lsq_det, T);
+  const bool wind = !L.wcoef1.empty();
+  size_t o_wc1 = wind ? cpy(L.wcoef1, T) : 0, o_wc2 = wind ? cpy(L.wcoef2, T) : 0;
   size_t o_nst = cpy(L.nst, T), o_ford = cpy(L.forder, T), o_hvm = cpy(L.hvmask, T), o_fk = cpy(L.fkind, T3);
   size_t o_vert = cpy(L.vert, T3), o_t3 = cpy(L.t2t3, T3), o_fref = cpy(L.fref, T3), o_sid = cpy(L.st_id, TK);
   size_t o_rcx = cpy(L.rc_x, T3), o_rcy = cpy(L.rc_y, T3), o_fnx = cpy(L.fnx, T3), o_fny = cpy(L.fny, T3);
@@ -354,6 +356,8 @@ int upload(StormFvtHandle* h) {
   d.delz_y = at<double>(B, o_dzy); d.zmax = at<double>(B, o_zmax); d.cd = at<double>(B, o_cd);
   d.lsq_a = at<double>(B, o_la); d.lsq_b = at<double>(B, o_lb); d.lsq_c = at<double>(B, o_lc);
   d.lsq_det = at<double>(B, o_ld);
+  d.wcoef1 = wind ? at<double>(B, o_wc1) : nullptr;
+  d.wcoef2 = wind ? at<double>(B, o_wc2) : nullptr;
   d.nst = at<uint8_t>(B, o_nst); d.forder = at<uint8_t>(B, o_ford); d.hvmask = at<uint8_t>(B, o_hvm);
   d.fkind = at<uint8_t>(B, o_fk);
   d.vert = at<int32_t>(B, o_vert); d.t2t3 = at<int32_t>(B, o_t3); d.fref = at<int32_t>(B, o_fref);

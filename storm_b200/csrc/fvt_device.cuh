@@ -50,6 +50,7 @@ struct Dev {
   double alpha[4][4], beta[4];
   // cells
   const double *area, *perim, *xc, *yc, *z, *delz_x, *delz_y, *zmax, *cd;
+  const double *wcoef1, *wcoef2;  // wind stress terms per cell (null: no wind)
   const double *lsq_a, *lsq_b, *lsq_c, *lsq_det;
   const uint8_t *nst, *forder, *hvmask, *fkind;
   const int32_t *vert, *t2t3, *fref, *st_id;

@@ -1090,6 +1090,10 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
     bed_source(d, G, c, h_c, &s2, &s3);
     p2 = p2 - s2;
     p3 = p3 - s3;
+    if (d.wcoef1) {  // wind forcing (solverFVT.f90:218-224)
+      p2 = p2 + d.wcoef1[c];
+      p3 = p3 + d.wcoef2[c];
+    }
   }
   *p1o = p1;
   *p2o = p2;

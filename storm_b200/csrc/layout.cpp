@@ -295,6 +295,7 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
   // ---- cells ---------------------------------------------------------------
   L.area.resize(T); L.perim.resize(T); L.xc.resize(T); L.yc.resize(T); L.z.resize(T);
   L.delz_x.resize(T); L.delz_y.resize(T); L.zmax.resize(T); L.cd.resize(T);
+  if (m.wcoef1 && m.wcoef2) { L.wcoef1.resize(T); L.wcoef2.resize(T); }
   L.lsq_a.resize(T); L.lsq_b.resize(T); L.lsq_c.resize(T); L.lsq_det.resize(T);
   L.nst.resize(T); L.forder.resize(T); L.hvmask.assign(T, 0);
   L.vert.resize(3 * (size_t)T); L.t2t3.resize(3 * (size_t)T); L.fref.assign(3 * (size_t)T, 0);
@@ -319,6 +320,10 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
     L.yc[c] = m.tri_yc[o];
     L.z[c] = m.z[o];
     L.cd[c] = m.cd[o];
+    if (m.wcoef1 && m.wcoef2) {
+      L.wcoef1[c] = m.wcoef1[o];
+      L.wcoef2[c] = m.wcoef2[o];
+    }
     L.lsq_a[c] = m.lsq_a[o];
     L.lsq_b[c] = m.lsq_b[o];
     L.lsq_c[c] = m.lsq_c[o];
@@ -506,6 +511,9 @@ void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& 
   M.flen.assign(T3, 0.0); M.fz0.assign(T3, 0.0);
   M.st_id.assign((size_t)kst * T, 0); M.st_w.assign((size_t)kst * T, 0.0);
   M.st_dx.assign((size_t)kst * T, 0.0); M.st_dy.assign((size_t)kst * T, 0.0);
+  bool any_wind = false;
+  for (size_t s = 0; s < S; s++) any_wind = any_wind || !parts[s].wcoef1.empty();
+  if (any_wind) { M.wcoef1.assign(T, 0.0); M.wcoef2.assign(T, 0.0); }
   M.node_sid.reserve(N); M.edge_sid.reserve(ne);
   int32_t eoff = 0, woff = 0, boff = 0, noff_nnz = 0, tsoff = 0;
   M.n2t_off.assign(1, 0);
@@ -520,6 +528,7 @@ void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& 
       M.z[g] = P.z[c]; M.delz_x[g] = P.delz_x[c]; M.delz_y[g] = P.delz_y[c]; M.zmax[g] = P.zmax[c];
       M.cd[g] = P.cd[c]; M.lsq_a[g] = P.lsq_a[c]; M.lsq_b[g] = P.lsq_b[c]; M.lsq_c[g] = P.lsq_c[c];
       M.lsq_det[g] = P.lsq_det[c]; M.nst[g] = P.nst[c]; M.forder[g] = P.forder[c]; M.hvmask[g] = P.hvmask[c];
+      if (!P.wcoef1.empty()) { M.wcoef1[g] = P.wcoef1[c]; M.wcoef2[g] = P.wcoef2[c]; }
       for (int j = 0; j < 3; j++) {
         const size_t q = (size_t)j * P.T + c, qg = (size_t)j * T + g;
         M.vert[qg] = P.vert[q] + no;

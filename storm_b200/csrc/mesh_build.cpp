@@ -52,7 +52,7 @@ inline uint64_t pair_key(int32_t a, int32_t b) {
 struct MeshStorage {
   std::vector<double> node_x, node_y, tri_area, tri_perim, tri_xc, tri_yc, edge_normal, edge_tang,
       edge_length, rc_x, rc_y, lsq_dx, lsq_dy, lsq_w, lsq_a, lsq_b, lsq_c, lsq_det, c2v_w, z, zvtx, cd,
-      qin, timelocq, timeserq, hbc, timeloch, timeserh;
+      qin, timelocq, timeserq, hbc, timeloch, timeserh, wcoef1, wcoef2;
   std::vector<int32_t> tri_vertex, tri_edge, edge_p, edge_e, t2t, t2t3, n2t, csortedz, flowedg1, walledg1,
       bcedges, hbar, qbar, vtype, bcedgesinflow, n_timeserq, htype, bcedgesoutflow, n_hbc, hbc_nodes,
       n_timeserh, n_qin, qin_nodes;
@@ -502,6 +502,29 @@ class Builder {
     vtx2ctr(m_.zvtx.data(), m_.z.data());
     if (p_.cd_at_vertices) vtx2ctr(p_.cd, m_.cd.data());
     else m_.cd.assign(p_.cd, p_.cd + T_);
+    // windforcing.f90 (text input, centred finite-volume solvers): per cell
+    // wcoef = c0 * w * |w| / rho, the inputs moved to the cells by vtx2ctr when they
+    // are given at the nodes
+    if (p_.wind_c0 && p_.wind_x && p_.wind_y) {
+      std::vector<double> c0(T_), wx(T_), wy(T_);
+      if (p_.wind_at_vertices) {
+        vtx2ctr(p_.wind_c0, c0.data());
+        vtx2ctr(p_.wind_x, wx.data());
+        vtx2ctr(p_.wind_y, wy.data());
+      } else {
+        c0.assign(p_.wind_c0, p_.wind_c0 + T_);
+        wx.assign(p_.wind_x, p_.wind_x + T_);
+        wy.assign(p_.wind_y, p_.wind_y + T_);
+      }
+      const double rho = 998.60;  // constants.f90:29
+      m_.wcoef1.resize(T_);
+      m_.wcoef2.resize(T_);
+      for (int32_t i = 0; i < T_; i++) {
+        const double windmag = std::sqrt(wx[i] * wx[i] + wy[i] * wy[i]);
+        m_.wcoef1[i] = c0[i] * wx[i] * windmag / rho;
+        m_.wcoef2[i] = c0[i] * wy[i] * windmag / rho;
+      }
+    }
     // rc (dataprepFVT.f90:161-173), before the normals are normalised
     m_.rc_x.resize(3 * (size_t)T_);
     m_.rc_y.resize(3 * (size_t)T_);
@@ -640,6 +663,8 @@ class Builder {
     v.timeloch = m_.timeloch.data();
     v.timeserh = m_.timeserh.data();
     v.bch_max = m_.bch_max;
+    v.wcoef1 = m_.wcoef1.empty() ? nullptr : m_.wcoef1.data();
+    v.wcoef2 = m_.wcoef2.empty() ? nullptr : m_.wcoef2.data();
   }
 };
 

@@ -46,6 +46,7 @@ struct HostLayout {
   std::vector<int32_t> node_new;
   // cells [T]
   std::vector<double> area, perim, xc, yc, z, delz_x, delz_y, zmax, cd;
+  std::vector<double> wcoef1, wcoef2;  // wind terms (empty: none)
   std::vector<double> lsq_a, lsq_b, lsq_c, lsq_det;
   std::vector<uint8_t> nst, forder, hvmask;
   std::vector<int32_t> bc_cells;  // cells with an open-boundary face, increasing

@@ -267,6 +267,24 @@ def dambreak(n_target: int = 1_000_000, radius: float = 500.0, col_radius: float
                     {"seed": seed, "spacing": h, "t_end": 60.0})
 
 
+def wind_fields(problem, at_vertices: bool, seed: int = 11, c0=(1.0e-3, 1.6e-3), wx=(-20.0, 20.0),
+                wy=(-5.0, 5.0)) -> dict:
+    """A spatially varying wind in the windforcing.f90 text-input form: drag
+    coefficient c0 and wind velocity (x, y) in m/s, uniform random in the given
+    ranges, on the vertices or the cells of a problem."""
+    n = problem.n_pts if at_vertices else problem.n_elems
+    rng = np.random.default_rng(seed)
+    return dict(c0=rng.uniform(*c0, n), x=rng.uniform(*wx, n), y=rng.uniform(*wy, n), at_vertices=at_vertices)
+
+
+def with_wind(sc: Scenario, wind: dict) -> Scenario:
+    """The same scenario with wind forcing terms."""
+    p = sc.problem
+    sc.problem = abi.ProblemHolder(p.x, p.y, p.tri, p.zb, p.cd, inflow=p.inflow_spec, outflow=p.outflow_spec,
+                                   wind=wind)
+    return sc
+
+
 def algorithmic_bytes_per_cell_stage(n_elems: int, n_edges: int, n_pts: int,
                                      mean_valence: float | None = None) -> float:
     """Compulsory HBM bytes of one perfectly fused FP64 RK stage per cell:

@@ -33,7 +33,14 @@ CASES = {
     "meander": lambda: scenarios.meander(n_target=12000, seed=7),
     "dambreak": lambda: scenarios.dambreak(n_target=12000, seed=8),
     "channel_cellbed": lambda: _cell_bed_channel(),
+    "channel_wind_cells": lambda: _wind_case(scenarios.channel(nx=40, ny=6), at_vertices=False),
+    "meander_wind_vertices": lambda: _wind_case(scenarios.meander(n_target=6000, seed=3), at_vertices=True),
 }
+
+
+
+def _wind_case(sc, at_vertices):
+    return scenarios.with_wind(sc, scenarios.wind_fields(sc.problem, at_vertices))
 
 
 def _cell_bed_channel():
@@ -53,7 +60,9 @@ def test_builder_matches_oracle(case, storm_lib, oracle_mod):
     sc = CASES[case]()
     o = oracle_mod.Oracle(sc.problem, sc.options)
     pm = fvt.build_mesh(sc.problem)
-    assert_mesh_equal(o.mesh_numpy(), pm.numpy())
+    mo = o.mesh_numpy()
+    assert_mesh_equal(mo, pm.numpy())
+    assert (mo["wcoef1"] is not None) == ("wind" in case)
 
 
 def test_channel_counts(storm_lib):

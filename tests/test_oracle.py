@@ -200,3 +200,25 @@ def test_residual_smoothing_options_checked(oracle_mod):
             setattr(o2, k, v)
         with pytest.raises(oracle_mod.OracleError):
             oracle_mod.Oracle(sc.problem, o2)
+
+
+def test_wind_drives_closed_basin_downwind(oracle_mod):
+    """Uniform wind in +x over a closed flat basin (solverFVT.f90:218-224 adds the
+    windforcing.f90 terms to phi of wet cells): mass is conserved, the water is pushed
+    downwind and the surface sets up at the downwind wall."""
+    sc = _basin()
+    T, N = sc.n_elems, sc.problem.n_pts
+    wind = dict(c0=np.full(N, 1.3e-3), x=np.full(N, 15.0), y=np.zeros(N), at_vertices=True)
+    sc = scenarios.with_wind(sc, wind)
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    m = o.mesh_numpy()
+    assert np.allclose(m["wcoef1"], 1.3e-3 * 15.0 * 15.0 / 998.60, rtol=1e-15) and not m["wcoef2"].any()
+    o.set_state(np.full(T, 1.0), np.zeros(T), np.zeros(T))
+    st = o.step(400)
+    s = o.state()
+    area = m["tri_area"]
+    assert st["tmass"] == pytest.approx(float(np.sum(area)), rel=1e-12)
+    mx, my = np.sum(s["h"] * s["u"] * area), np.sum(s["h"] * s["v"] * area)
+    assert mx > 0 and abs(my) < 0.2 * mx  # the diagonal triangulation turns some of it
+    xc = m["tri_xc"]
+    assert s["h"][xc > 25.0].mean() > s["h"][xc < 5.0].mean()
