@@ -142,6 +142,14 @@ typedef struct StormFvtProblem {
   const double* wind_x;
   const double* wind_y;
   int32_t wind_at_vertices;  /*  1: the three arrays are [n_pts]; 0: [n_elems]     */
+  /* culverts (the data file of ioculvert.f90), n_culvert = 0: none */
+  int32_t n_culvert;
+  int32_t cv_ld;             /* rows of the performance tables (>= every ncvtable) */
+  const double* cvptoin;     /* (3,n_culvert) inlet x, y and invert elevation      */
+  const double* cvptoout;    /* (2,n_culvert) outlet x, y                          */
+  const int32_t* ncvtable;   /* [n_culvert] rows of each performance curve (>= 1)  */
+  const double* cvhead;      /* (cv_ld,n_culvert) headwater elevations, ascending  */
+  const double* cvq;         /* (cv_ld,n_culvert) discharges                       */
 } StormFvtProblem;
 
 /*
@@ -219,6 +227,16 @@ typedef struct StormFvtMesh {
   double bch_max;                /* dataprepFVT.f90:278-286                         */
   const double* wcoef1;          /* [n_elems] wind terms added to phi(:,2:3) of wet */
   const double* wcoef2;          /*  cells (dep_vars.f90:33), NULL: no wind terms   */
+  /* culverts (dep_vars.f90:68-82; cvprep.f90 placed the ends), n_culvert = 0: none */
+  int32_t n_culvert;
+  int32_t cv_ld;                 /* SIZE(cvhead,1)                                  */
+  const int32_t* cvtrigin;       /* [n_culvert] 1-based triangle of the inlet       */
+  const int32_t* cvtrigout;      /* [n_culvert] 1-based triangle of the outlet      */
+  const double* cvptoin;         /* (3,n_culvert) inlet x, y, invert elevation      */
+  const double* cvrin;           /* (2,n_culvert) inlet minus the inlet centroid    */
+  const int32_t* ncvtable;       /* [n_culvert] rows of each performance curve      */
+  const double* cvhead;          /* (cv_ld,n_culvert) headwater elevations          */
+  const double* cvq;             /* (cv_ld,n_culvert) discharges                    */
 } StormFvtMesh;
 
 /* Per-call statistics, the scalars solverFVT prints per iteration

@@ -91,6 +91,10 @@ struct orc {
   int32_t *flowedg1, *walledg1, *bcedges, *hbar, *qbar;
   double *z, *zvtx, *cd;
   double *wcoef1, *wcoef2; /* dep_vars.f90:33, NULL: no wind terms */
+  /* culverts, dep_vars.f90:68-82 */
+  int32_t ncv, cv_ld;
+  int32_t *cvtrigin, *cvtrigout, *ncvtable;
+  double *cvptoin, *cvrin, *cvhead, *cvq, *cvsrc;
   /* boundaries */
   int32_t n_in, qin_ld, bcin_ld, tsq_ld;
   int32_t *vtype, *n_qin, *qin_nodes, *bcedgesinflow, *n_timeserq;
@@ -749,6 +753,93 @@ static int check_options(const StormFvtOptions* op) {
   return 0;
 }
 
+/* pto_in_triangle.f90:1-45: barycentric test of (x, y) against triangle e */
+static int pto_in_triangle(const orc_t* o, int32_t e, double x, double y) {
+  const double tarea = AREA(e);
+  const double x1 = NX(GV(e, 1)), y1 = NY(GV(e, 1));
+  const double x2 = NX(GV(e, 2)), y2 = NY(GV(e, 2));
+  const double x3 = NX(GV(e, 3)), y3 = NY(GV(e, 3));
+  const double s = half / tarea * (y1 * x3 - x1 * y3 + (y3 - y1) * x + (x1 - x3) * y);
+  const double t = half / tarea * (x1 * y2 - y1 * x2 + (y1 - y2) * x + (x2 - x1) * y);
+  if (s < zero) return 0;
+  if (t < zero) return 0;
+  if (one - s - t < zero) return 0;
+  return 1;
+}
+
+/* ioculvert.f90 checks + cvprep.f90:20-54: copy the culvert data, find the inlet and
+ * outlet triangles (first triangle in index order that holds the point) */
+static int cvprep(orc_t* o, const StormFvtProblem* p) {
+  const int32_t T = o->n_elems, n = p->n_culvert;
+  if (n <= 0) return 0;
+  if (!p->cvptoin || !p->cvptoout || !p->ncvtable || !p->cvhead || !p->cvq || p->cv_ld < 1)
+    return set_err(STORM_ERR_ARG, "culverts: missing data");
+  for (int32_t i = 0; i < n; i++)
+    if (p->ncvtable[i] < 1 || p->ncvtable[i] > p->cv_ld)
+      return set_err(STORM_ERR_ARG, "culvert %d: too few (or too many) entries in the performance curve", i + 1);
+  o->ncv = n;
+  o->cv_ld = p->cv_ld;
+  o->cvptoin = (double*)xcalloc((size_t)3 * n, sizeof(double));
+  o->cvrin = (double*)xcalloc((size_t)2 * n, sizeof(double));
+  o->cvtrigin = (int32_t*)xcalloc((size_t)n, sizeof(int32_t));
+  o->cvtrigout = (int32_t*)xcalloc((size_t)n, sizeof(int32_t));
+  o->ncvtable = (int32_t*)xcalloc((size_t)n, sizeof(int32_t));
+  o->cvhead = (double*)xcalloc((size_t)p->cv_ld * n, sizeof(double));
+  o->cvq = (double*)xcalloc((size_t)p->cv_ld * n, sizeof(double));
+  o->cvsrc = (double*)xcalloc((size_t)n, sizeof(double));
+  memcpy(o->cvptoin, p->cvptoin, sizeof(double) * 3 * (size_t)n);
+  memcpy(o->ncvtable, p->ncvtable, sizeof(int32_t) * (size_t)n);
+  memcpy(o->cvhead, p->cvhead, sizeof(double) * (size_t)p->cv_ld * n);
+  memcpy(o->cvq, p->cvq, sizeof(double) * (size_t)p->cv_ld * n);
+  for (int32_t i = 1; i <= n; i++) {
+    const double xi = p->cvptoin[3 * (i - 1)], yi = p->cvptoin[3 * (i - 1) + 1];
+    const double xo = p->cvptoout[2 * (i - 1)], yo = p->cvptoout[2 * (i - 1) + 1];
+    int32_t j;
+    for (j = 1; j <= T; j++)
+      if (pto_in_triangle(o, j, xi, yi)) break;
+    if (j > T) return set_err(STORM_ERR_MESH, "inlet of culvert %d not in computational domain", i);
+    o->cvtrigin[i - 1] = j;
+    o->cvrin[2 * (i - 1)] = xi - XC(j);
+    o->cvrin[2 * (i - 1) + 1] = yi - YC(j);
+    for (j = 1; j <= T; j++)
+      if (pto_in_triangle(o, j, xo, yo)) break;
+    if (j > T) return set_err(STORM_ERR_MESH, "outlet of culvert %d not in computational domain", i);
+    o->cvtrigout[i - 1] = j;
+  }
+  return 0;
+}
+
+/* cvdisch.f90:19-49: discharge of each culvert from the headwater at its inlet
+ * (zeta + the reconstructed stage gradient, minus the invert), interpolated in the
+ * performance curve */
+static void cvdisch(orc_t* o) {
+  const int32_t ld = o->cv_ld;
+  for (int32_t i = 1; i <= o->ncv; i++) o->cvsrc[i - 1] = zero;
+  for (int32_t i = 1; i <= o->ncv; i++) {
+    const int32_t c = o->cvtrigin[i - 1];
+    if (DRY(c)) continue;
+    double head = ZETA(c) + (o->delh_x[c - 1] + o->delz_x[c - 1]) * o->cvrin[2 * (i - 1)] +
+                  (o->delh_y[c - 1] + o->delz_y[c - 1]) * o->cvrin[2 * (i - 1) + 1];
+    head = head - o->cvptoin[3 * (i - 1) + 2];
+    if (head < o->opt.h_dry) continue;
+    const double* hd = o->cvhead + (size_t)(i - 1) * ld;
+    const double* q = o->cvq + (size_t)(i - 1) * ld;
+    const int32_t nt = o->ncvtable[i - 1];
+    if (head < hd[0]) {
+      o->cvsrc[i - 1] = q[0];
+    } else if (head >= hd[nt - 1]) {
+      o->cvsrc[i - 1] = q[nt - 1];
+    } else {
+      for (int32_t j = 1; j <= nt - 1; j++)
+        if (head < hd[j]) {
+          const double t = (head - hd[j - 1]) / (hd[j] - hd[j - 1]);
+          o->cvsrc[i - 1] = q[j] * t + q[j - 1] * (one - t);
+          break;
+        }
+    }
+  }
+}
+
 int orc_create(const StormFvtProblem* p, const StormFvtOptions* opt, orc_t** out) {
   g_err[0] = 0;
   if (!p || !opt || !out) return set_err(STORM_ERR_ARG, "null argument");
@@ -912,6 +1003,7 @@ int orc_create(const StormFvtProblem* p, const StormFvtOptions* opt, orc_t** out
   o->rkv = (double*)xcalloc(L * T, sizeof(double));
   o->fedge = (double*)xcalloc((size_t)3 * (o->flow_edges1 + 1), sizeof(double));
   o->fedge_set = (int32_t*)xcalloc((size_t)o->flow_edges1 + 1, sizeof(int32_t));
+  if ((rc = cvprep(o, p))) { orc_destroy(o); return rc; } /* dataprepFVT.f90:308-309 */
   *out = o;
   return 0;
 }
@@ -927,7 +1019,8 @@ void orc_destroy(orc_t* o) {
                   o->bcedgesoutflow, o->n_timeserh, o->hbc, o->timeloch, o->timeserh, o->h, o->u, o->v,
                   o->zeta, o->u_mag, o->wavec, o->hvtx, o->zetavtx, o->rough, o->delh_x, o->delh_y, o->delu_x,
                   o->delu_y, o->delv_x, o->delv_y, o->delz_x, o->delz_y, o->phi, o->drycell, o->rkh, o->rku,
-                  o->rkv, o->fedge, o->fedge_set, o->phi0, o->rs_seq, o->wcoef1, o->wcoef2};
+                  o->rkv, o->fedge, o->fedge_set, o->phi0, o->rs_seq, o->wcoef1, o->wcoef2,
+                  o->cvtrigin, o->cvtrigout, o->ncvtable, o->cvptoin, o->cvrin, o->cvhead, o->cvq, o->cvsrc};
   for (size_t i = 0; i < sizeof ptrs / sizeof ptrs[0]; i++) free(ptrs[i]);
   free(o);
 }
@@ -962,6 +1055,9 @@ int orc_export_mesh(const orc_t* o, StormFvtMesh* m) {
   m->bch_max = o->bch_max;
   m->wcoef1 = o->wcoef1;
   m->wcoef2 = o->wcoef2;
+  m->n_culvert = o->ncv; m->cv_ld = o->cv_ld;
+  m->cvtrigin = o->cvtrigin; m->cvtrigout = o->cvtrigout; m->cvptoin = o->cvptoin; m->cvrin = o->cvrin;
+  m->ncvtable = o->ncvtable; m->cvhead = o->cvhead; m->cvq = o->cvq;
   return 0;
 }
 
@@ -1876,6 +1972,13 @@ static int rk_stage(orc_t* o, int rkstep, int upto, double* delt_io) {
       PHI(i, 2) = PHI(i, 2) + o->wcoef1[i - 1];
       PHI(i, 3) = PHI(i, 3) + o->wcoef2[i - 1];
     }
+  if (o->ncv > 0) { /* solverFVT.f90:227-233 */
+    cvdisch(o);
+    for (int32_t i = 1; i <= o->ncv; i++) {
+      PHI(o->cvtrigin[i - 1], 1) = PHI(o->cvtrigin[i - 1], 1) - o->cvsrc[i - 1];
+      PHI(o->cvtrigout[i - 1], 1) = PHI(o->cvtrigout[i - 1], 1) + o->cvsrc[i - 1];
+    }
+  }
   if (op->rsavg_passes > 0) rsavg(o);
   if (upto <= 4) return bad;
   /* :259-283 */

@@ -88,6 +88,8 @@ class Problem(C.Structure):
         ("n_inflow", C.c_int32), ("inflow", C.POINTER(Boundary)),
         ("n_outflow", C.c_int32), ("outflow", C.POINTER(Boundary)),
         ("wind_c0", _d), ("wind_x", _d), ("wind_y", _d), ("wind_at_vertices", C.c_int32),
+        ("n_culvert", C.c_int32), ("cv_ld", C.c_int32), ("cvptoin", _d), ("cvptoout", _d),
+        ("ncvtable", _i), ("cvhead", _d), ("cvq", _d),
     ]
 
 
@@ -120,6 +122,8 @@ class Mesh(C.Structure):
         ("tsh_ld", C.c_int32), ("n_timeserh", _i), ("timeloch", _d), ("timeserh", _d),
         ("bch_max", C.c_double),
         ("wcoef1", _d), ("wcoef2", _d),
+        ("n_culvert", C.c_int32), ("cv_ld", C.c_int32), ("cvtrigin", _i), ("cvtrigout", _i),
+        ("cvptoin", _d), ("cvrin", _d), ("ncvtable", _i), ("cvhead", _d), ("cvq", _d),
     ]
 
 
@@ -162,7 +166,7 @@ class ProblemHolder:
     """
 
     def __init__(self, x, y, tri, zb, cd, *, zb_at_vertices=True, cd_at_vertices=False,
-                 inflow=(), outflow=(), edge_p=None, edge_e=None, wind=None):
+                 inflow=(), outflow=(), edge_p=None, edge_e=None, wind=None, culverts=()):
         self._keep = []
         self.x = np.ascontiguousarray(x, dtype=np.float64)
         self.y = np.ascontiguousarray(y, dtype=np.float64)
@@ -194,6 +198,23 @@ class ProblemHolder:
             self.wind_y = np.ascontiguousarray(wind["y"], dtype=np.float64)
             p.wind_c0, p.wind_x, p.wind_y = dptr(self.wind_c0), dptr(self.wind_x), dptr(self.wind_y)
             p.wind_at_vertices = int(bool(wind.get("at_vertices", False)))
+        # culverts: list of dicts(inlet=(x, y, invert), outlet=(x, y), head=[...], q=[...]),
+        # the ioculvert.f90 input (performance curve in ascending head)
+        self.culverts = [dict(c) for c in culverts]
+        if self.culverts:
+            n = len(self.culverts)
+            ld = max(len(c["head"]) for c in self.culverts)
+            self.cvptoin = np.ascontiguousarray([c["inlet"] for c in self.culverts], dtype=np.float64).reshape(-1)
+            self.cvptoout = np.ascontiguousarray([c["outlet"] for c in self.culverts], dtype=np.float64).reshape(-1)
+            self.ncvtable = np.array([len(c["head"]) for c in self.culverts], dtype=np.int32)
+            self.cvhead = np.zeros(ld * n)
+            self.cvq = np.zeros(ld * n)
+            for i, c in enumerate(self.culverts):
+                self.cvhead[i * ld:i * ld + len(c["head"])] = c["head"]
+                self.cvq[i * ld:i * ld + len(c["q"])] = c["q"]
+            p.n_culvert, p.cv_ld = n, ld
+            p.cvptoin, p.cvptoout, p.ncvtable = dptr(self.cvptoin), dptr(self.cvptoout), iptr(self.ncvtable)
+            p.cvhead, p.cvq = dptr(self.cvhead), dptr(self.cvq)
         self.problem = p
 
     def _bdr(self, specs):
@@ -263,6 +284,12 @@ def mesh_to_numpy(m: Mesh) -> dict:
         d[name] = _arr(getattr(m, name), n, dt)
     for name in ("wcoef1", "wcoef2"):
         d[name] = _arr(getattr(m, name), T, f64) if getattr(m, name) else None
+    n, ld = m.n_culvert, m.cv_ld
+    for name, k, dt in (("cvtrigin", n, i32), ("cvtrigout", n, i32), ("cvptoin", 3 * n, f64),
+                        ("cvrin", 2 * n, f64), ("ncvtable", n, i32), ("cvhead", ld * n, f64),
+                        ("cvq", ld * n, f64)):
+        d[name] = _arr(getattr(m, name), k, dt) if n > 0 else None
+    d["n_culvert"], d["cv_ld"] = (n, ld) if n > 0 else (0, 0)
     for name in ("t2t_ncol", "n2t_ncol", "c2v_ncol", "flow_edges1", "wall_edges1", "n_bcedges",
                  "n_inflowbdr", "n_outflowbdr", "bcin_ld", "bcout_ld", "hbc_ld", "tsq_ld",
                  "tsh_ld", "bch_max"):

@@ -175,6 +175,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     k_node<<<gN, h->bs_node, 0, h->stream>>>(d, hs, dry);
     if (done() || mark(KT_GRAD)) return STORM_ERR_CUDA;
     launch(STAGE_GRAD, gT, h->bs_grad, 0, h->stream, s, hs, dry, dry_next);
+    if (d.ncv > 0) launch(STAGE_CULVERT, (d.ncv + 127) / 128, 128, 0, h->stream, s, hs, dry, dry_next);
     if (done()) return STORM_ERR_CUDA;
     const bool rs = h->opt.rsavg_passes > 0;
     const int sF = rs ? STAGE_PHI : STAGE_FLUX, sFB = rs ? STAGE_PHI_BC : STAGE_FLUX_BC;
@@ -291,6 +292,12 @@ int upload(StormFvtHandle* h) {
   size_t o_ld = cpy(L.lsq_det, T);
   const bool wind = !L.wcoef1.empty();
   size_t o_wc1 = wind ? cpy(L.wcoef1, T) : 0, o_wc2 = wind ? cpy(L.wcoef2, T) : 0;
+  const size_t ncv = std::max(L.ncv, 1), ncvc = std::max<size_t>(L.cvc_cell.size(), 1);
+  const size_t ncvt = std::max<size_t>(L.cv_head.size(), 1);
+  size_t o_cvin = cpy(L.cv_in, ncv), o_cvn = cpy(L.cv_n, ncv), o_cvrx = cpy(L.cv_rx, ncv);
+  size_t o_cvry = cpy(L.cv_ry, ncv), o_cvz = cpy(L.cv_zinv, ncv), o_cvh = cpy(L.cv_head, ncvt);
+  size_t o_cvq = cpy(L.cv_q, ncvt), o_cvcc = cpy(L.cvc_cell, ncvc), o_cvco = cpy(L.cvc_code, ncvc);
+  size_t o_cvsrc = A.take(sizeof(double) * ncv);
   size_t o_nst = cpy(L.nst, T), o_ford = cpy(L.forder, T), o_hvm = cpy(L.hvmask, T), o_fk = cpy(L.fkind, T3);
   size_t o_vert = cpy(L.vert, T3), o_t3 = cpy(L.t2t3, T3), o_fref = cpy(L.fref, T3), o_sid = cpy(L.st_id, TK);
   size_t o_rcx = cpy(L.rc_x, T3), o_rcy = cpy(L.rc_y, T3), o_fnx = cpy(L.fnx, T3), o_fny = cpy(L.fny, T3);
@@ -358,6 +365,11 @@ int upload(StormFvtHandle* h) {
   d.lsq_det = at<double>(B, o_ld);
   d.wcoef1 = wind ? at<double>(B, o_wc1) : nullptr;
   d.wcoef2 = wind ? at<double>(B, o_wc2) : nullptr;
+  d.ncv = L.ncv; d.cv_ld = L.cv_ld; d.ncvc = (int32_t)L.cvc_cell.size();
+  d.cv_in = at<int32_t>(B, o_cvin); d.cv_n = at<int32_t>(B, o_cvn); d.cv_rx = at<double>(B, o_cvrx);
+  d.cv_ry = at<double>(B, o_cvry); d.cv_zinv = at<double>(B, o_cvz); d.cv_head = at<double>(B, o_cvh);
+  d.cv_q = at<double>(B, o_cvq); d.cvc_cell = at<int32_t>(B, o_cvcc); d.cvc_code = at<int32_t>(B, o_cvco);
+  d.cvsrc = at<double>(B, o_cvsrc);
   d.nst = at<uint8_t>(B, o_nst); d.forder = at<uint8_t>(B, o_ford); d.hvmask = at<uint8_t>(B, o_hvm);
   d.fkind = at<uint8_t>(B, o_fk);
   d.vert = at<int32_t>(B, o_vert); d.t2t3 = at<int32_t>(B, o_t3); d.fref = at<int32_t>(B, o_fref);

@@ -51,6 +51,12 @@ struct Dev {
   // cells
   const double *area, *perim, *xc, *yc, *z, *delz_x, *delz_y, *zmax, *cd;
   const double *wcoef1, *wcoef2;  // wind stress terms per cell (null: no wind)
+  // culverts: inlet cell, table rows, inlet offset from the centroid, invert elevation,
+  // performance curves [ncv][cv_ld]; per-cell term list (cvc_*); discharges cvsrc
+  int32_t ncv, cv_ld, ncvc;
+  const int32_t *cv_in, *cv_n, *cvc_cell, *cvc_code;
+  const double *cv_rx, *cv_ry, *cv_zinv, *cv_head, *cv_q;
+  double* cvsrc;
   const double *lsq_a, *lsq_b, *lsq_c, *lsq_det;
   const uint8_t *nst, *forder, *hvmask, *fkind;
   const int32_t *vert, *t2t3, *fref, *st_id;
@@ -106,7 +112,7 @@ struct Geo {
 
 // One launch of a templated stage kernel (see launch_stage in fvt_kernels.cu).
 enum StageKernel { STAGE_GRAD, STAGE_BC, STAGE_EFLUX, STAGE_FLUX, STAGE_FLUX_BC, STAGE_PHI, STAGE_PHI_BC,
-                   STAGE_UPDATE };
+                   STAGE_UPDATE, STAGE_CULVERT };
 struct StageLaunch {
   int which;
   dim3 grid, block;

@@ -1095,6 +1095,19 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
       p3 = p3 + d.wcoef2[c];
     }
   }
+  if (ord & kOrderHasCulvert) {  // culvert sources and sinks (solverFVT.f90:227-233)
+    int lo = 0, hi = d.ncvc;  // first term of cell c
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (d.cvc_cell[mid] < c) lo = mid + 1;
+      else hi = mid;
+    }
+    for (int k = lo; k < d.ncvc && d.cvc_cell[k] == c; k++) {
+      const int code = d.cvc_code[k];
+      if (code & 1) p1 = p1 + d.cvsrc[code >> 1];
+      else p1 = p1 - d.cvsrc[code >> 1];
+    }
+  }
   *p1o = p1;
   *p2o = p2;
   *p3o = p3;
@@ -1637,6 +1650,42 @@ void launch_output(const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bo
   }
 }
 
+// Discharge of every culvert (cvdisch.f90:19-49), one thread per culvert, after the
+// stage's gradients: the headwater at the inlet is the stage reconstructed from the
+// inlet cell's centroid (zeta + (delh + delz) . rcv) minus the invert elevation, and
+// the discharge is interpolated linearly in the culvert's performance curve.
+template <class R>
+__global__ void k_culvert(Dev d, Geo<R> G, const double* __restrict__ hs, const uint8_t* __restrict__ dry) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.ncv) return;
+  double src = kZero;
+  const int c = d.cv_in[i];
+  if (!dry[c]) {
+    const double zeta = hs[c] + d.z[c];
+    const double dhx = (double)G.delh_x[c], dhy = (double)G.delh_y[c];
+    double head = zeta + (dhx + d.delz_x[c]) * d.cv_rx[i] + (dhy + d.delz_y[c]) * d.cv_ry[i];
+    head = head - d.cv_zinv[i];
+    if (!(head < d.h_dry)) {
+      const double* hd = d.cv_head + (size_t)i * d.cv_ld;
+      const double* q = d.cv_q + (size_t)i * d.cv_ld;
+      const int nt = d.cv_n[i];
+      if (head < hd[0]) {
+        src = q[0];
+      } else if (head >= hd[nt - 1]) {
+        src = q[nt - 1];
+      } else {
+        for (int j = 1; j <= nt - 1; j++)
+          if (head < hd[j]) {
+            const double t = (head - hd[j - 1]) / (hd[j] - hd[j - 1]);
+            src = q[j] * t + q[j - 1] * (kOne - t);
+            break;
+          }
+      }
+    }
+  }
+  d.cvsrc[i] = src;
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers of the templated stage kernels (api.cu is not templated).
 template <class R>
@@ -1665,6 +1714,9 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
       break;
     case STAGE_UPDATE:
       k_update<<<L.grid, L.block, 0, L.stream>>>(d, L.s, L.hs, L.dry, L.dry_next);
+      break;
+    case STAGE_CULVERT:
+      k_culvert<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry);
       break;
   }
 }

@@ -413,6 +413,37 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
       if (L.fkind[(size_t)j * T + c] == FACE_BC) L.forder[c] |= kOrderHasBc;
     if (L.forder[c] & kOrderHasBc) L.bc_cells.push_back(c);
   }
+  // culverts (cvprep.f90 placed them; solverFVT.f90:227-233 adds their terms)
+  if (m.n_culvert > 0) {
+    const int32_t n = m.n_culvert, ld = m.cv_ld;
+    if (!m.cvtrigin || !m.cvtrigout || !m.cvptoin || !m.cvrin || !m.ncvtable || !m.cvhead || !m.cvq || ld < 1)
+      return set_error(STORM_ERR_MESH, "storm_fvt_create: culvert arrays missing");
+    L.ncv = n;
+    L.cv_ld = ld;
+    L.cv_in.resize(n); L.cv_n.resize(n); L.cv_rx.resize(n); L.cv_ry.resize(n); L.cv_zinv.resize(n);
+    L.cv_head.assign(m.cvhead, m.cvhead + (size_t)ld * n);
+    L.cv_q.assign(m.cvq, m.cvq + (size_t)ld * n);
+    std::vector<std::pair<int32_t, int32_t>> terms;  // (cell, code), in the reference's order
+    for (int32_t i = 0; i < n; i++) {
+      const int32_t a = m.cvtrigin[i], b = m.cvtrigout[i];
+      if (a < 1 || a > T || b < 1 || b > T) return set_error(STORM_ERR_MESH, "storm_fvt_create: culvert triangle out of range");
+      if (m.ncvtable[i] < 1 || m.ncvtable[i] > ld)
+        return set_error(STORM_ERR_MESH, "storm_fvt_create: culvert performance curve size out of range");
+      L.cv_in[i] = CN(a);
+      L.cv_n[i] = m.ncvtable[i];
+      L.cv_rx[i] = m.cvrin[2 * (size_t)i];
+      L.cv_ry[i] = m.cvrin[2 * (size_t)i + 1];
+      L.cv_zinv[i] = m.cvptoin[3 * (size_t)i + 2];
+      terms.push_back({CN(a), i << 1});
+      terms.push_back({CN(b), (i << 1) | 1});
+    }
+    std::stable_sort(terms.begin(), terms.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    for (const auto& t : terms) {
+      L.cvc_cell.push_back(t.first);
+      L.cvc_code.push_back(t.second);
+      L.forder[t.first] |= kOrderHasCulvert;
+    }
+  }
   // Greedy colouring of the t2t stencil made symmetric, cells in reference index order,
   // each taking the smallest colour none of its already coloured neighbours has (the
   // order residual smoothing visits them; the oracle builds the same colouring).
@@ -591,6 +622,29 @@ void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& 
     noff_nnz += P.n2t_nnz;
   }
   M.nbdr = (int32_t)M.bdr_kind.size();
+  // culverts: concatenated, performance curves padded to the widest table
+  M.ncv = 0;
+  M.cv_ld = 0;
+  for (const HostLayout& P : parts) { M.ncv += P.ncv; M.cv_ld = std::max(M.cv_ld, P.cv_ld); }
+  M.cv_head.assign((size_t)M.ncv * M.cv_ld, 0.0);
+  M.cv_q.assign((size_t)M.ncv * M.cv_ld, 0.0);
+  for (size_t s = 0, cvo = 0; s < S; s++) {
+    const HostLayout& P = parts[s];
+    const int32_t co = info[s].cell_off;
+    for (int32_t i = 0; i < P.ncv; i++) {
+      M.cv_in.push_back(P.cv_in[i] + co); M.cv_n.push_back(P.cv_n[i]);
+      M.cv_rx.push_back(P.cv_rx[i]); M.cv_ry.push_back(P.cv_ry[i]); M.cv_zinv.push_back(P.cv_zinv[i]);
+      for (int32_t j = 0; j < P.cv_n[i]; j++) {
+        M.cv_head[(cvo + i) * M.cv_ld + j] = P.cv_head[(size_t)i * P.cv_ld + j];
+        M.cv_q[(cvo + i) * M.cv_ld + j] = P.cv_q[(size_t)i * P.cv_ld + j];
+      }
+    }
+    for (size_t k = 0; k < P.cvc_cell.size(); k++) {
+      M.cvc_cell.push_back(P.cvc_cell[k] + co);
+      M.cvc_code.push_back(P.cvc_code[k] + (int32_t)(cvo << 1));
+    }
+    cvo += P.ncv;
+  }
   // residual-smoothing colours: colour c of every scenario together (scenarios share no cell)
   size_t ncol = 0;
   for (const HostLayout& P : parts) ncol = std::max(ncol, P.rs_off.empty() ? 0 : P.rs_off.size() - 1);

@@ -52,10 +52,10 @@ inline uint64_t pair_key(int32_t a, int32_t b) {
 struct MeshStorage {
   std::vector<double> node_x, node_y, tri_area, tri_perim, tri_xc, tri_yc, edge_normal, edge_tang,
       edge_length, rc_x, rc_y, lsq_dx, lsq_dy, lsq_w, lsq_a, lsq_b, lsq_c, lsq_det, c2v_w, z, zvtx, cd,
-      qin, timelocq, timeserq, hbc, timeloch, timeserh, wcoef1, wcoef2;
+      qin, timelocq, timeserq, hbc, timeloch, timeserh, wcoef1, wcoef2, cvptoin, cvrin, cvhead, cvq;
   std::vector<int32_t> tri_vertex, tri_edge, edge_p, edge_e, t2t, t2t3, n2t, csortedz, flowedg1, walledg1,
       bcedges, hbar, qbar, vtype, bcedgesinflow, n_timeserq, htype, bcedgesoutflow, n_hbc, hbc_nodes,
-      n_timeserh, n_qin, qin_nodes;
+      n_timeserh, n_qin, qin_nodes, cvtrigin, cvtrigout, ncvtable;
   int32_t t2t_ncol = 0, n2t_ncol = 0, c2v_ncol = 0, qin_ld = 1, hbc_ld = 1, tsq_ld = 1, tsh_ld = 1;
   double bch_max = 0.0;
   StormFvtMesh view{};
@@ -80,6 +80,7 @@ class Builder {
     node_db();
     elemnt_db();
     dataprep();
+    culverts();
     fill_view();
   }
 
@@ -595,6 +596,58 @@ class Builder {
     }
   }
 
+  // pto_in_triangle.f90: barycentric test of (x, y) against triangle e
+  bool pto_in_triangle(int32_t e, double x, double y) {
+    const double tarea = m_.tri_area[e - 1];
+    const double x1 = nx(gv(e, 1)), y1 = ny(gv(e, 1));
+    const double x2 = nx(gv(e, 2)), y2 = ny(gv(e, 2));
+    const double x3 = nx(gv(e, 3)), y3 = ny(gv(e, 3));
+    const double s = kHalf / tarea * (y1 * x3 - x1 * y3 + (y3 - y1) * x + (x1 - x3) * y);
+    const double t = kHalf / tarea * (x1 * y2 - y1 * x2 + (y1 - y2) * x + (x2 - x1) * y);
+    if (s < 0.0) return false;
+    if (t < 0.0) return false;
+    if (1.0 - s - t < 0.0) return false;
+    return true;
+  }
+
+  // The first triangle in index order that holds (x, y), 0 if none.
+  int32_t locate(double x, double y) {
+    for (int32_t j = 1; j <= T_; j++)
+      if (pto_in_triangle(j, x, y)) return j;
+    return 0;
+  }
+
+  // ioculvert.f90 checks + cvprep.f90:20-54 (run at dataprepFVT.f90:308-309)
+  void culverts() {
+    const int32_t n = p_.n_culvert;
+    if (n <= 0) return;
+    if (!p_.cvptoin || !p_.cvptoout || !p_.ncvtable || !p_.cvhead || !p_.cvq || p_.cv_ld < 1)
+      fail(STORM_ERR_ARG, "culverts: missing data");
+    const size_t ld = (size_t)p_.cv_ld;
+    for (int32_t i = 0; i < n; i++)
+      if (p_.ncvtable[i] < 1 || p_.ncvtable[i] > p_.cv_ld)
+        fail(STORM_ERR_ARG, "culvert " + std::to_string(i + 1) +
+                                ": too few (or too many) entries in the performance curve");
+    m_.cvptoin.assign(p_.cvptoin, p_.cvptoin + 3 * (size_t)n);
+    m_.ncvtable.assign(p_.ncvtable, p_.ncvtable + n);
+    m_.cvhead.assign(p_.cvhead, p_.cvhead + ld * n);
+    m_.cvq.assign(p_.cvq, p_.cvq + ld * n);
+    m_.cvtrigin.resize(n);
+    m_.cvtrigout.resize(n);
+    m_.cvrin.resize(2 * (size_t)n);
+    for (int32_t i = 0; i < n; i++) {
+      const double xi = p_.cvptoin[3 * (size_t)i], yi = p_.cvptoin[3 * (size_t)i + 1];
+      const int32_t a = locate(xi, yi);
+      if (a == 0) fail(STORM_ERR_MESH, "inlet of culvert " + std::to_string(i + 1) + " not in computational domain");
+      m_.cvtrigin[i] = a;
+      m_.cvrin[2 * (size_t)i] = xi - m_.tri_xc[a - 1];
+      m_.cvrin[2 * (size_t)i + 1] = yi - m_.tri_yc[a - 1];
+      const int32_t b = locate(p_.cvptoout[2 * (size_t)i], p_.cvptoout[2 * (size_t)i + 1]);
+      if (b == 0) fail(STORM_ERR_MESH, "outlet of culvert " + std::to_string(i + 1) + " not in computational domain");
+      m_.cvtrigout[i] = b;
+    }
+  }
+
   void fill_view() {
     StormFvtMesh& v = m_.view;
     std::memset(&v, 0, sizeof v);
@@ -665,6 +718,17 @@ class Builder {
     v.bch_max = m_.bch_max;
     v.wcoef1 = m_.wcoef1.empty() ? nullptr : m_.wcoef1.data();
     v.wcoef2 = m_.wcoef2.empty() ? nullptr : m_.wcoef2.data();
+    if (!m_.cvtrigin.empty()) {
+      v.n_culvert = p_.n_culvert;
+      v.cv_ld = p_.cv_ld;
+      v.cvtrigin = m_.cvtrigin.data();
+      v.cvtrigout = m_.cvtrigout.data();
+      v.cvptoin = m_.cvptoin.data();
+      v.cvrin = m_.cvrin.data();
+      v.ncvtable = m_.ncvtable.data();
+      v.cvhead = m_.cvhead.data();
+      v.cvq = m_.cvq.data();
+    }
   }
 };
 

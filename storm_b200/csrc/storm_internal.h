@@ -33,6 +33,7 @@ enum BcKind : int32_t {
 };
 
 constexpr uint8_t kOrderHasBc = 0x40;  // forder flag: the cell has an open-boundary face
+constexpr uint8_t kOrderHasCulvert = 0x80;  // forder flag: a culvert end lies in the cell
 constexpr int kMaxStencil = 19;   // elemnt_db.f90:42 maxdim = 20 (count + 19 ids)
 constexpr int kMaxBcEdges = 8192; // edges per open boundary handled by one CTA
 
@@ -83,6 +84,13 @@ struct HostLayout {
   std::vector<double> ts_t, ts_v;
   double bch_max = 0.0;
   int32_t last_cell_new = 0;  // new id of element n_elems (steady friction dt)
+  // culverts [ncv] (cells in new ids); performance curves [ncv][cv_ld]
+  int32_t ncv = 0, cv_ld = 0;
+  std::vector<int32_t> cv_in, cv_n;
+  std::vector<double> cv_rx, cv_ry, cv_zinv, cv_head, cv_q;
+  // culvert terms of phi(:,1), sorted by cell and, within a cell, in the order the
+  // reference adds them: code = culvert << 1 | (1: outlet, adds; 0: inlet, subtracts)
+  std::vector<int32_t> cvc_cell, cvc_code;
   // merged layouts only
   std::vector<int32_t> cell_sid, node_sid, edge_sid, bdr_sid;
 };

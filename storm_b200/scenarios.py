@@ -281,8 +281,36 @@ def with_wind(sc: Scenario, wind: dict) -> Scenario:
     """The same scenario with wind forcing terms."""
     p = sc.problem
     sc.problem = abi.ProblemHolder(p.x, p.y, p.tri, p.zb, p.cd, inflow=p.inflow_spec, outflow=p.outflow_spec,
-                                   wind=wind)
+                                   wind=wind, culverts=p.culverts)
     return sc
+
+
+def with_culverts(sc: Scenario, culverts) -> Scenario:
+    """The same scenario with culverts (ioculvert.f90 input, see ProblemHolder)."""
+    p = sc.problem
+    sc.problem = abi.ProblemHolder(p.x, p.y, p.tri, p.zb, p.cd, inflow=p.inflow_spec, outflow=p.outflow_spec,
+                                   wind=p.wind, culverts=culverts)
+    return sc
+
+
+def culvert_channel(nx: int = 60, ny: int = 8, q: float = 2.0, crest: float = 1.5, **kw) -> Scenario:
+    """A 60 x 8 m channel crossed by an embankment (bed raised by `crest` m for
+    28 m <= x <= 32 m) with two culverts through it: water ponds upstream, the
+    culverts carry it across by their performance curves (head above the invert
+    -> discharge), and it flows on to the outlet."""
+    sc = channel(nx=nx, ny=ny, length=60.0, width=8.0, q=q, **kw)
+    p = sc.problem
+    zb = p.zb.copy()
+    zb[(p.x >= 28.0) & (p.x <= 32.0)] += crest
+    sc.problem = abi.ProblemHolder(p.x, p.y, p.tri, zb, p.cd, inflow=p.inflow_spec, outflow=p.outflow_spec)
+    # dry embankment cells at the start (their bed is above the initial surface)
+    xc = p.x[p.tri.reshape(-1, 3) - 1].mean(axis=1)
+    sc.h0 = np.where((xc > 28.0) & (xc < 32.0), 0.0, sc.h0)
+    zin = 0.001 * (60.0 - 25.0) - 0.05  # invert just below the bed plane at x = 25
+    curve = dict(head=[0.1, 0.5, 1.0, 2.0], q=[0.0, 0.6, 1.5, 3.5])
+    cvs = [dict(inlet=(25.1, 2.05, zin), outlet=(35.2, 2.1), **curve),
+           dict(inlet=(25.3, 5.95, zin), outlet=(35.1, 6.0), head=[0.2, 1.2], q=[0.1, 1.1])]
+    return with_culverts(sc, cvs)
 
 
 def algorithmic_bytes_per_cell_stage(n_elems: int, n_edges: int, n_pts: int,

@@ -35,6 +35,7 @@ CASES = {
     "channel_cellbed": lambda: _cell_bed_channel(),
     "channel_wind_cells": lambda: _wind_case(scenarios.channel(nx=40, ny=6), at_vertices=False),
     "meander_wind_vertices": lambda: _wind_case(scenarios.meander(n_target=6000, seed=3), at_vertices=True),
+    "culvert_channel": lambda: scenarios.culvert_channel(),
 }
 
 
@@ -63,6 +64,7 @@ def test_builder_matches_oracle(case, storm_lib, oracle_mod):
     mo = o.mesh_numpy()
     assert_mesh_equal(mo, pm.numpy())
     assert (mo["wcoef1"] is not None) == ("wind" in case)
+    assert (mo["n_culvert"] > 0) == ("culvert" in case)
 
 
 def test_channel_counts(storm_lib):

@@ -222,3 +222,66 @@ def test_wind_drives_closed_basin_downwind(oracle_mod):
     assert mx > 0 and abs(my) < 0.2 * mx  # the diagonal triangulation turns some of it
     xc = m["tri_xc"]
     assert s["h"][xc > 25.0].mean() > s["h"][xc < 5.0].mean()
+
+
+def _flat_basin_with_culverts(cvs):
+    sc = _basin()
+    return scenarios.with_culverts(sc, cvs)
+
+
+def test_culvert_discharge_known_answers(oracle_mod):
+    """cvdisch.f90:19-49 on a flat lake at rest (stage 1.0, zero gradients, so the
+    headwater is 1.0 minus the invert): interpolated, below-the-table, above-the-table
+    and below-h_dry discharges, entered in phi(:,1) at both ends (solverFVT.f90:227-233)."""
+    curve = dict(head=[0.5, 1.5], q=[1.0, 3.0])
+    cvs = [dict(inlet=(3.3, 3.6, 0.0), outlet=(26.3, 3.6), **curve),      # head 1.0: 2.0
+           dict(inlet=(3.3, 10.6, 0.9), outlet=(26.3, 10.6), **curve),    # head 0.1: q(1) = 1.0
+           dict(inlet=(3.3, 17.6, -1.0), outlet=(26.3, 17.6), **curve),   # head 2.0: q(2) = 3.0
+           dict(inlet=(3.3, 24.6, 0.9995), outlet=(26.3, 24.6), **curve)]  # head 5e-4 < h_dry: 0
+    sc = _flat_basin_with_culverts(cvs)
+    T = sc.n_elems
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    m = o.mesh_numpy()
+    o.set_state(np.full(T, 1.0), np.zeros(T), np.zeros(T))
+    phi = o.stage_probe(1, 4)["phi"]
+    expect = np.zeros(T)
+    for (a, b), q in zip(zip(m["cvtrigin"], m["cvtrigout"]), (2.0, 1.0, 3.0, 0.0)):
+        expect[a - 1] -= q
+        expect[b - 1] += q
+    assert np.array_equal(phi[:, 0], expect)
+    # the inlet offsets are the points minus the centroids of their triangles
+    xc, yc = m["tri_xc"][m["cvtrigin"] - 1], m["tri_yc"][m["cvtrigin"] - 1]
+    assert np.array_equal(m["cvrin"].reshape(-1, 2), np.stack([3.3 - xc, np.array([3.6, 10.6, 17.6, 24.6]) - yc], 1))
+
+
+def test_culvert_closed_basin_conserves_mass(oracle_mod):
+    cvs = [dict(inlet=(4.2, 15.1, -0.5), outlet=(25.7, 14.8), head=[0.2, 1.0, 2.0], q=[0.1, 0.8, 2.0])]
+    sc = _flat_basin_with_culverts(cvs)
+    T = sc.n_elems
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    m = o.mesh_numpy()
+    o.set_state(np.full(T, 1.0), np.zeros(T), np.zeros(T))
+    st = o.step(300)
+    s = o.state()
+    assert st["tmass"] == pytest.approx(float(np.sum(m["tri_area"])), rel=1e-12)
+    xc = m["tri_xc"]
+    assert s["h"][xc > 25.0].mean() > s["h"][xc < 5.0].mean()  # water moved through the culvert
+
+
+def test_culvert_input_errors(oracle_mod, storm_lib):
+    from storm_b200 import fvt
+    bad_pt = [dict(inlet=(-5.0, 3.0, 0.0), outlet=(20.0, 3.0), head=[1.0], q=[1.0])]
+    bad_tab = [dict(inlet=(5.0, 3.0, 0.0), outlet=(20.0, 3.0), head=[], q=[])]
+    for cvs, code in ((bad_pt, abi.STORM_ERR_MESH), (bad_tab, abi.STORM_ERR_ARG)):
+        sc = _basin()
+        if cvs is bad_tab:  # an empty performance curve (ncvtable = 0)
+            sc = scenarios.with_culverts(sc, [dict(cvs[0], head=[0.0], q=[0.0])])
+            sc.problem.ncvtable[0] = 0
+        else:
+            sc = scenarios.with_culverts(sc, cvs)
+        with pytest.raises(Exception) as e:
+            oracle_mod.Oracle(sc.problem, sc.options)
+        assert getattr(e.value, "code", code) == code
+        with pytest.raises(fvt.StormError) as e:
+            fvt.build_mesh(sc.problem)
+        assert e.value.code == code
