@@ -398,12 +398,13 @@ def pipeline(train_n=4096, eval_n=64, lo=2000, hi=8000, gen_batch=512, istop=400
 
 
 def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, device=0, seed=7,
-             plain_n=8, reference=True) -> dict:
+             plain_n=8, reference=True, warm_rstops=()) -> dict:
     """Held-out scenarios (seeds disjoint from the training data) run to the stop test:
     cold FP64 and cold mixed (batched), warm mixed (batched, from the network's
     prediction), the plain FP64 solver on each scenario alone (the first `plain_n`),
     and an FP64 continuation to RMS dh < 1e-10 as the steady state the depth errors
-    are measured against."""
+    are measured against.  `warm_rstops` adds warm mixed runs to tighter residuals
+    (time and depth error of each, and how many members end within 1 cm)."""
     import torch
     dev = torch.device(f"cuda:{device}")
     ev = _member_list(eval_n, lo, hi, seed=seed * 100003 + 99_999_989, limiter=limiter)
@@ -458,6 +459,15 @@ def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, dev
                                                     "cold_mixed": float(np.median(dh_cold)),
                                                     "cold_fp64": float(np.median(dh_cold64)),
                                                     "prediction": float(np.median(dh_pred))}}
+    for rs in warm_rstops:
+        w = run_steady_batch(ev, states=warm_states, istop=istop, precision=abi.PREC_MIXED, device=device,
+                             rstop=rs)
+        dw = dmax(w["states"])
+        out[f"warm_mixed_rstop_{rs:g}"] = dict(summ(w), depth_err_vs_steady_median_m=float(np.median(dw)),
+                                                depth_err_vs_steady_max_m=max(dw),
+                                                within_1cm=int(sum(x <= 0.01 for x in dw)))
+    out["within_1cm"] = {"warm_mixed": int(sum(x <= 0.01 for x in dh_warm)),
+                         "cold_fp64": int(sum(x <= 0.01 for x in dh_cold64)), "of": len(ev)}
     plain = []
     for sc in ev[:plain_n]:
         pm = fvt.build_mesh(sc.problem)
@@ -482,6 +492,11 @@ def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, dev
                                     "converged": int(sum(p["converged"] for p in plain))}
         out["speedup_per_scenario_vs_plain_fp64_single_cold"] = w_plain / warm_wall
         out["warm_batched_wall_s_per_scenario_incl_network"] = warm_wall
+        for rs in warm_rstops:
+            r = out[f"warm_mixed_rstop_{rs:g}"]
+            ww = (r["wall_s_batch"] + infer_ms / 1e3 + tm["host_s"] + feat_s) / len(ev)
+            r["wall_s_per_scenario_incl_network"] = ww
+            r["speedup_per_scenario_vs_plain_fp64_single_cold"] = w_plain / ww
     return out
 
 
@@ -502,6 +517,8 @@ def main(argv=None):
     ap.add_argument("--json-out", default=None)
     ap.add_argument("--model", default=None, help="evaluate this trained model (.npz) instead of training")
     ap.add_argument("--plain-n", type=int, default=8)
+    ap.add_argument("--warm-rstop", type=float, nargs="*", default=[],
+                    help="also run the warm start to these residuals (evaluation of --model)")
     a = ap.parse_args(argv)
     from . import build
     build.build()
@@ -509,7 +526,8 @@ def main(argv=None):
         import torch
         torch.cuda.set_device(0)
         net, norm = load_model(a.model)
-        res = {"model": a.model, "eval": evaluate(net, norm, a.eval_n, a.lo, a.hi, a.istop, plain_n=a.plain_n)}
+        res = {"model": a.model, "eval": evaluate(net, norm, a.eval_n, a.lo, a.hi, a.istop, plain_n=a.plain_n,
+                                                  warm_rstops=a.warm_rstop)}
         s = json.dumps(res)
         print(s)
         if a.json_out:
