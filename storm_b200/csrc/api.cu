@@ -492,7 +492,6 @@ int upload(StormFvtHandle* h) {
   for (int b = 0; b < L.nbdr; b++) maxcnt = std::max(maxcnt, L.bdr_cnt[b]);
   h->bc_smem = (size_t)maxcnt * 2 * sizeof(double) + (((size_t)maxcnt + 7) & ~(size_t)7);
   if (h->bc_smem > 48 * 1024) set_bc_smem_limit((int)h->bc_smem);
-  set_stage_smem_limits();
   return 0;
 }
 
@@ -711,14 +710,10 @@ int storm_fvt_step(StormFvtHandle* h, int32_t nsteps, StormFvtStepStats* stats) 
   CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->last_step_ms = ms;
   if (stats) fill_stats(h, h->sc_host[0], stats);
-  for (int sI = 0; sI < h->nscen; sI++) {
+  for (int sI = 0; sI < h->nscen; sI++)
     if (h->sc_host[sI].status & 1)
       return set_error(STORM_ERR_DEVICE, "storm_fvt_step: non-finite depth or velocity in scenario " +
                                              std::to_string(sI));
-    if (h->sc_host[sI].status & 4)
-      return set_error(STORM_ERR_DEVICE, "storm_fvt_step: a shared-memory staging wait ran out in scenario " +
-                                             std::to_string(sI));
-  }
   return STORM_OK;
 }
 

@@ -126,7 +126,6 @@ struct StageLaunch {
 };
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed);
 void set_bc_smem_limit(int bytes);
-void set_stage_smem_limits();  // dynamic shared memory above 48 KiB of the staged kernels
 void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st);
 
 // The output pass (to_vertices, ctr2vtx of cd, error_est(2)) after an iteration.

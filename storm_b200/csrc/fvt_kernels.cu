@@ -25,7 +25,6 @@
 #include <cstdint>
 
 #include "fvt_device.cuh"
-#include "umma.cuh"
 #include "storm_internal.h"
 
 namespace storm {
@@ -428,154 +427,41 @@ __device__ __forceinline__ float limited_r(double q0, double qn, float g_x, floa
   return (fabsf(num) >= fabsf(delq)) ? 1.0f : num / delq;
 }
 
-// ---- bulk staging of a block's per-cell segments into shared memory --------------
-// Cell-major arrays ([T] or [k][T], T a multiple of 256) are read by a block of B
-// cells as contiguous segments; one bulk copy (cp.async.bulk, the TMA engine's
-// untiled form) per segment brings them into shared memory with every byte in
-// flight at once, independent of the registers of the computing threads.
-// Segments start at 16-byte multiples (cell offsets are multiples of B >= 64, the
-// arena aligns every array to 256 bytes) and their sizes are multiples of 16.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   umma::smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(umma::smem_addr(bar))
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::smem_addr(bar)), "r"(bytes)
-               : "memory");
-}
-constexpr int32_t kStatusStageTimeout = 4;  // Scalars::status bit: a staging wait ran out
-
-// Issues the copies of one block from warp 0: every lane walks the same sequence of
-// segments and issues those with its index modulo 32; lane 0 then arms the barrier
-// with the byte total (the transaction count may run below zero until it does).
-struct Stager {
-  uint64_t* bar;
-  int lane;
-  int idx = 0;
-  uint32_t total = 0;
-  __device__ __forceinline__ Stager(uint64_t* b, int l) : bar(b), lane(l) {}
-  __device__ __forceinline__ void add(void* dst, const void* src, uint32_t bytes) {
-    if ((idx & 31) == lane) bulk_g2s(dst, src, bytes, bar);
-    idx++;
-    total += bytes;
-  }
-  __device__ __forceinline__ void finish() {
-    __syncwarp();
-    if (lane == 0) mbar_expect_tx(bar, total);
-  }
-};
-
-__device__ __forceinline__ void stage_init(uint64_t* bar) {
-  if (threadIdx.x == 0) {
-    umma::mbar_init(bar, 1);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  }
-  __syncthreads();
-}
-
-// Bounded wait of all threads for the block's copies.  Returns false when the wait ran
-// out: the status bit is set and the block waits once more for its copies before the
-// caller returns.
-__device__ __forceinline__ bool stage_wait(uint64_t* bar, int32_t* status) {
-  if (umma::mbar_wait(bar, 0)) return true;
-  if (threadIdx.x == 0) atomicOr(status, kStatusStageTimeout);
-  umma::mbar_wait(bar, 0);
-  return false;
-}
-
-// Shared memory of k_grad per cell: 5 doubles, 21 R, 9 int32, 2 bytes.
 template <class R>
-constexpr size_t grad_smem_per_cell() {
-  return 5 * sizeof(double) + 21 * sizeof(R) + 9 * sizeof(int32_t) + 2;
-}
-
-template <class R, int B>
-__global__ void __launch_bounds__(B, (B == 256 ? 3 : (B == 128 ? 7 : 14)))
-    k_grad(Dev d, Geo<R> G, const double* __restrict__ hs, const uint8_t* __restrict__ dry,
-           double* __restrict__ rku_prev, double* __restrict__ rkv_prev) {
-  extern __shared__ __align__(128) unsigned char g_smem[];
-  __shared__ uint64_t bar;
-  const int T = d.T;
-  const int c0 = blockIdx.x * B, t = threadIdx.x, c = c0 + t;
-  // scenarios start on multiples of 256 cells, so a block is all in one scenario or
-  // (its tail) padding; a padding or converged block issues no copies
-  const int sid0 = d.cell_sid[c0];
-  if (sid0 < 0 || d.sc[sid0].converged) return;
-  double* s_hs = reinterpret_cast<double*>(g_smem);
-  double *s_z = s_hs + B, *s_ua = s_z + B, *s_va = s_ua + B, *s_zmax = s_va + B;
-  R* s_r = reinterpret_cast<R*>(s_zmax + B);
-  R *s_stw = s_r, *s_stdx = s_r + 3 * B, *s_stdy = s_r + 6 * B, *s_la = s_r + 9 * B, *s_lb = s_r + 10 * B;
-  R *s_lc = s_r + 11 * B, *s_ldet = s_r + 12 * B, *s_rcx = s_r + 13 * B, *s_rcy = s_r + 16 * B;
-  R *s_dzx = s_r + 19 * B, *s_dzy = s_r + 20 * B;
-  int32_t* s_i = reinterpret_cast<int32_t*>(s_r + 21 * B);
-  int32_t *s_stid = s_i, *s_t3 = s_i + 3 * B, *s_vt = s_i + 6 * B;
-  uint8_t* s_dry = reinterpret_cast<uint8_t*>(s_i + 9 * B);
-  uint8_t* s_nst = s_dry + B;
-  stage_init(&bar);
-  if (t < 32) {
-    Stager L(&bar, t);
-    constexpr uint32_t b8 = B * 8, bR = B * sizeof(R), b4 = B * 4;
-    L.add(s_hs, hs + c0, b8);
-    L.add(s_z, d.z + c0, b8);
-    L.add(s_ua, d.u_a + c0, b8);
-    L.add(s_va, d.v_a + c0, b8);
-    L.add(s_zmax, d.zmax + c0, b8);
-    L.add(s_dzx, G.delz_x + c0, bR);
-    L.add(s_dzy, G.delz_y + c0, bR);
-    L.add(s_dry, dry + c0, B);
-    L.add(s_nst, d.nst + c0, B);
-    for (int j = 0; j < 3; j++) {
-      L.add(s_t3 + j * B, d.t2t3 + (size_t)j * T + c0, b4);
-      L.add(s_vt + j * B, d.vert + (size_t)j * T + c0, b4);
-    }
-    if (d.lim == 1 || d.lim == 2) {
-      for (int k = 0; k < 3 && k < d.kst; k++) {
-        const size_t q = (size_t)k * T + c0;
-        L.add(s_stid + k * B, d.st_id + q, b4);
-        L.add(s_stw + k * B, G.st_w + q, bR);
-        L.add(s_stdx + k * B, G.st_dx + q, bR);
-        L.add(s_stdy + k * B, G.st_dy + q, bR);
-      }
-      L.add(s_la, G.lsq_a + c0, bR);
-      L.add(s_lb, G.lsq_b + c0, bR);
-      L.add(s_lc, G.lsq_c + c0, bR);
-      L.add(s_ldet, G.lsq_det + c0, bR);
-    }
-    if (d.lim == 2)
-      for (int j = 0; j < 3; j++) {
-        L.add(s_rcx + j * B, G.rc_x + (size_t)j * T + c0, bR);
-        L.add(s_rcy + j * B, G.rc_y + (size_t)j * T + c0, bR);
-      }
-    L.finish();
-  }
-  if (!stage_wait(&bar, &d.sc[sid0].status)) return;
+__global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, double* __restrict__ rku_prev,
+                                              double* __restrict__ rkv_prev) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.T) return;
   const int sid = d.cell_sid[c];
-  if (sid < 0) return;
-  const double zeta_c = s_hs[t] + s_z[t];
-  const double u_c = s_ua[t], v_c = s_va[t];
+  if (sid < 0 || d.sc[sid].converged) return;
+  const int T = d.T;
+  const double zeta_c = hs[c] + d.z[c];
+  const double u_c = d.u_a[c], v_c = d.v_a[c];
+  // face neighbours and vertices first: their loads (and the flags read through them
+  // below) are in flight while the stencil is gathered
   int t3[3], vt[3];
 #pragma unroll
   for (int j = 0; j < 3; j++) {
-    t3[j] = s_t3[j * B + t];
-    vt[j] = s_vt[j * B + t];
+    t3[j] = d.t2t3[(size_t)j * T + c];
+    vt[j] = d.vert[(size_t)j * T + c];
   }
-  const bool dry_c = s_dry[t];
+  const bool dry_c = dry[c];
   R hx = R(0), hy = R(0), ux = R(0), uy = R(0), vx = R(0), vy = R(0);
   if (d.lim == 1 || d.lim == 2) {
     R dz = R(0), ez = R(0), du = R(0), eu = R(0), dv = R(0), ev = R(0);
-    const int n = s_nst[t];
+    const int n = d.nst[c];
     int k0 = 0;
     if (n >= 3) {  // interior cells: the three face neighbours, all gathers issued together
       int jj[3];
       R w[3], dx[3], dy[3], pz[3], pu[3], pv[3];
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        jj[k] = s_stid[k * B + t];
-        w[k] = s_stw[k * B + t];
-        dx[k] = s_stdx[k * B + t];
-        dy[k] = s_stdy[k * B + t];
+        const size_t q = (size_t)k * T + c;
+        jj[k] = d.st_id[q];
+        w[k] = G.st_w[q];
+        dx[k] = G.st_dx[q];
+        dy[k] = G.st_dy[q];
       }
 #pragma unroll
       for (int k = 0; k < 3; k++) {
@@ -596,11 +482,8 @@ __global__ void __launch_bounds__(B, (B == 256 ? 3 : (B == 128 ? 7 : 14)))
     }
     for (int k = k0; k < n; k++) {
       const size_t q = (size_t)k * T + c;
-      const bool st = k < 3;
-      const int j = st ? s_stid[k * B + t] : d.st_id[q];
-      const R w = st ? s_stw[k * B + t] : G.st_w[q];
-      const R dx = st ? s_stdx[k * B + t] : G.st_dx[q];
-      const R dy = st ? s_stdy[k * B + t] : G.st_dy[q];
+      const int j = d.st_id[q];
+      const R w = G.st_w[q], dx = G.st_dx[q], dy = G.st_dy[q];
       const R pz = (R)((hs[j] + d.z[j]) - zeta_c);
       const R pu = (R)(d.u_a[j] - u_c);
       const R pv = (R)(d.v_a[j] - v_c);
@@ -611,7 +494,7 @@ __global__ void __launch_bounds__(B, (B == 256 ? 3 : (B == 128 ? 7 : 14)))
       dv = dv + w * pv * dx;
       ev = ev + w * pv * dy;
     }
-    const R ai = s_la[t], bi = s_lb[t], ci = s_lc[t], det = s_ldet[t];
+    const R ai = G.lsq_a[c], bi = G.lsq_b[c], ci = G.lsq_c[c], det = G.lsq_det[c];
     hx = (ci * dz - bi * ez) / det;
     hy = (ai * ez - dz * bi) / det;
     ux = (ci * du - bi * eu) / det;
@@ -623,8 +506,9 @@ __global__ void __launch_bounds__(B, (B == 256 ? 3 : (B == 128 ? 7 : 14)))
     R rz[3], ru[3], rv[3];
 #pragma unroll
     for (int j = 0; j < 3; j++) {
+      const size_t q = (size_t)j * T + c;
       const int k = t3[j];
-      const R rx = s_rcx[j * B + t], ry = s_rcy[j * B + t];
+      const R rx = G.rc_x[q], ry = G.rc_y[q];
       const double qz = k < 0 ? zeta_c : hs[k] + d.z[k];
       const double qu = k < 0 ? u_c : d.u_a[k];
       const double qv = k < 0 ? v_c : d.v_a[k];
@@ -639,12 +523,12 @@ __global__ void __launch_bounds__(B, (B == 256 ? 3 : (B == 128 ? 7 : 14)))
     ux = pu * ux; uy = pu * uy;
     vx = pv * vx; vy = pv * vy;
   }
-  hx = hx - s_dzx[t];
-  hy = hy - s_dzy[t];
+  hx = hx - G.delz_x[c];
+  hy = hy - G.delz_y[c];
   double ub = u_c, vb = v_c;
   if (!dry_c) {
     // hgradfix2.f90:48-98
-    bool setgrad = zeta_c < s_zmax[t];
+    bool setgrad = zeta_c < d.zmax[c];
 #pragma unroll
     for (int j = 0; j < 3; j++) {
       const int l = t3[j];
@@ -652,8 +536,8 @@ __global__ void __launch_bounds__(B, (B == 256 ? 3 : (B == 128 ? 7 : 14)))
       if (dry[l] && d.z[l] < zeta_c) setgrad = false;
     }
     if (setgrad) {
-      hx = -s_dzx[t];
-      hy = -s_dzy[t];
+      hx = -G.delz_x[c];
+      hy = -G.delz_y[c];
       ub = kZero;
       vb = kZero;
       rku_prev[c] = kZero;
@@ -1807,14 +1691,9 @@ __global__ void k_culvert(Dev d, Geo<R> G, const double* __restrict__ hs, const 
 template <class R>
 static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) {
   switch (L.which) {
-    case STAGE_GRAD: {
-      const int B = L.block.x;
-      const size_t smem = grad_smem_per_cell<R>() * B;
-      if (B == 64) k_grad<R, 64><<<L.grid, L.block, smem, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev);
-      else if (B == 128) k_grad<R, 128><<<L.grid, L.block, smem, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev);
-      else k_grad<R, 256><<<L.grid, L.block, smem, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev);
+    case STAGE_GRAD:
+      k_grad<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev);
       break;
-    }
     case STAGE_BC:
       k_bc<R><<<L.grid, L.block, L.smem, L.stream>>>(d, G, L.hs, L.dry);
       break;
@@ -1849,13 +1728,6 @@ void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, con
 
 void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st) {
   if (cnt > 0) k_rsavg<<<(cnt + 255) / 256, 256, 0, st>>>(d, off, cnt);
-}
-
-void set_stage_smem_limits() {
-  cudaFuncSetAttribute(k_grad<double, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(grad_smem_per_cell<double>() * 256));
-  cudaFuncSetAttribute(k_grad<float, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(grad_smem_per_cell<float>() * 256));
 }
 
 void set_bc_smem_limit(int bytes) {
