@@ -44,6 +44,43 @@ constexpr double kVlarge = 1.7976931348623157e+308; // HUGE(zero)
 __device__ __forceinline__ double fmin2(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double fmax2(double a, double b) { return (b > a) ? b : a; }
 
+// The IEEE quotient a / b, with a zero numerator answered without the division: for
+// a nonzero b that is not a NaN, a signed zero divided by b is the zero whose sign is
+// the exclusive or of the two signs, which is exactly what the division returns.  A
+// zero quotient is rare in general code but common here (dry cells, still water, a
+// limiter ratio whose numerator is the cell's own extremum, axis-aligned normals),
+// and the division's own handling of that case costs far more than this test.
+__device__ __forceinline__ double qdiv(double a, double b) {
+  double r;
+  if (a == 0.0 && b != 0.0 && b == b)
+    r = __longlong_as_double((__double_as_longlong(a) ^ __double_as_longlong(b)) &
+                             (long long)0x8000000000000000ULL);
+  else
+    r = a / b;
+  return r;
+}
+__device__ __forceinline__ float qdiv(float a, float b) {
+  float r;
+  if (a == 0.0f && b != 0.0f && b == b)
+    r = __int_as_float((__float_as_int(a) ^ __float_as_int(b)) & (int)0x80000000u);
+  else
+    r = a / b;
+  return r;
+}
+
+// sqrt with a zero argument answered directly (sqrt(+-0) = +-0 under IEEE), for the
+// same reason as qdiv: still water and dry sides make zero arguments common.
+__device__ __forceinline__ double qsqrt(double x) {
+  double r = x;
+  if (x != 0.0) r = sqrt(x);
+  return r;
+}
+__device__ __forceinline__ float qsqrt(float x) {
+  float r = x;
+  if (x != 0.0f) r = sqrtf(x);
+  return r;
+}
+
 // equals.f90:1-27
 __device__ __forceinline__ bool equals(double a, double b) {
   double eps = fabs(a) * kFmachp;
@@ -56,7 +93,7 @@ __device__ __forceinline__ bool dry_flag(double h, double u, double v, double h_
                                          double* umag) {
   bool dry = h < h_dry;
   double um = kZero;
-  if (!dry) um = sqrt(u * u + v * v);
+  if (!dry) um = qsqrt(u * u + v * v);
   *umag = um;
   if (!dry && (h < h_wet) && equals(um, kZero)) dry = true;
   return dry;
@@ -96,8 +133,8 @@ __device__ __forceinline__ void flux_roe(R nx, R ny, R hleft, R uleft, R vleft, 
   hright = fmax2(hright, R(SMALL_F));
   R hrs = sqrt(hright);
   R denom = hrs + hls;
-  R uavg = (uright * hrs + uleft * hls) / denom;
-  R vavg = (vright * hrs + vleft * hls) / denom;
+  R uavg = qdiv(uright * hrs + uleft * hls, denom);
+  R vavg = qdiv(vright * hrs + vleft * hls, denom);
   R cavg = sqrt(R(kHalf) * R(kG) * (hleft + hright));
   R q[3];
   q[0] = hright - hleft;
@@ -110,12 +147,12 @@ __device__ __forceinline__ void flux_roe(R nx, R ny, R hleft, R uleft, R vleft, 
   lev[0][0] = -(uavg * ny - vavg * nx);
   lev[0][1] = ny;
   lev[0][2] = -nx;
-  lev[1][0] = R(kHalf) * (uavg * nx + vavg * ny) / cavg + R(kHalf);
-  lev[1][1] = -(R(kHalf) * nx / cavg);
-  lev[1][2] = -(R(kHalf) * ny / cavg);
-  lev[2][0] = -(R(kHalf) * (uavg * nx + vavg * ny) / cavg) + R(kHalf);
-  lev[2][1] = R(kHalf) * nx / cavg;
-  lev[2][2] = R(kHalf) * ny / cavg;
+  lev[1][0] = qdiv(R(kHalf) * (uavg * nx + vavg * ny), cavg) + R(kHalf);
+  lev[1][1] = -qdiv(R(kHalf) * nx, cavg);
+  lev[1][2] = -qdiv(R(kHalf) * ny, cavg);
+  lev[2][0] = -qdiv(R(kHalf) * (uavg * nx + vavg * ny), cavg) + R(kHalf);
+  lev[2][1] = qdiv(R(kHalf) * nx, cavg);
+  lev[2][2] = qdiv(R(kHalf) * ny, cavg);
   eig[0] = fmax2(fabs(uavg * nx + vavg * ny), delta);
   eig[1] = fmax2(fabs(uavg * nx + vavg * ny - cavg), delta);
   eig[2] = fmax2(fabs(uavg * nx + vavg * ny + cavg), delta);
@@ -141,8 +178,8 @@ __device__ __forceinline__ void flux_roe(R nx, R ny, R hleft, R uleft, R vleft, 
 template <class R>
 __device__ __forceinline__ void flux_hll(R nx, R ny, R hleft, R uleft, R vleft, R hright, R uright, R vright,
                                          R h0, R* flux, bool* bad) {
-  R cleft = sqrt(R(kG) * hleft);
-  R cright = sqrt(R(kG) * hright);
+  R cleft = qsqrt(R(kG) * hleft);
+  R cright = qsqrt(R(kG) * hright);
   R ustar = R(kHalf) * ((uleft + uright) * nx + (vleft + vright) * ny) + cleft - cright;
   R cstar = R(kHalf) * (cleft + cright) + ((uleft - uright) * nx + (vleft - vright) * ny) / R(4.0);
   R sleft, sright, aux1, aux2;
@@ -180,11 +217,11 @@ __device__ __forceinline__ void flux_hll(R nx, R ny, R hleft, R uleft, R vleft, 
     for (int i = 0; i < 3; i++) flux[i] = fr[i] + gr[i];
   } else {
     aux1 = sright - sleft;
-    flux[0] = (sright * (fl[0] + gl[0]) - sleft * (fr[0] + gr[0]) + sleft * sright * (hright - hleft)) / aux1;
-    flux[1] = (sright * (fl[1] + gl[1]) - sleft * (fr[1] + gr[1]) +
-               sleft * sright * (hright * uright - hleft * uleft)) / aux1;
-    flux[2] = (sright * (fl[2] + gl[2]) - sleft * (fr[2] + gr[2]) +
-               sleft * sright * (hright * vright - hleft * vleft)) / aux1;
+    flux[0] = qdiv(sright * (fl[0] + gl[0]) - sleft * (fr[0] + gr[0]) + sleft * sright * (hright - hleft), aux1);
+    flux[1] = qdiv(sright * (fl[1] + gl[1]) - sleft * (fr[1] + gr[1]) +
+                       sleft * sright * (hright * uright - hleft * uleft), aux1);
+    flux[2] = qdiv(sright * (fl[2] + gl[2]) - sleft * (fr[2] + gr[2]) +
+                       sleft * sright * (hright * vright - hleft * vleft), aux1);
   }
 }
 
@@ -413,7 +450,7 @@ __device__ __forceinline__ double limited_r(double q0, double qn, double g_x, do
     // When |num| > |delq| the exact quotient exceeds one, so the rounded one is
     // >= 1 and the limiter's min(r,1) is 1: the division is skipped, same bits.
     const double num = (delq < 0) ? (qmin - q0) : (qmax - q0);
-    rj = (fabs(num) > fabs(delq)) ? kOne : num / delq;
+    rj = (fabs(num) > fabs(delq)) ? kOne : qdiv(num, delq);
   }
   const double a = fmin2(kOne * rj, kOne);
   const double b = fmin2(rj, kOne);
@@ -424,7 +461,7 @@ __device__ __forceinline__ float limited_r(double q0, double qn, float g_x, floa
   const float delq = g_x * rx + g_y * ry;
   if (fabsf(delq) <= 1e-30f) return 1.0f;
   const float num = (delq < 0) ? dmin : dmax;
-  return (fabsf(num) >= fabsf(delq)) ? 1.0f : num / delq;
+  return (fabsf(num) >= fabsf(delq)) ? 1.0f : qdiv(num, delq);
 }
 
 template <class R>
@@ -495,12 +532,12 @@ __global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* 
       ev = ev + w * pv * dy;
     }
     const R ai = G.lsq_a[c], bi = G.lsq_b[c], ci = G.lsq_c[c], det = G.lsq_det[c];
-    hx = (ci * dz - bi * ez) / det;
-    hy = (ai * ez - dz * bi) / det;
-    ux = (ci * du - bi * eu) / det;
-    uy = (ai * eu - du * bi) / det;
-    vx = (ci * dv - bi * ev) / det;
-    vy = (ai * ev - dv * bi) / det;
+    hx = qdiv(ci * dz - bi * ez, det);
+    hy = qdiv(ai * ez - dz * bi, det);
+    ux = qdiv(ci * du - bi * eu, det);
+    uy = qdiv(ai * eu - du * bi, det);
+    vx = qdiv(ci * dv - bi * ev, det);
+    vy = qdiv(ai * ev - dv * bi, det);
   }
   if (d.lim == 2) {  // limiterBJ.f90:42-81, beta = one
     R rz[3], ru[3], rv[3];
@@ -1057,7 +1094,7 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
       if (d.btype == 0) {  // wenslp3_fluxes.f90:34-67
         const int w = fre[t];
         const double h1 = d.hvtx[d.wall_p1[w]], h2 = d.hvtx[d.wall_p2[w]];
-        double hedge = sqrt((h1 * h1 + h1 * h2 + h2 * h2) * kOneThird);
+        double hedge = qsqrt((h1 * h1 + h1 * h2 + h2 * h2) * kOneThird);
         if (hedge < kZero) hedge = kZero;
         if (hedge < d.h_dry) continue;
         p2 = p2 - kHalf * kG * hedge * hedge * nx * len;
@@ -1121,7 +1158,7 @@ __device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c
   const double u_c = d.u_a[c], v_c = d.v_a[c];
   double delt;
   if (d.steady) {
-    const double um = (h_c < d.h_dry) ? kZero : sqrt(u_c * u_c + v_c * v_c);
+    const double um = (h_c < d.h_dry) ? kZero : qsqrt(u_c * u_c + v_c * v_c);
     const double wc = dry_c ? kZero : sqrt(kG * h_c);
     delt = um + wc;
     if (delt < SMALL_F) delt = 1.044;
@@ -1156,8 +1193,8 @@ __device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c
   double un, vn;
   const double h_delta = dry_c ? d.h_wet : d.h_dry;
   if (rh > h_delta) {
-    un = ru / rh;
-    vn = rv / rh;
+    un = qdiv(ru, rh);
+    vn = qdiv(rv, rh);
   } else {
     ru = kZero; rv = kZero; un = kZero; vn = kZero;
   }
@@ -1296,7 +1333,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
         break;
       case 3:
         if (!dry2) {
-          double re = um * h / d.visc;
+          double re = qdiv(um * h, d.visc);
           re = fmax2(re, 1000.0);
           re = fmin2(re, (double)2.5e7f);
           rough = cd;
