@@ -349,6 +349,27 @@ STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, i
 STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t* chosen);
 
 /*
+ * Partitions of one mesh (SURVEY-style domain decomposition, single-device form):
+ * the scenarios of a batch handle are the parts of one mesh, each extended by two
+ * rings of vertex-adjacent halo cells taken from its neighbours.  After this call:
+ *  - after every RK stage but the last, and after the friction step, each halo cell
+ *    (scenario dst_scen[i], 1-based element dst_elem[i]) takes the state of its owner
+ *    (src_scen[i], src_elem[i]): depth, discharges and velocities of that level and
+ *    the dry flags the next stage reads;
+ *  - halo cells are left out of the mass, residual and CFL reductions, and the
+ *    scenarios share one dt (the minimum over all of them), one stop test (on the
+ *    combined residual) and, steady, the friction dt of the local dt of element
+ *    n_elems of the whole mesh, taken from scenario fric_scen.
+ * With two halo rings every owned cell's update reads exactly the values it reads in
+ * the undivided mesh, so the parts evolve bit for bit as the whole (the combined mass
+ * and residual sums round in another order).  Requires nscen >= 2, no residual
+ * smoothing, no culverts; the graph is re-captured.  Calling it twice is an error.
+ */
+STORM_FVT_API int storm_fvt_link_partitions(StormFvtHandle* hd, int32_t n_halo, const int32_t* dst_scen,
+                                            const int32_t* dst_elem, const int32_t* src_scen,
+                                            const int32_t* src_elem, int32_t fric_scen);
+
+/*
  * Boundary data of the output-time vertex pass (Fortran module arrays the host holds
  * after read_data: walls.f90:170-195 and ibc_arrays.f90:56-135, 181-252, 266-345).
  * Vectors (TYPE(vector) arrays) are x,y interleaved, 2-D arrays column-major.

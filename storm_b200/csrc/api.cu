@@ -74,6 +74,7 @@ struct StormFvtHandle {
   // output pass (storm_fvt_output_vertices): device buffers, allocated at first use
   void* out_buf = nullptr;
   size_t out_bytes = 0;
+  void* halo_buf = nullptr;  // linked partitions: halo slots, owner slots, halo mask
 };
 
 namespace {
@@ -166,6 +167,8 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     L.rkv_prev = d.rkv + (size_t)(s - 1) * T;
     launch_stage(L, d, h->gd, h->gf, h->mixed);
   };
+  const bool linked = d.linked != 0;
+  if (linked && !d.steady && d.dt_op != 0) launch_link_dt(d, h->stream);
   for (int s = 1; s <= K; s++) {
     const double* hs = d.rkh + (size_t)(s - 1) * T;
     uint8_t* dry = (s & 1) ? d.dry_a : d.dry_b;
@@ -215,12 +218,18 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
       launch(STAGE_UPDATE, (T + 127) / 128, 128, 0, h->stream, s, hs, dry, dry_next);
       if (done()) return STORM_ERR_CUDA;
     }
+    // halo cells of linked partitions take their owners' new level and flags
+    if (d.nhalo > 0 && s < K) launch_halo(d, s, dry_next, nullptr, h->stream);
   }
+  if (linked && d.steady) launch_link_fric(d, h->stream);
   if (mark(KT_FRIC)) return STORM_ERR_CUDA;
   k_fric<<<d.nblk_red, kRed, 0, h->stream>>>(d);
-  if (done() || mark(KT_FINAL)) return STORM_ERR_CUDA;
+  if (done()) return STORM_ERR_CUDA;
+  if (d.nhalo > 0) launch_halo(d, 0, d.dry_a, d.dry_out, h->stream);
+  if (mark(KT_FINAL)) return STORM_ERR_CUDA;
   k_final<<<d.nscen, kRed, 0, h->stream>>>(d);
   if (done()) return STORM_ERR_CUDA;
+  if (linked) launch_link(d, h->stream);
   CK(cudaGetLastError());
   return 0;
 }
@@ -262,6 +271,7 @@ void release(StormFvtHandle* h) {
   if (h->arena32) cudaFree(h->arena32);
   if (h->sc_host) cudaFreeHost(h->sc_host);
   if (h->out_buf) cudaFree(h->out_buf);
+  if (h->halo_buf) cudaFree(h->halo_buf);
   delete h;
 }
 
@@ -998,6 +1008,64 @@ int storm_fvt_autotune(StormFvtHandle* h, int32_t iters, int32_t* chosen) {
     chosen[3] = h->bs_flux;
   }
   // re-capture the iteration graph with the chosen shapes
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->exec = nullptr;
+  h->graph = nullptr;
+  return capture_graph(h);
+}
+
+int storm_fvt_link_partitions(StormFvtHandle* h, int32_t n_halo, const int32_t* dst_scen, const int32_t* dst_elem,
+                              const int32_t* src_scen, const int32_t* src_elem, int32_t fric_scen) {
+  clear_error();
+  if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: null handle");
+  if (h->nscen < 2) return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: needs a batch of at least 2 parts");
+  if (h->d.linked) return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: already linked");
+  if (h->opt.rsavg_passes > 0)
+    return set_error(STORM_ERR_UNSUPPORTED, "storm_fvt_link_partitions: residual smoothing is not supported");
+  if (h->L.ncv > 0) return set_error(STORM_ERR_UNSUPPORTED, "storm_fvt_link_partitions: culverts are not supported");
+  if (n_halo < 0 || (n_halo > 0 && (!dst_scen || !dst_elem || !src_scen || !src_elem)))
+    return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: bad halo arrays");
+  if (fric_scen < 0 || fric_scen >= h->nscen) return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: fric_scen out of range");
+  const int T = h->L.T;
+  auto slot = [&](int32_t s, int32_t e, int32_t* out) -> bool {
+    if (s < 0 || s >= h->nscen) return false;
+    const HostLayout& P = h->parts[s];
+    if (e < 1 || e > P.T) return false;
+    *out = h->info[s].cell_off + P.cell_new[e - 1];
+    return true;
+  };
+  std::vector<int32_t> dst(n_halo), src(n_halo);
+  std::vector<uint8_t> mask(T, 0);
+  for (int32_t i = 0; i < n_halo; i++) {
+    if (!slot(dst_scen[i], dst_elem[i], &dst[i]) || !slot(src_scen[i], src_elem[i], &src[i]))
+      return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: halo entry " + std::to_string(i) + " out of range");
+    if (dst_scen[i] == src_scen[i]) return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: a halo cell's owner is in its own part");
+    if (mask[dst[i]]) return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: halo cell listed twice");
+    mask[dst[i]] = 1;
+  }
+  for (int32_t i = 0; i < n_halo; i++)
+    if (mask[src[i]]) return set_error(STORM_ERR_ARG, "storm_fvt_link_partitions: an owner is itself a halo cell");
+  CK(cudaSetDevice(h->device));
+  const size_t nh = std::max<int32_t>(n_halo, 1);
+  const size_t o_dst = 0, o_src = (nh * 4 + 255) & ~(size_t)255, o_mask = o_src + ((nh * 4 + 255) & ~(size_t)255);
+  const size_t bytes = o_mask + (size_t)T;
+  void* buf = nullptr;
+  cudaError_t e = cudaMalloc(&buf, bytes);
+  if (e != cudaSuccess) return set_error(STORM_ERR_NOMEM, std::string("storm_fvt_link_partitions: ") + cudaGetErrorString(e));
+  h->halo_buf = buf;
+  char* b = static_cast<char*>(buf);
+  if (n_halo > 0) {
+    CK(cudaMemcpy(b + o_dst, dst.data(), 4 * (size_t)n_halo, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b + o_src, src.data(), 4 * (size_t)n_halo, cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(b + o_mask, mask.data(), (size_t)T, cudaMemcpyHostToDevice));
+  h->d.nhalo = n_halo;
+  h->d.halo_dst = reinterpret_cast<const int32_t*>(b + o_dst);
+  h->d.halo_src = reinterpret_cast<const int32_t*>(b + o_src);
+  h->d.halo_mask = reinterpret_cast<const uint8_t*>(b + o_mask);
+  h->d.linked = 1;
+  h->d.fric_scen = fric_scen;
   if (h->exec) cudaGraphExecDestroy(h->exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   h->exec = nullptr;

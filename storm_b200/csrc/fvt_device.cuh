@@ -30,6 +30,7 @@ struct Scalars {
   double cqin3[kMaxBdrDev], cqout3[kMaxBdrDev];
   double qin_it[kMaxBdrDev], hbc_it[kMaxBdrDev];  // values the last iteration ran with
   double bch_max;               // dataprepFVT.f90:278-286
+  double sumtop, sumbot, rmax_phi;  // this iteration's residual sums (linked partitions)
   // static: boundary series and the scenario's ranges in the merged arrays
   int32_t n_in, n_out;
   int32_t last_cell;            // merged id of element n_elems (steady friction dt)
@@ -51,6 +52,11 @@ struct Dev {
   // cells
   const double *area, *perim, *xc, *yc, *z, *delz_x, *delz_y, *zmax, *cd;
   const double *wcoef1, *wcoef2;  // wind stress terms per cell (null: no wind)
+  // linked partitions of one mesh: halo cell slots and their owners' slots, the halo
+  // mask (null: no halo), the scenario holding element n_elems of the whole mesh
+  int32_t nhalo, linked, fric_scen;
+  const int32_t *halo_dst, *halo_src;
+  const uint8_t* halo_mask;
   // culverts: inlet cell, table rows, inlet offset from the centroid, invert elevation,
   // performance curves [ncv][cv_ld]; per-cell term list (cvc_*); discharges cvsrc
   int32_t ncv, cv_ld, ncvc;
@@ -126,6 +132,12 @@ struct StageLaunch {
 };
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed);
 void set_bc_smem_limit(int bytes);
+// Linked partitions: halo exchange of one level (+ up to two flag arrays), the shared
+// friction dt before k_fric, the shared dt / stop test after k_final.
+void launch_halo(const Dev& d, int level, uint8_t* f1, uint8_t* f2, cudaStream_t st);
+void launch_link_fric(const Dev& d, cudaStream_t st);
+void launch_link(const Dev& d, cudaStream_t st);
+void launch_link_dt(const Dev& d, cudaStream_t st);
 void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st);
 
 // The output pass (to_vertices, ctr2vtx of cd, error_est(2)) after an iteration.

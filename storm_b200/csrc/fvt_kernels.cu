@@ -1387,7 +1387,11 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
     rm = dry2 ? kZero : d.phimax[c];
     const double wc1 = dry1 ? kZero : sqrt(kG * h);
     dtc = d.cfl * d.area[c] / ((um1 + wc1 + SMALL_F) * d.perim[c]);
-    if (!isfinite(h) || !isfinite(u) || !isfinite(v)) atomicOr(&d.sc[sid].status, 1);
+    if (d.halo_mask && d.halo_mask[c]) {  // a halo copy: its owner counts it
+      st = kZero; sb = kZero; tm = kZero; rm = kZero; dtc = kVlarge;
+    } else if (!isfinite(h) || !isfinite(u) || !isfinite(v)) {
+      atomicOr(&d.sc[sid].status, 1);
+    }
   }
   double* pb = d.part + 8 * blockIdx.x;
   double r0 = block_sum<kRedThreads>(st, sm);
@@ -1422,6 +1426,9 @@ __global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
   const double rmax_phi = block_max<kRedThreads>(a3, sm);
   const double dtmin = block_min<kRedThreads>(a4, sm);
   if (threadIdx.x == 0) {
+    sc->sumtop = sumtop;
+    sc->sumbot = sumbot;
+    sc->rmax_phi = rmax_phi;
     sc->iter = sc->iter + 1;
     sc->ttime = sc->ttime + sc->delt;
     double sbot = sumbot;
@@ -1722,6 +1729,77 @@ __global__ void k_culvert(Dev d, Geo<R> G, const double* __restrict__ hs, const 
   }
   d.cvsrc[i] = src;
 }
+
+// ---------------------------------------------------------------------------
+// Linked partitions of one mesh (storm_fvt_link_partitions).  The scenarios share
+// one clock, so the first one's stop flag stands for all.
+
+// Every halo cell takes its owner's values of one RK level, the velocities and up to
+// two flag arrays.
+__global__ void __launch_bounds__(256) k_halo(Dev d, int level, uint8_t* f1, uint8_t* f2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.nhalo || d.sc[0].converged) return;
+  const int dst = d.halo_dst[i], src = d.halo_src[i];
+  const size_t off = (size_t)level * d.T;
+  d.rkh[off + dst] = d.rkh[off + src];
+  d.rku[off + dst] = d.rku[off + src];
+  d.rkv[off + dst] = d.rkv[off + src];
+  d.u_a[dst] = d.u_a[src];
+  d.v_a[dst] = d.v_a[src];
+  if (f1) f1[dst] = f1[src];
+  if (f2) f2[dst] = f2[src];
+}
+
+// Unsteady runs: the first dt after a state is set comes from each part's own CFL
+// minimum; every iteration starts from the smallest (later ones are already equal).
+__global__ void k_link_dt(Dev d) {
+  if (threadIdx.x != 0 || d.sc[0].converged) return;
+  double dmin = kVlarge;
+  for (int s = 0; s < d.nscen; s++) dmin = fmin2(dmin, d.sc[s].delt);
+  for (int s = 0; s < d.nscen; s++) d.sc[s].delt = dmin;
+}
+
+// Steady runs: the friction step of every part uses the local dt of element n_elems
+// of the whole mesh (solverFVT.f90:155 and :335-356), set in the part that owns it.
+__global__ void k_link_fric(Dev d) {
+  if (threadIdx.x != 0 || d.sc[0].converged) return;
+  const double v = d.sc[d.fric_scen].delt_fric;
+  for (int s = 0; s < d.nscen; s++) d.sc[s].delt_fric = v;
+}
+
+// After k_final: the residual, mass and dt of the whole mesh from the parts' sums
+// (added in scenario order), and one stop test for all parts.
+__global__ void k_link(Dev d) {
+  if (threadIdx.x != 0 || d.sc[0].converged) return;
+  double top = kZero, bot = kZero, tm = kZero, rmx = kZero, dmin = kVlarge;
+  for (int s = 0; s < d.nscen; s++) {
+    top = top + d.sc[s].sumtop;
+    bot = bot + d.sc[s].sumbot;
+    tm = tm + d.sc[s].tmass;
+    rmx = fmax2(rmx, d.sc[s].rmax_phi);
+    dmin = fmin2(dmin, d.sc[s].delt);
+  }
+  double sbot = bot;
+  if (equals(sbot, kZero)) sbot = kOne;
+  const double rms = sqrt(top / sbot);
+  const double rmax = (d.steady && d.stop_cr != 0) ? rms : rmx;
+  const int conv = d.steady && rmax < d.rstop;
+  for (int s = 0; s < d.nscen; s++) {
+    Scalars* sc = &d.sc[s];
+    sc->rms = rms;
+    sc->tmass = tm;
+    sc->rmax = rmax;
+    sc->converged = conv;
+    if (!d.steady && d.dt_op != 0) sc->delt = dmin;
+  }
+}
+
+void launch_halo(const Dev& d, int level, uint8_t* f1, uint8_t* f2, cudaStream_t st) {
+  k_halo<<<(d.nhalo + 255) / 256, 256, 0, st>>>(d, level, f1, f2);
+}
+void launch_link_fric(const Dev& d, cudaStream_t st) { k_link_fric<<<1, 32, 0, st>>>(d); }
+void launch_link_dt(const Dev& d, cudaStream_t st) { k_link_dt<<<1, 32, 0, st>>>(d); }
+void launch_link(const Dev& d, cudaStream_t st) { k_link<<<1, 32, 0, st>>>(d); }
 
 // ---------------------------------------------------------------------------
 // Host launchers of the templated stage kernels (api.cu is not templated).

@@ -29,7 +29,7 @@ EXPORTS = (
     "storm_fvt_last_timing", "storm_fvt_kernel_times", "storm_fvt_destroy",
     "storm_fvt_cfl_dt_noalloc", "storm_fvt_create_batch", "storm_fvt_num_scenarios",
     "storm_fvt_set_scenario_state", "storm_fvt_get_scenario_state", "storm_fvt_scenario_stats",
-    "storm_fvt_autotune", "storm_fvt_output_vertices",
+    "storm_fvt_autotune", "storm_fvt_output_vertices", "storm_fvt_link_partitions",
 )
 
 KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux")
@@ -83,6 +83,7 @@ def lib():
     L.storm_fvt_scenario_stats.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.StepStats)]
     L.storm_fvt_autotune.argtypes = [C.c_void_p, C.c_int32, ip]
     L.storm_fvt_output_vertices.argtypes = [C.c_void_p, C.POINTER(abi.OutputBoundary), C.c_int32] + [dp] * 5
+    L.storm_fvt_link_partitions.argtypes = [C.c_void_p, C.c_int32, ip, ip, ip, ip, C.c_int32]
     _lib = L
     return L
 
