@@ -272,6 +272,49 @@ def halo_pairs(parts: list[Part], part_of_cell: np.ndarray):
     return cat(ds), cat(de), cat(ss), cat(se)
 
 
+def exchange_plan(parts: list[Part], part_of_cell: np.ndarray) -> dict:
+    """Per ordered pair (owner q, receiver p): the owner's local elements (1-based) to
+    send and the receiver's local elements to fill, in the same order, for one part
+    per process.  Every halo cell appears in exactly one receive list."""
+    plan = {}
+    for p, P in enumerate(parts):
+        halo = P.cells[~P.owned]
+        owner = part_of_cell[halo]
+        for q in np.unique(owner):
+            g = halo[owner == q]
+            plan[(int(q), p)] = (np.searchsorted(parts[q].cells, g) + 1, np.searchsorted(P.cells, g) + 1)
+    return plan
+
+
+def exchange_halo(rank: int, plan: dict, fields: list, dist) -> None:
+    """One halo exchange between processes (one part each) over a torch.distributed
+    process group: every owner sends the values of its cells that other parts hold as
+    halo, every part writes what it receives into its halo cells.  `fields` are this
+    rank's per-cell arrays (numpy, or tensors on the process group's device).  The
+    sends and receives are posted together in (owner, receiver) order, so every rank
+    takes the same steps."""
+    import torch
+    reqs, inbox = [], []
+    for (q, p), (src, dst) in sorted(plan.items()):
+        if q == rank:
+            for f in fields:
+                t = torch.as_tensor(f)
+                reqs.append(dist.isend(t[torch.as_tensor(src - 1)].contiguous(), dst=p))
+        if p == rank:
+            for f in fields:
+                t = torch.as_tensor(f)
+                buf = torch.empty(len(dst), dtype=t.dtype, device=t.device)
+                reqs.append(dist.irecv(buf, src=q))
+                inbox.append((f, dst, buf))
+    for r in reqs:
+        r.wait()
+    for f, dst, buf in inbox:
+        if isinstance(f, np.ndarray):
+            f[dst - 1] = buf.numpy()
+        else:
+            f[torch.as_tensor(dst - 1, device=f.device)] = buf
+
+
 class PartitionedSolver:
     """One mesh solved as `nparts` linked parts of one batch handle; state and
     statistics in the global element order, as ``fvt.Solver``."""

@@ -204,3 +204,59 @@ def test_check_part_sees_a_thin_halo(storm_lib):
             pm.close()
         counts.append(n)
     assert counts[0] > 0 and counts[1] == 0
+
+
+def _free_port():
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _exchange_rank(rank, world, port, out):
+    import os
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sc = scenarios.meander(n_target=6000, seed=11)
+        mn = _global(sc)
+        T = int(mn["n_elems"])
+        part = partition.partition_cells(sc.problem, mn, world)
+        parts = partition.extended_parts(sc.problem, mn, part)
+        plan = partition.exchange_plan(parts, part)
+        rng = np.random.default_rng(0)
+        glob = [rng.random(T), rng.random(T)]          # a whole-mesh state, the same on every rank
+        P = parts[rank]
+        mine = [np.where(P.owned, g[P.cells], np.nan) for g in glob]  # halo unknown before the exchange
+        partition.exchange_halo(rank, plan, mine, dist)
+        ok = all(np.array_equal(m, g[P.cells]) for m, g in zip(mine, glob))
+        # the whole-mesh mass of this state from the owned cells of every rank
+        import torch
+        local = torch.tensor([float(np.sum(glob[0][P.cells[P.owned]] * mn["tri_area"][P.cells[P.owned]]))],
+                             dtype=torch.float64)
+        dist.all_reduce(local)
+        out.put((rank, ok, float(local[0]), float(np.sum(glob[0] * mn["tri_area"]))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_halo_exchange_over_two_gloo_ranks():
+    """One part per process: after one exchange over gloo every rank's halo cells hold
+    the owners' values, and the owned-cell sums add up to the whole mesh's."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_exchange_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=180) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+    for rank, ok, total, whole in res:
+        assert ok, rank
+        assert total == pytest.approx(whole, rel=1e-13)
