@@ -406,6 +406,50 @@ def warm_start_eval(args, local) -> dict:
     }
 
 
+def run_parts(args, rank, world, local) -> int:
+    """`--parts P`: the meander (or dam break) as P linked parts of one handle on this
+    GPU (storm_b200/partition.py) against the undivided mesh, K timed iterations of
+    each; cell-stage updates count owned cells only, so the halo's redundant work and
+    the exchange kernels show as the difference.  Also checks the final states bit for
+    bit."""
+    import torch
+    from storm_b200 import build, fvt, partition
+    build.build()
+    torch.cuda.set_device(local)
+    sc = build_workload(args)
+    opt = sc.options
+    opt.device = local
+    t0 = time.perf_counter()
+    ps = partition.PartitionedSolver(sc.problem, opt, args.parts)
+    setup_s = time.perf_counter() - t0
+    pm = fvt.build_mesh(sc.problem)
+    whole = fvt.Solver(pm, opt, keep=pm)
+    res = {}
+    for name, s in (("undivided", whole), ("parts", ps)):
+        s.set_state(sc.h0, sc.u0, sc.v0)
+        s.step(args.warmup)
+        torch.cuda.synchronize()
+        s.step(args.steps)
+        tm = (s.batch if name == "parts" else s).last_timing()
+        res[name] = {"ms_per_step": tm["step_ms"] / args.steps,
+                     "value": sc.n_elems * opt.rkorder * args.steps / (tm["step_ms"] / 1e3)}
+    a, b = whole.state(), ps.state()
+    same = all(np.array_equal(a[k].view(np.uint64), b[k].view(np.uint64)) for k in ("h", "u", "v"))
+    halo = sum(int((~P.owned).sum()) for P in ps.parts)
+    line = {"metric": f"cell-stage updates/s (FVT time step, {args.config}, {args.parts} linked parts on one GPU)",
+            "value": res["parts"]["value"], "unit": "cell-stage updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["parts"]["ms_per_step"], "higher_is_better": True,
+            "dtype": "f64" if opt.precision == 0 else "mixed", "data": "synthetic",
+            "config": {"workload": f"{args.config}-{sc.n_elems}", "parts": args.parts,
+                       "halo_cells": halo, "halo_fraction": halo / sc.n_elems},
+            "undivided": res["undivided"], "bitwise_equal_to_undivided": bool(same),
+            "partition_setup_s": setup_s}
+    print(json.dumps(line), flush=True)
+    ps.close()
+    whole.close()
+    return 0
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -438,6 +482,8 @@ def main():
                     help="held-out scenarios of the warm- vs cold-start time-to-steady (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=200, help="iterations of the end-to-end pass")
     ap.add_argument("--kt-steps", type=int, default=5, help="iterations of the per-kernel timing pass")
+    ap.add_argument("--parts", type=int, default=1,
+                    help="run the mesh as this many linked parts on one GPU (domain decomposition)")
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -486,6 +532,10 @@ def main():
         if rank != 0:
             return 0
         return run_steady_channel(args, rank, world, local)
+    if args.parts > 1:
+        if rank != 0:
+            return 0
+        return run_parts(args, rank, world, local)
 
     import torch
     dist = None
