@@ -349,7 +349,7 @@ STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, i
 STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t* chosen);
 
 /*
- * Partitions of one mesh (SURVEY-style domain decomposition, single-device form):
+ * Partitions of one mesh (domain decomposition, single-device form):
  * the scenarios of a batch handle are the parts of one mesh, each extended by two
  * rings of vertex-adjacent halo cells taken from its neighbours.  After this call:
  *  - after every RK stage but the last, and after the friction step, each halo cell

@@ -73,3 +73,20 @@ def test_culvert_batch_member_equals_alone(storm_lib, oracle_mod):
         a, g = o.state(), b.scenario_state(i)
         for k in ("h", "u", "v"):
             assert np.array_equal(_bits(a[k]), _bits(g[k])), (i, k)
+
+
+def test_culvert_mixed_precision_close(storm_lib):
+    """The mixed path (FP32 gradients and fluxes, FP64 state) with culverts stays
+    within 1 cm of FP64 over 200 iterations and conserves mass in the same way."""
+    sc = scenarios.culvert_channel()
+    pm = fvt.build_mesh(sc.problem)
+    out = []
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        with fvt.Solver(pm, _opts(sc, precision=prec), keep=pm) as g:
+            g.set_state(sc.h0, sc.u0, sc.v0)
+            st = g.step(200)
+            out.append((g.state()["h"], st))
+    (h64, s64), (hmx, smx) = out
+    assert np.all(np.isfinite(hmx))
+    assert np.max(np.abs(h64 - hmx)) < 0.01
+    assert smx["tmass"] == pytest.approx(s64["tmass"], rel=1e-6)

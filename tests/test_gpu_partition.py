@@ -86,3 +86,11 @@ def test_link_errors(storm_lib):
                                                       abi.iptr(ss), abi.iptr(se), 0))
     assert e.value.code == abi.STORM_ERR_ARG
     b.close()
+
+
+def test_wind_meander_three_parts(storm_lib):
+    """Wind terms at the vertices travel into every part with its nodes."""
+    sc = scenarios.meander(n_target=9000, seed=6)
+    sc.problem.cd[:] = 0.0
+    sc = scenarios.with_wind(sc, scenarios.wind_fields(sc.problem, at_vertices=True, seed=3))
+    _compare(sc, sc.options, 3, rounds=1, steps=30)
