@@ -478,8 +478,8 @@ def main():
                     help="arithmetic of the headline run")
     ap.add_argument("--no-mixed", action="store_true", help="skip the secondary mixed-precision run")
     ap.add_argument("--cpu-budget-s", type=float, default=60.0, help="CPU seconds of the reference arm")
-    ap.add_argument("--warm-eval", type=int, default=16,
-                    help="held-out scenarios of the warm- vs cold-start time-to-steady (0: skip)")
+    ap.add_argument("--warm-eval", type=int, default=64,
+                    help="held-out scenarios of the warm- vs cold-start time-to-steady, one batch (0: skip)")
     ap.add_argument("--e2e-steps", type=int, default=200, help="iterations of the end-to-end pass")
     ap.add_argument("--kt-steps", type=int, default=5, help="iterations of the per-kernel timing pass")
     ap.add_argument("--parts", type=int, default=1,
