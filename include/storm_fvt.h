@@ -411,8 +411,8 @@ STORM_FVT_API int storm_fvt_destroy(StormFvtHandle* hd);
 /*
  * CFL time step without any device allocation.  No counterpart in the reference:
  * it exists for callers that cannot call cudaMalloc -- a host whose device memory
- * is owned by an external pool, code running while a CUDA graph is captured, or a
- * loop that cannot take the synchronisation an allocation may bring.  It computes,
+ * is owned by an external pool, or a loop that cannot take the synchronisation an
+ * allocation may bring.  It computes,
  * from device arrays in any cell order, the value storm_fvt_step reports as the next
  * dt for dt_op = 1:  *d_dt = MIN over cells of cfl*area/((|u|+c+small)*perim) with
  * |u| and c = sqrt(g h) of the find_dry_cells classification (deltatFVT.f90:32-38,

@@ -2,10 +2,8 @@
 //
 // Some callers cannot call cudaMalloc: a host program whose device memory is owned by
 // an external pool (the pool hands out every byte, and a stray allocation would
-// break its accounting or fail), code that runs while a CUDA graph is being
-// captured (an allocation there is not captured and may serialise the device), and
-// time-critical loops that cannot afford the implicit synchronisation an allocation
-// can bring.  storm_fvt_cfl_dt_noalloc gives them the same CFL time step that
+// break its accounting or fail), and time-critical loops that cannot afford the
+// implicit synchronisation an allocation can bring.  storm_fvt_cfl_dt_noalloc gives them the same CFL time step that
 // storm_fvt_step computes for dt_op = 1 without allocating anything: its scratch
 // (one FP64 partial minimum per thread block) lives in the file-scope array below,
 // which every GPU that loads this library holds (32 KiB) until the process exits.

@@ -1,8 +1,8 @@
 """The allocation-free CFL time step (storm_fvt_cfl_dt_noalloc) against storm_fvt_step.
 
 Callers that cannot allocate device memory (an external memory pool owns the GPU,
-a CUDA graph is being captured, or the loop cannot take an allocation's implicit
-synchronisation) use storm_fvt_cfl_dt_noalloc, whose scratch is a static device
+or the loop cannot take an allocation's implicit synchronisation) use
+storm_fvt_cfl_dt_noalloc, whose scratch is a static device
 array.  This test allocates the input/output buffers itself (the caller's side),
 then checks that two calls in a row give exactly the dt that storm_fvt_step reports
 for the next iteration (dt_op = 1): the CFL minimum is order independent and both
