@@ -12,6 +12,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fvt_device.cuh"
@@ -75,6 +76,8 @@ struct StormFvtHandle {
   void* out_buf = nullptr;
   size_t out_bytes = 0;
   void* halo_buf = nullptr;  // linked partitions: halo slots, owner slots, halo mask
+  double* io_host = nullptr;  // pinned staging of state transfers (grown on demand)
+  size_t io_n = 0;
 };
 
 namespace {
@@ -272,6 +275,7 @@ void release(StormFvtHandle* h) {
   if (h->sc_host) cudaFreeHost(h->sc_host);
   if (h->out_buf) cudaFree(h->out_buf);
   if (h->halo_buf) cudaFree(h->halo_buf);
+  if (h->io_host) cudaFreeHost(h->io_host);
   delete h;
 }
 
@@ -505,9 +509,39 @@ int upload(StormFvtHandle* h) {
   return 0;
 }
 
-template <class Tv>
-void scatter_old(const std::vector<int32_t>& new2old, const Tv* src_new, Tv* dst_old, size_t n) {
-  for (size_t i = 0; i < n; i++) dst_old[new2old[i]] = src_new[i];
+// fn(i0, i1) over [0, n) in contiguous chunks on up to 8 host threads (one below
+// 256k items): the state permutations of large meshes are memory-latency bound.
+template <class F>
+void par_chunks(size_t n, F fn) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = n < (size_t)1 << 18 ? 1 : std::min<size_t>(std::min(8u, hw), n >> 16);
+  if (nt <= 1) {
+    fn((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t step = (n + nt - 1) / nt;
+  for (size_t t = 1; t < nt; t++) th.emplace_back(fn, std::min(n, t * step), std::min(n, (t + 1) * step));
+  fn((size_t)0, std::min(n, step));
+  for (auto& x : th) x.join();
+}
+
+// Pinned host staging of at least n doubles for the state transfers (page-locked
+// memory copies at full PCIe/C2C speed and asynchronously); nullptr if it cannot be
+// had, and the caller then stages in pageable memory.
+double* io_buffer(StormFvtHandle* h, size_t n) {
+  if (h->io_n >= n) return h->io_host;
+  if (h->io_host) cudaFreeHost(h->io_host);
+  h->io_host = nullptr;
+  h->io_n = 0;
+  void* p = nullptr;
+  if (cudaMallocHost(&p, n * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  h->io_host = static_cast<double*>(p);
+  h->io_n = n;
+  return h->io_host;
 }
 
 }  // namespace
@@ -614,17 +648,24 @@ int storm_fvt_set_scenario_state(StormFvtHandle* h, int32_t sid, const double* h
   const HostLayout& P = h->parts[sid];
   const ScenarioInfo& I = h->info[sid];
   const int Ts = P.T;
-  std::vector<double> buf(3 * (size_t)Ts);
-  for (int c = 0; c < Ts; c++) {
-    int o = P.cell_old[c];
-    buf[c] = hh[o];
-    buf[Ts + c] = u[o];
-    buf[2 * (size_t)Ts + c] = v[o];
+  std::vector<double> pageable;
+  double* buf = io_buffer(h, 3 * (size_t)Ts);
+  if (!buf) {
+    pageable.resize(3 * (size_t)Ts);
+    buf = pageable.data();
   }
+  par_chunks((size_t)Ts, [&](size_t c0, size_t c1) {
+    for (size_t c = c0; c < c1; c++) {
+      const int o = P.cell_old[c];
+      buf[c] = hh[o];
+      buf[Ts + c] = u[o];
+      buf[2 * (size_t)Ts + c] = v[o];
+    }
+  });
   const Dev& d = h->d;
-  CK(cudaMemcpyAsync(d.rkh + I.cell_off, buf.data(), 8 * (size_t)Ts, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(d.u_a + I.cell_off, buf.data() + Ts, 8 * (size_t)Ts, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(d.v_a + I.cell_off, buf.data() + 2 * (size_t)Ts, 8 * (size_t)Ts, cudaMemcpyHostToDevice,
+  CK(cudaMemcpyAsync(d.rkh + I.cell_off, buf, 8 * (size_t)Ts, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(d.u_a + I.cell_off, buf + Ts, 8 * (size_t)Ts, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(d.v_a + I.cell_off, buf + 2 * (size_t)Ts, 8 * (size_t)Ts, cudaMemcpyHostToDevice,
                      h->stream));
   k_init<<<I.blk_cnt, kRed, 0, h->stream>>>(d, I.cell_off);
   k_init_final<<<1, kRed, 0, h->stream>>>(d, sid);
@@ -743,24 +784,47 @@ int storm_fvt_get_scenario_state(StormFvtHandle* h, int32_t sid, double* hh, dou
   const HostLayout& P = h->parts[sid];
   const ScenarioInfo& I = h->info[sid];
   const int Ts = P.T, Ns = P.N;
-  std::vector<double> buf(std::max(Ts, Ns));
-  auto pull = [&](const double* dev, double* dst, int n, const std::vector<int32_t>& perm) -> int {
-    if (!dst) return 0;
-    CK(cudaMemcpyAsync(buf.data(), dev, 8 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+  const size_t m = (size_t)std::max(Ts, Ns);
+  // up to three arrays per round trip: their copies are issued together into the
+  // staging buffer, then each is permuted back to the caller's element order
+  std::vector<double> pageable;
+  double* buf = io_buffer(h, 3 * m);
+  if (!buf) {
+    pageable.resize(3 * m);
+    buf = pageable.data();
+  }
+  struct Pull {
+    const double* dev;
+    double* dst;
+    int n;
+    const std::vector<int32_t>* perm;
+  };
+  auto round = [&](std::initializer_list<Pull> items) -> int {
+    size_t k = 0;
+    for (const Pull& it : items)
+      if (it.dst) CK(cudaMemcpyAsync(buf + (k++) * m, it.dev, 8 * (size_t)it.n, cudaMemcpyDeviceToHost, h->stream));
+    if (k == 0) return 0;
     CK(cudaStreamSynchronize(h->stream));
-    scatter_old(perm, buf.data(), dst, n);
+    k = 0;
+    for (const Pull& it : items) {
+      if (!it.dst) continue;
+      const double* src = buf + (k++) * m;
+      par_chunks((size_t)it.n, [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; i++) it.dst[(*it.perm)[i]] = src[i];
+      });
+    }
     return 0;
   };
   const Dev& d = h->d;
   const int co = I.cell_off, no = I.node_off;
   int rc;
-  if ((rc = pull(d.rkh + co, hh, Ts, P.cell_old))) return rc;
-  if ((rc = pull(d.u_a + co, u, Ts, P.cell_old))) return rc;
-  if ((rc = pull(d.v_a + co, v, Ts, P.cell_old))) return rc;
-  if ((rc = pull(d.rkh + co, rkh, Ts, P.cell_old))) return rc;
-  if ((rc = pull(d.rku + co, rku, Ts, P.cell_old))) return rc;
-  if ((rc = pull(d.rkv + co, rkv, Ts, P.cell_old))) return rc;
-  if ((rc = pull(d.hvtx + no, hvtx, Ns, P.node_old))) return rc;
+  if ((rc = round({{d.rkh + co, hh, Ts, &P.cell_old}, {d.u_a + co, u, Ts, &P.cell_old},
+                   {d.v_a + co, v, Ts, &P.cell_old}})))
+    return rc;
+  if ((rc = round({{d.rkh + co, rkh, Ts, &P.cell_old}, {d.rku + co, rku, Ts, &P.cell_old},
+                   {d.rkv + co, rkv, Ts, &P.cell_old}})))
+    return rc;
+  if ((rc = round({{d.hvtx + no, hvtx, Ns, &P.node_old}}))) return rc;
   return STORM_OK;
 }
 
