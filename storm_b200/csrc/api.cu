@@ -12,6 +12,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -521,8 +522,16 @@ void par_chunks(size_t n, F fn) {
   }
   std::vector<std::thread> th;
   const size_t step = (n + nt - 1) / nt;
-  for (size_t t = 1; t < nt; t++) th.emplace_back(fn, std::min(n, t * step), std::min(n, (t + 1) * step));
+  size_t done = step;  // chunks [step, done) are covered by started threads
+  try {
+    for (size_t t = 1; t < nt; t++) {
+      th.emplace_back(fn, std::min(n, t * step), std::min(n, (t + 1) * step));
+      done = std::min(n, (t + 1) * step);
+    }
+  } catch (const std::system_error&) {  // no more threads: the caller's thread does the rest
+  }
   fn((size_t)0, std::min(n, step));
+  if (done < n) fn(done, n);
   for (auto& x : th) x.join();
 }
 

@@ -465,7 +465,7 @@ __device__ __forceinline__ float limited_r(double q0, double qn, float g_x, floa
 }
 
 template <class R>
-__global__ void __launch_bounds__(256, 4) k_grad(Dev d, Geo<R> G, const double* __restrict__ hs,
+__global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* __restrict__ hs,
                                               const uint8_t* __restrict__ dry, double* __restrict__ rku_prev,
                                               double* __restrict__ rkv_prev) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
