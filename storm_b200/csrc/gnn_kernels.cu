@@ -189,8 +189,8 @@ __device__ __forceinline__ void stage_segment(const Seg& s, int row0, uint8_t* d
     return;
   }
   // aggregation: sum of the three edge rows of each cell, in rounds of eight chunks
-  // per thread (24 loads in flight) for the 128 producer threads, four otherwise
-  if (nthr <= 128) stage_agg_rounds<8>(s, row0, dst, tid, nthr, cpr, total);
+  // per thread (24 loads in flight) for the forward kernel's producers, four otherwise
+  if (nthr <= 224) stage_agg_rounds<8>(s, row0, dst, tid, nthr, cpr, total);
   else stage_agg_rounds<4>(s, row0, dst, tid, nthr, cpr, total);
 }
 
@@ -254,7 +254,7 @@ __device__ __forceinline__ void stage_matrix(const bf16* src, int nrows, int nco
   }
 }
 
-constexpr int kProducersAsync = 128;
+constexpr int kProducersAsync = 352;
 
 // Asynchronous copy of one 16-byte chunk global -> shared (zero-filled when `valid` is
 // false); the copies of a thread are grouped with commit / wait_group.
@@ -270,9 +270,9 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Issue (without waiting) the copies of one gathered, non-aggregated segment tile by
-// the 128 producer threads: every thread resolves the source rows of its (at most 16)
+// the 352 producer threads: every thread resolves the source rows of its (at most 6)
 // chunks first, all index loads in flight together, then issues its copies.
-constexpr int kMaxAsyncChunks = 16;  // 128 rows x 16 chunks / 128 threads
+constexpr int kMaxAsyncChunks = (kRows * 16 + kProducersAsync - 1) / kProducersAsync;  // 128 x 16 chunks
 __device__ __forceinline__ void stage_segment_async(const Seg& s, int row0, uint8_t* dst, int tid) {
   const int cpr = s.width >> 3;
   const int total = kRows * cpr;
@@ -318,20 +318,22 @@ __host__ __device__ constexpr size_t fwd_smem_bytes(int k_in, int n_out) {
          2 * (kRows * 128 * 2) + kRows * kHid * 2 + 256;
 }
 
-// Warp roles of the forward kernel (288 threads):
-//   warps 0-3  producers: gather each input segment of the CTA's tiles into the
-//              two-buffer staging ring (a buffer is refilled once the MMAs that read
-//              it have completed);
-//   warps 4-7  epilogue: TMEM -> bias + ReLU -> hidden tile, then TMEM -> bias
-//              (+ residual) -> output; warp 4+q reads TMEM lanes 32q..32q+31;
-//   warp 8     one thread issues the MMAs: D1[slot] = A W1^T over the segments, then
-//              D2[slot] = a1 W2^T once the epilogue has written the hidden tile.
+// Warp roles of the forward kernel (512 threads, sixteen warps, so up to 128
+// registers each):
+//   warps 0-10  producers: gather each input segment of the CTA's tiles into the
+//               two-buffer staging ring (a buffer is refilled once the MMAs that read
+//               it have completed); the gathers of scattered rows are what bounds the
+//               kernel, so most warps do them;
+//   warps 11-14 epilogue: TMEM -> bias + ReLU -> hidden tile, then TMEM -> bias
+//               (+ residual) -> output; warp w reads TMEM lanes 32(w%4)..32(w%4)+31;
+//   warp 15     one thread issues the MMAs: D1[slot] = A W1^T over the segments, then
+//               D2[slot] = a1 W2^T once the epilogue has written the hidden tile.
 // D1 and D2 are double-buffered in TMEM (slot = tile parity), so the MMAs of tile t+1
 // proceed while the epilogue drains tile t.  Every wait is bounded; a wait that runs
 // out raises the abort flag, which every role polls.
-constexpr int kFwdThreads = 288;
+constexpr int kFwdThreads = 512;
 __device__ __forceinline__ bool aborted(const int* flag) { return *reinterpret_cast<const volatile int*>(flag) != 0; }
-constexpr int kProducers = 128;
+constexpr int kProducers = 352;
 
 __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(MlpFwd p) {
   extern __shared__ uint8_t smem_raw[];
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(MlpFwd p) {
   uint8_t* abuf = w2s + p.n_out * kHid * 2;  // 2 x 32 KB
   uint8_t* a1s = abuf + 2 * (kRows * 128 * 2);
   uint64_t* bars = reinterpret_cast<uint64_t*>(a1s + kRows * kHid * 2);
-  uint64_t* full = bars;        // [2] staging buffer filled (128 producer arrivals)
+  uint64_t* full = bars;        // [2] staging buffer filled (one arrival per producer)
   uint64_t* empty = bars + 2;   // [2] MMAs reading the buffer done (commit)
   uint64_t* d1full = bars + 4;  // [2] D1[slot] complete (commit)
   uint64_t* a1full = bars + 6;  // hidden tile written (128 epilogue arrivals)
@@ -388,7 +390,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(MlpFwd p) {
   const uint32_t tmem = *tmem_slot;
   const int ntiles = p.rows / kRows;
 
-  if (warp < 4) {
+  if (warp < 11) {
     // ---- producers
     // Gathered segments are copied with cp.async, keeping the copies of two segments
     // in flight (a segment is announced once the next one has been issued); the
@@ -431,7 +433,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(MlpFwd p) {
       umma::fence_async_smem();
       umma::mbar_arrive(&full[pending]);
     }
-  } else if (warp < 8) {
+  } else if (warp < 15) {
     // ---- epilogue
     const int q = warp & 3;
     const int r = q * 32 + lane;  // row of the tile = TMEM lane
