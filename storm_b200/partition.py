@@ -23,8 +23,8 @@ with one part per GPU the exchange reads the owners' values from the peer GPUs.
 
 Open-boundary strings are kept whole: every cell within two rings of a string's
 nodes belongs to the part that owns the string, so no other part's owned or first-
-ring cell touches a boundary node or edge.  Culverts (which couple distant cells) and residual
-smoothing (an order-dependent sweep) are not supported.
+ring cell touches a boundary node or edge.  Culverts (which couple distant cells)
+and residual smoothing (an order-dependent sweep) are not supported.
 """
 from __future__ import annotations
 
