@@ -24,7 +24,6 @@ namespace storm {
 __global__ void k_init(Dev d, int c0);
 __global__ void k_init_final(Dev d, int sid);
 __global__ void k_node(Dev d, const double* hs, const uint8_t* dry);
-__global__ void k_fric(Dev d);
 __global__ void k_final(Dev d);
 
 static thread_local std::string g_err;
@@ -227,7 +226,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
   }
   if (linked && d.steady) launch_link_fric(d, h->stream);
   if (mark(KT_FRIC)) return STORM_ERR_CUDA;
-  k_fric<<<d.nblk_red, kRed, 0, h->stream>>>(d);
+  launch_fric(d, h->stream);
   if (done()) return STORM_ERR_CUDA;
   if (d.nhalo > 0) launch_halo(d, 0, d.dry_a, d.dry_out, h->stream);
   if (mark(KT_FINAL)) return STORM_ERR_CUDA;

@@ -138,6 +138,8 @@ void launch_halo(const Dev& d, int level, uint8_t* f1, uint8_t* f2, cudaStream_t
 void launch_link_fric(const Dev& d, cudaStream_t st);
 void launch_link(const Dev& d, cudaStream_t st);
 void launch_link_dt(const Dev& d, cudaStream_t st);
+// Friction, hvalve and the iteration partials (halo cells left out when linked).
+void launch_fric(const Dev& d, cudaStream_t st);
 void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st);
 
 // The output pass (to_vertices, ctr2vtx of cd, error_est(2)) after an iteration.

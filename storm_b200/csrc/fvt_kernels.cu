@@ -1302,6 +1302,8 @@ __global__ void __launch_bounds__(128) k_flux_bc(Dev d, Geo<R> G, int s, const d
 // ---------------------------------------------------------------------------
 // After the RK stages: find_dry_cells, fric_terms_impl, hvalve, rk level copy and the
 // block partials of the iteration's reductions (solverFVT.f90:335-386, 407-445).
+// kHalo: the handle links partitions, and halo cells stay out of the partials.
+template <bool kHalo>
 __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
   __shared__ double sm[kRedThreads / 32];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1387,7 +1389,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
     rm = dry2 ? kZero : d.phimax[c];
     const double wc1 = dry1 ? kZero : sqrt(kG * h);
     dtc = d.cfl * d.area[c] / ((um1 + wc1 + SMALL_F) * d.perim[c]);
-    if (d.halo_mask && d.halo_mask[c]) {  // a halo copy: its owner counts it
+    if (kHalo && d.halo_mask[c]) {  // a halo copy: its owner counts it
       st = kZero; sb = kZero; tm = kZero; rm = kZero; dtc = kVlarge;
     } else if (!isfinite(h) || !isfinite(u) || !isfinite(v)) {
       atomicOr(&d.sc[sid].status, 1);
@@ -1798,6 +1800,10 @@ void launch_halo(const Dev& d, int level, uint8_t* f1, uint8_t* f2, cudaStream_t
   k_halo<<<(d.nhalo + 255) / 256, 256, 0, st>>>(d, level, f1, f2);
 }
 void launch_link_fric(const Dev& d, cudaStream_t st) { k_link_fric<<<1, 32, 0, st>>>(d); }
+void launch_fric(const Dev& d, cudaStream_t st) {
+  if (d.nhalo > 0) k_fric<true><<<d.nblk_red, kRedThreads, 0, st>>>(d);
+  else k_fric<false><<<d.nblk_red, kRedThreads, 0, st>>>(d);
+}
 void launch_link_dt(const Dev& d, cudaStream_t st) { k_link_dt<<<1, 32, 0, st>>>(d); }
 void launch_link(const Dev& d, cudaStream_t st) { k_link<<<1, 32, 0, st>>>(d); }
 
