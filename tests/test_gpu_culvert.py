@@ -91,3 +91,22 @@ def test_culvert_mixed_precision_close(storm_lib):
     assert np.all(np.isfinite(hmx))
     assert np.max(np.abs(h64 - hmx)) < 0.01
     assert smx["tmass"] == pytest.approx(s64["tmass"], rel=1e-4)
+
+
+def test_culvert_wind_and_smoothing_together_bitwise(storm_lib, oracle_mod):
+    """All three extra source paths at once (culverts, wind, residual smoothing in
+    colour order) against the oracle, bit for bit."""
+    sc = scenarios.culvert_channel()
+    sc.problem.cd[:] = 0.0
+    sc = scenarios.with_wind(sc, scenarios.wind_fields(sc.problem, at_vertices=False, seed=5))
+    opt = _opts(sc, rsavg_passes=2, rsavg_order=1, rsavg_eps=0.5)
+    o = oracle_mod.Oracle(sc.problem, opt)
+    pm = fvt.build_mesh(sc.problem)
+    with fvt.Solver(pm, opt, keep=pm) as g:
+        for s in (o, g):
+            s.set_state(sc.h0, sc.u0, sc.v0)
+        o.step(40)
+        g.step(40)
+        a, b = o.state(), g.state()
+        for k in ("h", "u", "v", "rkh", "rku", "rkv"):
+            assert np.array_equal(_bits(a[k]), _bits(b[k])), k
