@@ -328,18 +328,20 @@ class PartitionedSolver:
         self.part = partition_cells(problem, mn, nparts)
         tri0 = problem.tri.reshape(self.T, 3).astype(np.int64) - 1
         adj = _Adjacency(tri0, self.N)
-        self.parts, self.meshes = [], []
-        for p in range(nparts):
+        def prepare(p):
             for rings in range(3, 9):
                 P = extended_parts(problem, mn, self.part, rings=rings, only=[p])[0]
                 pm = fvt.build_mesh(P.problem)
                 if check_part(mn, pm.numpy(), P, adj) == 0:
-                    break
+                    return P, pm
                 pm.close()
-            else:
-                raise ValueError(f"part {p}: no halo depth reproduces the global mesh's data")
-            self.parts.append(P)
-            self.meshes.append(pm)
+            raise ValueError(f"part {p}: no halo depth reproduces the global mesh's data")
+        # the parts are prepared side by side (the mesh builder runs outside the GIL)
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=min(nparts, 8)) as ex:
+            done = list(ex.map(prepare, range(nparts)))
+        self.parts = [P for P, _ in done]
+        self.meshes = [pm for _, pm in done]
         for m in self.meshes:  # the inflow safety-net elevation is a whole-mesh figure
             m.mesh.bch_max = gm.mesh.bch_max
         gm.close()
