@@ -39,7 +39,6 @@ CASES = {
 }
 
 
-
 def _wind_case(sc, at_vertices):
     return scenarios.with_wind(sc, scenarios.wind_fields(sc.problem, at_vertices))
 
@@ -145,3 +144,19 @@ def test_fewer_than_four_triangles_rejected(storm_lib, oracle_mod):
     assert e.value.code == abi.STORM_ERR_MESH
     with pytest.raises(oracle_mod.OracleError):
         oracle_mod.Oracle(p, abi.default_options())
+
+
+def test_host_checks_of_the_newer_entry_points(storm_lib):
+    """Argument checks that run before any device work: linking a null handle, and
+    residual-smoothing options out of range."""
+    L = fvt.lib()
+    z = np.zeros(1, dtype=np.int32)
+    rc = L.storm_fvt_link_partitions(None, 1, abi.iptr(z), abi.iptr(z), abi.iptr(z), abi.iptr(z), 0)
+    assert rc == abi.STORM_ERR_ARG
+    assert b"null handle" in L.storm_fvt_last_error()
+    sc = scenarios.channel(nx=10, ny=4)
+    pm = fvt.build_mesh(sc.problem)
+    for kw in ({"rsavg_passes": -1}, {"rsavg_passes": 2, "rsavg_order": 1, "rsavg_eps": -0.5}):
+        with pytest.raises(fvt.StormError) as e:
+            fvt.Solver(pm, fvt.default_options(**kw))
+        assert e.value.code == abi.STORM_ERR_ARG, kw
