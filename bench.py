@@ -18,8 +18,13 @@ Arms:
                     port (the Fortran reference has no compiler on these machines),
                     all host threads, same mesh and metric.
 
-Multi-GPU (torchrun, one rank per GPU): every rank advances its own copy of the
-scenario (independent units, no collective on the data path): weak scaling.
+Multi-GPU (one rank per GPU): `--gpus N` outside a torchrun environment re-launches
+this script under torch.distributed.run with N local ranks (127.0.0.1 rendezvous).
+On the single-mesh workloads every rank advances its own copy of the scenario
+(replicas: independent units, no collective on the data path): weak scaling.  On
+`--config batch` the ensemble's members are shared over the ranks by cell count.
+`--dist-check` brings the ranks up on the gloo backend and reports them, with no GPU
+work (a CPU check of the launch path).
 """
 from __future__ import annotations
 
@@ -41,8 +46,8 @@ import numpy as np  # noqa: E402
 from storm_b200 import scenarios  # noqa: E402
 
 METRIC = "cell-stage updates/s (FVT time step, 2M-triangle meander)"
-# DRAM bytes (read + write) per cell-stage of the stage kernels, from one ncu capture of
-# the same kernels on the 500k-cell meander (profiles/fvt_stage_kernels_meander.md);
+# DRAM bytes (read + write) per cell-stage of one iteration's kernels, from ncu
+# captures of the same kernels on the 500k-cell meander (one kernel per capture);
 # traffic grows in proportion to the cells, so it is scaled to the workload's mesh.
 NCU_DRAM_BYTES_PER_CELL_STAGE = {"meander": 714.6}
 UNIT = "cell-stage updates/s"
@@ -274,7 +279,7 @@ def run_steady_channel(args, rank, world, local):
            "config": {"workload": "channel-8000", "rstop": 1e-8, "istop": args.istop, "flux": "HLL",
                       "limiter": "LSQ + BJ", "rk": 3, "cfl": 0.9}, "gpu": res}
     if not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
+        threads = len(os.sched_getaffinity(0)) or 1
         sc = scenarios.channel()
         n = max(1, min(args.istop, args.cpu_steps))
         for th, key in ((1, "cpu_1_thread"), (threads, "cpu_all_threads")):
@@ -450,6 +455,44 @@ def run_parts(args, rank, world, local) -> int:
     return 0
 
 
+def workload_config(args, T, E, N, rkorder, flux, world, dry_fraction):
+    """The `config` object of the JSON line, the same keys in both arms."""
+    return {"workload": f"{args.config}-{T}", "cells": T, "edges": E, "nodes": N, "rkorder": rkorder,
+            "flux": int(flux), "precision": args.precision, "parallelism": f"replicas x{world}",
+            "l2": "working set > L2 (inputs larger than the 126 MB L2)", "dry_fraction": dry_fraction}
+
+
+def spawn_ranks(n: int) -> int:
+    """Re-launch this script with the same arguments as n local ranks under
+    torch.distributed.run (rendezvous on 127.0.0.1, a free port); returns its status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def dist_check(args, rank, world) -> int:
+    """Bring the ranks up on gloo (no GPU), sum one value over them and report."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+        t = torch.ones(1, dtype=torch.float64)
+        dist.all_reduce(t)
+        seen = int(t.item())
+        dist.destroy_process_group()
+    else:
+        seen = 1
+    if rank == 0:
+        print(json.dumps({"metric": "launch check (no GPU work)", "dist_check": True, "n_gpus": world,
+                          "ranks_seen": seen, "backend": "gloo" if world > 1 else None}))
+    return 0 if seen == world else 1
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -484,13 +527,19 @@ def main():
     ap.add_argument("--kt-steps", type=int, default=5, help="iterations of the per-kernel timing pass")
     ap.add_argument("--parts", type=int, default=1,
                     help="run the mesh as this many linked parts on one GPU (domain decomposition)")
+    ap.add_argument("--dist-check", action="store_true",
+                    help="bring up --gpus ranks on gloo and report them (no GPU work)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args.gpus)
     rank, world, local = dist_env()
+    if args.dist_check:
+        return dist_check(args, rank, world)
 
     if args.impl == "reference":
         if rank != 0:
             return 0
-        threads = os.cpu_count() or 1
+        threads = len(os.sched_getaffinity(0)) or 1
         sc = build_workload(args)
         from oracle import oracle as _o
         _o.build()
@@ -498,6 +547,9 @@ def main():
         # number of timed iterations is capped so the arm ends within about a minute
         from oracle.oracle import Oracle
         o = Oracle(sc.problem, sc.options, threads=threads)
+        om = o.mesh()
+        ref_config = workload_config(args, sc.n_elems, om.n_edges, om.n_pts, sc.options.rkorder, sc.options.flux,
+                                     world, sc.info.get("dry_fraction"))
         o.set_state(sc.h0, sc.u0, sc.v0)
         t0 = time.perf_counter()
         o.step(max(1, min(args.warmup, 2)))
@@ -512,8 +564,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / n_timed,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator)",
-            "config": {"workload": f"{args.config}-{sc.n_elems}", "cells": sc.n_elems,
-                       "rkorder": sc.options.rkorder, "parallelism": "host threads"},
+            "config": ref_config, "host_threads": threads,
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{n_timed} of the {args.steps} requested iterations of the "
                                        f"{sc.n_elems}-cell workload, timed ({secs:.1f} s)"},
@@ -672,10 +723,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
         "data": "synthetic (seeded generator; no public dataset exists for this path)",
-        "config": {"workload": f"{args.config}-{T}", "cells": T, "edges": E, "nodes": N, "rkorder": K_rk,
-                   "flux": int(sc.options.flux), "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "working set > L2 (inputs larger than the 126 MB L2)",
-                   "dry_fraction": sc.info.get("dry_fraction")},
+        "config": workload_config(args, T, E, N, K_rk, sc.options.flux, world, sc.info.get("dry_fraction")),
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "gpu_launches": gpu_launches,
@@ -689,7 +737,7 @@ def main():
     if rank == 0 and world == 1 and args.warm_eval > 0 and args.config == "meander":
         out["time_to_steady"] = warm_start_eval(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
+        threads = len(os.sched_getaffinity(0)) or 1
         cv, secs = run_cpu(sc, args.cpu_steps, threads)
         out["cpu_baseline"] = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
                                "sample": f"{args.cpu_steps} iterations of the same {T}-cell workload "

@@ -419,8 +419,13 @@ STORM_FVT_API int storm_fvt_destroy(StormFvtHandle* hd);
  * with the cell area and perimeter).  Its scratch is a 32 KiB static device array,
  * so at most 1,048,576 cells per call (larger n: STORM_ERR_ARG, nothing launched).
  * Asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).  The
- * first call on a device resolves the array's address (make it before any stream
- * capture); calls share the array, so calls that overlap on the GPU race.
+ * array's address belongs to a CUDA context: a call outside stream capture resolves
+ * it in the current context and records it; a call during capture uses the recorded
+ * address of the current context (STORM_ERR_ARG if there is none).  The first call
+ * in a context also loads the library's device module (lazy loading), which
+ * allocates device memory and may synchronise: make it while allocation is still
+ * allowed and outside capture, and again after cudaDeviceReset or a context change.
+ * Calls share the array, so calls that overlap on the GPU race.
  */
 STORM_FVT_API int storm_fvt_cfl_dt_noalloc(const double* d_h, const double* d_u, const double* d_v,
                                            const double* d_area, const double* d_perim, int32_t n,

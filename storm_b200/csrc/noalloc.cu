@@ -11,9 +11,17 @@
 // Limits and rules of use:
 //   * at most kNoAllocMaxCells cells per call (4,096 blocks x 256 threads); larger
 //     inputs are rejected with STORM_ERR_ARG before anything is launched;
-//   * the first call on a device resolves the array's device address with
-//     cudaGetSymbolAddress (once per device, with that device current); make that
-//     first call before any stream capture;
+//   * the array's address belongs to a CUDA context, not to a device ordinal.  A call
+//     made outside stream capture resolves it with cudaGetSymbolAddress in the
+//     calling thread's current context and records it for that context; a call made
+//     while `stream` is being captured uses the recorded address of the current
+//     context and fails (STORM_ERR_ARG) if that context has none;
+//   * with CUDA's lazy module loading, the first call in a context loads this
+//     library's device module, and loading it allocates device memory for the array
+//     and the code and may synchronise.  Make that first call while allocation is
+//     still allowed: before an external pool takes the device's memory, and outside
+//     any stream capture.  After cudaDeviceReset, or when a context is destroyed and
+//     another made current, make one call outside capture again before capturing;
 //   * every call shares the one array, which keeps the last call's partials; a call
 //     overwrites every partial it reads, so nothing needs clearing, but calls that
 //     overlap on the GPU (different streams, or different host threads) race;
@@ -22,6 +30,8 @@
 
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "storm_internal.h"
 
@@ -31,7 +41,6 @@ namespace {
 constexpr int kNaThreads = 256;
 constexpr int kNaMaxBlocks = 4096;
 constexpr int64_t kNoAllocMaxCells = (int64_t)kNaMaxBlocks * kNaThreads;  // 1,048,576
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_dt_partials[kNaMaxBlocks];
 
@@ -93,8 +102,26 @@ __global__ void __launch_bounds__(kNaThreads) k_cfl_dt_final(const double* __res
   }
 }
 
+// Address of g_dt_partials per CUDA context (the driver's CUcontext handle), looked up
+// through the runtime's driver entry point so the library needs no link to libcuda.
+using CtxGetCurrentFn = int (*)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
 std::mutex g_na_mutex;
-double* g_na_addr[kMaxDevices] = {nullptr};
+CtxGetCurrentFn g_ctx_get = nullptr;
+std::vector<std::pair<void*, double*>> g_na_addr;
+
+int current_context(void** ctx) {
+  if (!g_ctx_get) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+      return set_error(STORM_ERR_CUDA, "storm_fvt_cfl_dt_noalloc: cuCtxGetCurrent is not available");
+    g_ctx_get = reinterpret_cast<CtxGetCurrentFn>(fn);
+  }
+  *ctx = nullptr;
+  if (g_ctx_get(ctx) != 0) return set_error(STORM_ERR_CUDA, "storm_fvt_cfl_dt_noalloc: cuCtxGetCurrent failed");
+  return STORM_OK;
+}
 
 }  // namespace
 }  // namespace storm
@@ -111,25 +138,44 @@ extern "C" int storm_fvt_cfl_dt_noalloc(const double* d_h, const double* d_u, co
     return set_error(STORM_ERR_ARG, "storm_fvt_cfl_dt_noalloc: n = " + std::to_string(n) +
                                         " exceeds the static scratch limit of " +
                                         std::to_string(kNoAllocMaxCells) + " cells");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cap);
   if (e != cudaSuccess)
     return set_error(STORM_ERR_CUDA, std::string("storm_fvt_cfl_dt_noalloc: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return set_error(STORM_ERR_ARG, "storm_fvt_cfl_dt_noalloc: device ordinal too large");
   double* part = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_addr[dev]) {  // once per device, with that device current
+    void* ctx = nullptr;
+    if (cap == cudaStreamCaptureStatusNone) {
+      // resolve in the current context (this also makes the primary context current
+      // on a thread that has none yet), then record it for that context
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_dt_partials);
       if (e != cudaSuccess || !p)
         return set_error(STORM_ERR_CUDA, std::string("storm_fvt_cfl_dt_noalloc: cudaGetSymbolAddress: ") +
                                              cudaGetErrorString(e));
-      g_na_addr[dev] = static_cast<double*>(p);
+      int rc = current_context(&ctx);
+      if (rc) return rc;
+      part = static_cast<double*>(p);
+      bool found = false;
+      for (auto& kv : g_na_addr)
+        if (kv.first == ctx) {
+          kv.second = part;
+          found = true;
+        }
+      if (!found) g_na_addr.emplace_back(ctx, part);
+    } else {
+      int rc = current_context(&ctx);
+      if (rc) return rc;
+      for (const auto& kv : g_na_addr)
+        if (kv.first == ctx) part = kv.second;
+      if (!part)
+        return set_error(STORM_ERR_ARG,
+                         "storm_fvt_cfl_dt_noalloc: first call in this CUDA context made during stream capture; "
+                         "make one call outside capture first");
     }
-    part = g_na_addr[dev];
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int nblk = (n + kNaThreads - 1) / kNaThreads;
   k_cfl_dt_partials<<<nblk, kNaThreads, 0, s>>>(d_h, d_u, d_v, d_area, d_perim, n, cfl, h_dry, h_wet, part);
   k_cfl_dt_final<<<1, kNaThreads, 0, s>>>(part, nblk, d_dt);

@@ -7,7 +7,9 @@ CGNS case.  The node coordinates live only in Case1.cgn (HDF5, no reader here), 
 fixture keeps the topology: edges, their element pairs, the boundary markers and the
 triangles rebuilt from the edges with one consistent orientation.
 
-Run from the repository root:  python tests/golden/make_tutorial1_fixture.py
+Run from the repository root, naming the reference checkout's Tutorial_1 folder:
+    python tests/golden/make_tutorial1_fixture.py <reference>/tests/Tutorial_1
+(or set STORM_TUTORIAL1_DIR to that folder).
 """
 import collections
 import os
@@ -15,7 +17,6 @@ import sys
 
 import numpy as np
 
-SRC = "/root/reference/tests/Tutorial_1"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tutorial1_topology.npz")
 
 
@@ -29,8 +30,11 @@ def read_table(path, ncol):
 
 
 def main():
-    e = read_table(os.path.join(SRC, "iRICZone.1.edge"), 4).astype(np.int64)
-    v = read_table(os.path.join(SRC, "iRICZone.1.v.edge"), 3).astype(np.int64)
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("STORM_TUTORIAL1_DIR")
+    if not src:
+        sys.exit("usage: make_tutorial1_fixture.py <reference>/tests/Tutorial_1")
+    e = read_table(os.path.join(src, "iRICZone.1.edge"), 4).astype(np.int64)
+    v = read_table(os.path.join(src, "iRICZone.1.v.edge"), 3).astype(np.int64)
     assert np.array_equal(e[:, 0], np.arange(1, len(e) + 1))
     assert np.array_equal(v[:, 0], np.arange(1, len(v) + 1))
     edge_p = e[:, 1:3]

@@ -21,12 +21,16 @@ pytestmark = pytest.mark.gpu
 
 class Cudart:
     def __init__(self):
+        self.rt = None
         for name in ("libcudart.so", "libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so"):
             try:
                 self.rt = C.CDLL(name)
                 break
             except OSError:
                 continue
+        if self.rt is None:
+            pytest.fail("no libcudart could be loaded to allocate the caller's buffers")
+        self.rt.cudaMemGetInfo.argtypes = [C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
         self.rt.cudaMalloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
         self.rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
         self.rt.cudaFree.argtypes = [C.c_void_p]
@@ -50,17 +54,29 @@ class Cudart:
         assert self.rt.cudaMemcpy(out.ctypes.data, p, out.nbytes, 2) == 0  # device to host
         return out
 
+    def free_bytes(self):
+        assert self.rt.cudaDeviceSynchronize() == 0
+        free, total = C.c_size_t(), C.c_size_t()
+        assert self.rt.cudaMemGetInfo(C.byref(free), C.byref(total)) == 0
+        return free.value
+
     def free(self):
         for p in self.bufs:
             self.rt.cudaFree(p)
         self.bufs = []
 
 
-def _noalloc_dt(rt, state, area, perim, o):
+def _noalloc_dt(rt, state, area, perim, o, check_free=False):
+    """One call on buffers the caller allocated beforehand.  With check_free, the
+    device's free memory is read right before and after the call (synchronised): an
+    entry point that allocates nothing leaves it unchanged."""
     d = [rt.upload(state["h"]), rt.upload(state["u"]), rt.upload(state["v"]), rt.upload(area), rt.upload(perim)]
     out = rt.empty(1)
+    f0 = rt.free_bytes() if check_free else None
     rc = fvt.lib().storm_fvt_cfl_dt_noalloc(*d, len(area), o.cfl, o.h_dry, o.h_wet, out, None)
     assert rc == 0, fvt.lib().storm_fvt_last_error().decode()
+    if check_free:
+        assert rt.free_bytes() == f0, "the allocation-free entry point changed the device's free memory"
     return rt.download(out, 1)[0]
 
 
@@ -78,7 +94,7 @@ def test_noalloc_cfl_dt_matches_step(storm_lib):
         dt1 = _noalloc_dt(rt, g.state(), area, perim, sc.options)  # first call
         assert dt1 == st["delt"], (dt1, st["delt"])
         st = g.step(2)
-        dt2 = _noalloc_dt(rt, g.state(), area, perim, sc.options)  # second call, same scratch
+        dt2 = _noalloc_dt(rt, g.state(), area, perim, sc.options, check_free=True)  # second call, same scratch
         assert dt2 == st["delt"], (dt2, st["delt"])
         assert dt1 != dt2
         # a smaller input after a larger one: stale partials of the earlier call are not read
