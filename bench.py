@@ -49,7 +49,7 @@ METRIC = "cell-stage updates/s (FVT time step, 2M-triangle meander)"
 # DRAM bytes (read + write) per cell-stage of one iteration's kernels, from ncu
 # captures of the same kernels on the 500k-cell meander (one kernel per capture);
 # traffic grows in proportion to the cells, so it is scaled to the workload's mesh.
-NCU_DRAM_BYTES_PER_CELL_STAGE = {"meander": 714.6}
+NCU_DRAM_BYTES_PER_CELL_STAGE = {("meander", "phases"): 714.6}
 UNIT = "cell-stage updates/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 
@@ -411,6 +411,77 @@ def warm_start_eval(args, local) -> dict:
     }
 
 
+def run_dambreak_trajectory(args, local) -> int:
+    """Config 3 in full: the circular dam break (Rusanov, Manning n = 0.025) run to
+    60 s simulated in FP64 and in mixed precision side by side, one iteration at a
+    time, with the mixed state compared to the FP64 state after every iteration
+    (--traj-every): depth, unit discharge (hu, hv) and total mass.  Each precision
+    takes its own CFL dt, so the simulated times drift apart slightly; that drift is
+    reported with the errors."""
+    import torch
+    from storm_b200 import abi, build, fvt
+    build.build()
+    torch.cuda.set_device(local)
+    sc = scenarios.dambreak(n_target=args.cells)
+    sc.options.device = local
+    t_end = float(sc.info.get("t_end", 60.0))
+    pm = fvt.build_mesh(sc.problem)
+    solvers = {}
+    for prec in ("fp64", "mixed"):
+        o = abi.Options.from_buffer_copy(sc.options)
+        o.precision = abi.PREC_MIXED if prec == "mixed" else abi.PREC_FP64
+        g = fvt.Solver(pm, o, keep=pm)
+        g.set_state(sc.h0, sc.u0, sc.v0)
+        solvers[prec] = g
+    a, b = solvers["fp64"], solvers["mixed"]
+    m0 = None
+    rows, worst = [], {"depth_max_abs_m": 0.0, "unit_discharge_max_abs_m2s": 0.0, "mass_rel": 0.0,
+                       "stime_diff_s": 0.0}
+    dev_ms = {"fp64": 0.0, "mixed": 0.0}
+    it = 0
+    t0 = time.perf_counter()
+    while True:
+        sa, sb = a.step(1), b.step(1)
+        dev_ms["fp64"] += a.last_timing()["step_ms"]
+        dev_ms["mixed"] += b.last_timing()["step_ms"]
+        it += 1
+        if m0 is None:
+            m0 = sa["tmass"]
+        mass_rel = abs(sb["tmass"] - sa["tmass"]) / sa["tmass"]
+        worst["mass_rel"] = max(worst["mass_rel"], mass_rel)
+        worst["stime_diff_s"] = max(worst["stime_diff_s"], abs(sb["stime"] - sa["stime"]))
+        done = sa["stime"] >= t_end or it >= args.istop
+        if it % args.traj_every == 0 or done:
+            xa, xb = a.state(), b.state()
+            dh = np.abs(xa["h"] - xb["h"])
+            dq = max(np.abs(xa["h"] * xa["u"] - xb["h"] * xb["u"]).max(),
+                     np.abs(xa["h"] * xa["v"] - xb["h"] * xb["v"]).max())
+            worst["depth_max_abs_m"] = max(worst["depth_max_abs_m"], float(dh.max()))
+            worst["unit_discharge_max_abs_m2s"] = max(worst["unit_discharge_max_abs_m2s"], float(dq))
+            if it % max(1, args.traj_every * 100) == 0 or done:
+                rows.append({"iter": it, "stime_fp64": sa["stime"], "stime_mixed": sb["stime"],
+                             "depth_max_abs_m": float(dh.max()), "depth_rms_m": float(np.sqrt(np.mean(dh * dh))),
+                             "unit_discharge_max_abs_m2s": float(dq), "mass_rel": mass_rel,
+                             "mass_drift_fp64": (sa["tmass"] - m0) / m0,
+                             "wet_cells_fp64": int((xa["h"] >= sc.options.h_dry).sum())})
+        if done:
+            break
+    wall = time.perf_counter() - t0
+    out = {"metric": "config 3: mixed precision vs FP64 along a 60 s dam break, compared every iteration",
+           "value": worst["depth_max_abs_m"], "unit": "m (max |h_mixed - h_fp64| over all iterations)",
+           "higher_is_better": False, "n_gpus": 1, "data": "synthetic (seeded generator)",
+           "config": {"workload": f"dambreak-{sc.n_elems}", "cells": sc.n_elems, "t_end_s": t_end,
+                      "flux": "Rusanov", "manning": 0.025, "compare_every": args.traj_every},
+           "iterations": it, "worst_over_trajectory": worst,
+           "device_ms_per_iteration": {k: v / it for k, v in dev_ms.items()},
+           "cell_stage_per_s": {k: sc.n_elems * 3 * it / (v / 1e3) for k, v in dev_ms.items()},
+           "wall_s_including_comparisons": wall, "trajectory": rows}
+    for g in solvers.values():
+        g.close()
+    print(json.dumps(out))
+    return 0
+
+
 def run_parts(args, rank, world, local) -> int:
     """`--parts P`: the meander (or dam break) as P linked parts of one handle on this
     GPU (storm_b200/partition.py) against the undivided mesh, K timed iterations of
@@ -527,6 +598,13 @@ def main():
     ap.add_argument("--kt-steps", type=int, default=5, help="iterations of the per-kernel timing pass")
     ap.add_argument("--parts", type=int, default=1,
                     help="run the mesh as this many linked parts on one GPU (domain decomposition)")
+    ap.add_argument("--stage-path", choices=["fused", "phases"], default="fused",
+                    help="stage kernels of the timed runs: the fused tile kernel (default) or the phase kernels")
+    ap.add_argument("--ab-steps", type=int, default=200,
+                    help="iterations of the other stage path, timed in the same run (0: skip)")
+    ap.add_argument("--trajectory", action="store_true",
+                    help="--config dambreak: run 60 s simulated in FP64 and mixed, compare every iteration")
+    ap.add_argument("--traj-every", type=int, default=1, help="iterations between full-state comparisons")
     ap.add_argument("--dist-check", action="store_true",
                     help="bring up --gpus ranks on gloo and report them (no GPU work)")
     args = ap.parse_args()
@@ -587,6 +665,10 @@ def main():
         if rank != 0:
             return 0
         return run_parts(args, rank, world, local)
+    if args.trajectory:
+        if rank != 0:
+            return 0
+        return run_dambreak_trajectory(args, local)
 
     import torch
     dist = None
@@ -606,6 +688,9 @@ def main():
     K_rk = sc.options.rkorder
     t0 = time.perf_counter()
     solver = fvt.Solver(pm, sc.options, keep=pm)
+    if args.stage_path == "phases":
+        solver.set_stage_path(fvt.STAGE_PHASES)
+    path_used = "fused" if solver.stage_path() == fvt.STAGE_FUSED else "phases"
     setup = {"mesh_build_s": mesh_ratios.build_s, "create_s": time.perf_counter() - t0,
              "what": "storm_fvt_mesh_build (topology, edges, walls, boundary arrays, LSQ and IDW set-up: "
                      "read_data + dataprepFVT, host C++) and storm_fvt_create (layout, upload, graph capture)"}
@@ -684,6 +769,30 @@ def main():
         }
         s2.close()
 
+    # ---- the other stage path on the same mesh: speed and bitwise agreement ----
+    ab = None
+    if args.ab_steps > 0:
+        n_ab = max(1, min(args.steps, args.ab_steps))
+        other_path = fvt.STAGE_PHASES if path_used == "fused" else fvt.STAGE_FUSED
+        s3 = fvt.Solver(pm, sc.options, keep=pm)
+        s3.set_stage_path(other_path)
+        if s3.stage_path() == other_path:
+            finals = []
+            for sv in (solver, s3):
+                sv.set_state(sc.h0, sc.u0, sc.v0)
+                sv.step(args.warmup)
+                barrier()
+                sv.step(n_ab)
+                barrier()
+                finals.append((sv.last_timing()["step_ms"], sv.state()))
+            same = all(np.array_equal(finals[0][1][k].view(np.uint64), finals[1][1][k].view(np.uint64))
+                       for k in ("h", "u", "v", "rku", "rkv", "hvtx"))
+            ab = {"stage_kernels": "phases" if path_used == "fused" else "fused", "steps": n_ab,
+                  "ms_per_step": finals[1][0] / n_ab, "this_path_ms_per_step": finals[0][0] / n_ab,
+                  "value": T * K_rk * n_ab / (finals[1][0] / 1e3),
+                  "bitwise_equal_states": bool(same)}
+        s3.close()
+
     # ---- per-kernel timing pass (roofline of the RK-stage kernel chain) ----
     solver.set_state(sc.h0, sc.u0, sc.v0)
     solver.set_kernel_timing(True)
@@ -691,7 +800,7 @@ def main():
     solver.step(kt_steps)
     kt = solver.kernel_times()
     solver.set_kernel_timing(False)
-    stage_ms = sum(kt[k][0] for k in ("node", "grad", "bc", "eflux", "flux"))
+    stage_ms = sum(kt[k][0] for k in ("node", "grad", "bc", "eflux", "flux", "tile"))
     B = scenarios.algorithmic_bytes_per_cell_stage(T, E, N)
     pk = peaks()
     # The launch unit is one graph replay = one iteration (K stages of every kernel,
@@ -703,18 +812,21 @@ def main():
     achieved_serial = B * T * K_rk * kt_steps / (stage_ms / 1e3) / 1e9
     iter_ms = sum(v[0] for v in kt.values())
     traffic = None
-    if args.config in NCU_DRAM_BYTES_PER_CELL_STAGE:
-        traffic = NCU_DRAM_BYTES_PER_CELL_STAGE[args.config] * T * K_rk
+    if (args.config, path_used) in NCU_DRAM_BYTES_PER_CELL_STAGE:
+        traffic = NCU_DRAM_BYTES_PER_CELL_STAGE[(args.config, path_used)] * T * K_rk
+    chain = ("K x [k_node, k_grad(boundary cells) -> k_bc || k_tile, k_flux_bc]" if path_used == "fused"
+             else "K x [k_node, k_grad, k_bc || k_eflux, k_flux, k_flux_bc]")
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
         "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
-        "kernel": "one iteration (CUDA graph: K x [k_node, k_grad, k_bc || k_eflux, k_flux], k_fric, k_final)",
+        "kernel": f"one iteration (CUDA graph: {chain}, k_fric, k_final)",
         "algorithmic_bytes_per_launch": B * T * K_rk, "bytes_per_cell_stage": B, "peak_source": pk["source"],
         "traffic_source": "ncu dram__bytes_read+write of the stage kernels on the 500k-cell meander, "
                           "per cell-stage, scaled to this mesh" if traffic else None,
         "achieved_serialised_stage_chain": achieved_serial,
         "kernel_ms_share": {k: round(v[0] / iter_ms, 4) for k, v in kt.items()},
-        "flux_kernel_avg_ms": kt["flux"][0] / max(1, kt["flux"][1]),
+        "stage_kernel_avg_ms": (kt["tile"][0] / max(1, kt["tile"][1]) if path_used == "fused"
+                                else kt["flux"][0] / max(1, kt["flux"][1])),
     }
 
     metric = METRIC if args.config == "meander" else f"cell-stage updates/s (FVT time step, {args.config})"
@@ -727,6 +839,7 @@ def main():
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "gpu_launches": gpu_launches,
+        "stage_kernels": path_used,
         "setup": setup,
         "roofline": roofline,
         "clocks": clk.summary(),
@@ -734,6 +847,8 @@ def main():
     }
     if other is not None:
         out["other_precision"] = other
+    if ab is not None:
+        out["other_stage_kernels"] = ab
     if rank == 0 and world == 1 and args.warm_eval > 0 and args.config == "meander":
         out["time_to_steady"] = warm_start_eval(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -339,7 +339,8 @@ STORM_FVT_API int storm_fvt_last_timing(const StormFvtHandle* hd, double* step_m
  * kernel timing mode, indexed 0 node (vertex depth), 1 grad (gradients/limiter),
  * 2 bc (open boundaries), 3 flux (per-cell gather of the face fluxes + sources + RK
  * update), 4 fric (friction and reduction partials), 5 final (iteration scalars),
- * 6 eflux (interior-edge fluxes); 7 is zero. */
+ * 6 eflux (interior-edge fluxes), 7 tile (the fused stage kernel).  On the fused path
+ * 1 and 3 time the boundary cells' gradient and update kernels only. */
 STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, int64_t* launches);
 
 /* Project autotuner: times `iters` iterations per candidate block size of the node,
@@ -347,6 +348,30 @@ STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, i
  * events), keeps the fastest of each, re-captures the iteration graph and restores
  * the state it started from.  `chosen` (may be NULL) receives the four sizes. */
 STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t* chosen);
+
+/* Stage kernels of the captured iteration.  No counterpart in the reference (it
+ * selects how this library schedules the same arithmetic; results are bitwise the
+ * same either way):
+ *   STORM_STAGE_PHASES  k_node, k_grad, k_eflux, k_flux per stage (gradients and edge
+ *                       fluxes pass through device memory between the kernels);
+ *   STORM_STAGE_FUSED   k_node, then one fused kernel per stage over Morton tiles of
+ *                       256 cells (gradients, edge fluxes and the RK update of a tile
+ *                       in shared memory), the default wherever it applies.
+ * The fused path does not apply to culverts, residual smoothing or linked partitions
+ * (those run the phase kernels whatever is set), nor to a mesh whose tiles do not fit
+ * in shared memory.  Setting re-captures the iteration graph. */
+enum { STORM_STAGE_PHASES = 0, STORM_STAGE_FUSED = 1 };
+STORM_FVT_API int storm_fvt_set_stage_path(StormFvtHandle* hd, int32_t path);
+/* The path the captured iteration runs (STORM_STAGE_PHASES or STORM_STAGE_FUSED). */
+STORM_FVT_API int32_t storm_fvt_stage_path(const StormFvtHandle* hd);
+
+/* Host-only check of the fused kernel's tile plan for a batch of prepared meshes
+ * (no device needed; no counterpart in the reference).  stats[8] receives: tiles,
+ * largest local cell count, largest gradient count, largest edge count, H1 cells,
+ * H2 cells, back edges, and 0 if every local index maps back to the cell or edge the
+ * layout names (else the number of the first failed check). */
+STORM_FVT_API int storm_fvt_tile_check(const StormFvtMesh* const* meshes, int32_t n, int32_t tile_cells,
+                                       int64_t* stats);
 
 /*
  * Partitions of one mesh (domain decomposition, single-device form):

@@ -13,7 +13,7 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libstorm_fvt.so")
-SOURCES = ["api.cu", "fvt_kernels.cu", "layout.cpp", "mesh_build.cpp", "noalloc.cu", "gnn_kernels.cu"]
+SOURCES = ["api.cu", "fvt_kernels.cu", "layout.cpp", "tiles.cpp", "mesh_build.cpp", "noalloc.cu", "gnn_kernels.cu"]
 HEADERS = ["fvt_device.cuh", "storm_internal.h", "umma.cuh", os.path.join("..", "..", "include", "storm_fvt.h"),
            os.path.join("..", "..", "include", "storm_gnn.h")]
 

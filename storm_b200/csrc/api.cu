@@ -78,6 +78,15 @@ struct StormFvtHandle {
   void* halo_buf = nullptr;  // linked partitions: halo slots, owner slots, halo mask
   double* io_host = nullptr;  // pinned staging of state transfers (grown on demand)
   size_t io_n = 0;
+  // fused stage kernel: tile plan, its device copy, the second velocity buffer
+  TilePlan tiles;
+  TileDev td{};
+  void* tile_buf = nullptr;
+  size_t tile_smem = 0;
+  bool tiles_ok = false;    // plan built and within the shared-memory limit
+  bool want_tiles = true;   // storm_fvt_set_stage_path
+  bool use_tiles = false;   // the captured iteration runs k_tile
+  double *u_a2 = nullptr, *v_a2 = nullptr;
 };
 
 namespace {
@@ -132,7 +141,11 @@ T* at(void* base, size_t off) {
 }
 
 // Kernel classes of the per-kernel timing mode.
-enum { KT_NODE = 0, KT_GRAD, KT_BC, KT_FLUX, KT_FRIC, KT_FINAL, KT_EFLUX, KT_COUNT };
+enum { KT_NODE = 0, KT_GRAD, KT_BC, KT_FLUX, KT_FRIC, KT_FINAL, KT_EFLUX, KT_TILE, KT_COUNT };
+static_assert(KT_COUNT <= 8, "per-class timing arrays hold 8 classes");
+
+constexpr int kTileCellsHost = 256;   // k_tile's tile (kTileCells in fvt_kernels.cu)
+constexpr int kTileThreadsHost = 256;
 
 int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
   const Dev& d = h->d;
@@ -154,6 +167,14 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     CK(cudaEventRecord(h->fev[(*fev_used)++], h->stream));
     return 0;
   };
+  const bool linked = d.linked != 0;
+  const bool rs = h->opt.rsavg_passes > 0;
+  // the fused tile kernel where its plan exists; the phase kernels for culverts,
+  // residual smoothing and linked partitions
+  const bool fused = h->tiles_ok && h->want_tiles && !linked && d.ncv == 0 && !rs;
+  h->use_tiles = fused;
+  const double *u_in = d.u_a, *v_in = d.v_a;
+  double *u_out = d.u_a, *v_out = d.v_a;
   auto launch = [&](int which, int grid, int block, size_t smem, cudaStream_t st, int s, const double* hs,
                     uint8_t* dry, uint8_t* dry_next) {
     StageLaunch L;
@@ -168,22 +189,67 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     L.dry_next = dry_next;
     L.rku_prev = d.rku + (size_t)(s - 1) * T;
     L.rkv_prev = d.rkv + (size_t)(s - 1) * T;
+    L.u_in = u_in;
+    L.v_in = v_in;
+    L.u_out = u_out;
+    L.v_out = v_out;
+    L.tiles = &h->td;
     launch_stage(L, d, h->gd, h->gf, h->mixed);
   };
-  const bool linked = d.linked != 0;
   if (linked && !d.steady && d.dt_op != 0) launch_link_dt(d, h->stream);
   for (int s = 1; s <= K; s++) {
     const double* hs = d.rkh + (size_t)(s - 1) * T;
     uint8_t* dry = (s & 1) ? d.dry_a : d.dry_b;
     uint8_t* dry_next = (s & 1) ? d.dry_b : d.dry_a;
     const int gB = (d.nbc_cells + kFluxThreads - 1) / kFluxThreads;
+    if (fused) {  // stage s reads one velocity buffer and writes the other
+      u_in = (s & 1) ? d.u_a : h->u_a2;
+      v_in = (s & 1) ? d.v_a : h->v_a2;
+      u_out = (s & 1) ? h->u_a2 : d.u_a;
+      v_out = (s & 1) ? h->v_a2 : d.v_a;
+    }
     if (mark(KT_NODE)) return STORM_ERR_CUDA;
     k_node<<<gN, h->bs_node, 0, h->stream>>>(d, hs, dry);
-    if (done() || mark(KT_GRAD)) return STORM_ERR_CUDA;
+    if (done()) return STORM_ERR_CUDA;
+    if (fused) {
+      const int nt = h->td.ntiles;
+      if (gB > 0 && !timing) {
+        // the boundary cells' gradients and k_bc on the side stream beside k_tile;
+        // k_flux_bc updates those cells once both are done
+        CK(cudaEventRecord(h->fork_ev[s], h->stream));
+        CK(cudaStreamWaitEvent(h->side, h->fork_ev[s], 0));
+        launch(STAGE_GRAD_BC, gB, kFluxThreads, 0, h->side, s, hs, dry, dry_next);
+        if (d.nbdr > 0) launch(STAGE_BC, d.nbdr, 128, h->bc_smem, h->side, s, hs, dry, dry_next);
+        CK(cudaEventRecord(h->join_ev[s], h->side));
+        launch(STAGE_TILE, nt, kTileThreadsHost, h->tile_smem, h->stream, s, hs, dry, dry_next);
+        CK(cudaStreamWaitEvent(h->stream, h->join_ev[s], 0));
+        launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+      } else {
+        if (gB > 0) {
+          if (mark(KT_GRAD)) return STORM_ERR_CUDA;
+          launch(STAGE_GRAD_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+          if (done()) return STORM_ERR_CUDA;
+          if (d.nbdr > 0) {
+            if (mark(KT_BC)) return STORM_ERR_CUDA;
+            launch(STAGE_BC, d.nbdr, 128, h->bc_smem, h->stream, s, hs, dry, dry_next);
+            if (done()) return STORM_ERR_CUDA;
+          }
+        }
+        if (mark(KT_TILE)) return STORM_ERR_CUDA;
+        launch(STAGE_TILE, nt, kTileThreadsHost, h->tile_smem, h->stream, s, hs, dry, dry_next);
+        if (done()) return STORM_ERR_CUDA;
+        if (gB > 0) {
+          if (mark(KT_FLUX)) return STORM_ERR_CUDA;
+          launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
+          if (done()) return STORM_ERR_CUDA;
+        }
+      }
+      continue;
+    }
+    if (mark(KT_GRAD)) return STORM_ERR_CUDA;
     launch(STAGE_GRAD, gT, h->bs_grad, 0, h->stream, s, hs, dry, dry_next);
     if (d.ncv > 0) launch(STAGE_CULVERT, (d.ncv + 127) / 128, 128, 0, h->stream, s, hs, dry, dry_next);
     if (done()) return STORM_ERR_CUDA;
-    const bool rs = h->opt.rsavg_passes > 0;
     const int sF = rs ? STAGE_PHI : STAGE_FLUX, sFB = rs ? STAGE_PHI_BC : STAGE_FLUX_BC;
     if (d.nbdr > 0 && !timing) {
       // k_bc on the side stream overlaps k_eflux and k_flux of the cells without
@@ -226,7 +292,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
   }
   if (linked && d.steady) launch_link_fric(d, h->stream);
   if (mark(KT_FRIC)) return STORM_ERR_CUDA;
-  launch_fric(d, h->stream);
+  launch_fric(d, u_out, v_out, h->stream);
   if (done()) return STORM_ERR_CUDA;
   if (d.nhalo > 0) launch_halo(d, 0, d.dry_a, d.dry_out, h->stream);
   if (mark(KT_FINAL)) return STORM_ERR_CUDA;
@@ -275,8 +341,64 @@ void release(StormFvtHandle* h) {
   if (h->sc_host) cudaFreeHost(h->sc_host);
   if (h->out_buf) cudaFree(h->out_buf);
   if (h->halo_buf) cudaFree(h->halo_buf);
+  if (h->tile_buf) cudaFree(h->tile_buf);
   if (h->io_host) cudaFreeHost(h->io_host);
   delete h;
+}
+
+// The tile plan of the fused stage kernel and its device copy.  A mesh whose tiles do
+// not fit (more than 65,534 local cells or edges, or more shared memory than a block
+// may have) keeps the phase kernels.
+int upload_tiles(StormFvtHandle* h) {
+  h->tiles_ok = false;
+  TilePlan& P = h->tiles;
+  if (build_tiles(h->L, kTileCellsHost, P) != 0 || check_tiles(h->L, P) != 0) {
+    P = TilePlan();
+    return 0;
+  }
+  TileDev& t = h->td;
+  t.tc = P.tc; t.ntiles = P.ntiles; t.kst = P.kst;
+  t.ns_max = P.ns_max; t.ng_max = P.ng_max; t.ne_max = P.ne_max;
+  const size_t smem = tile_smem_bytes(t, h->mixed);
+  int dev_max = 0;
+  CK(cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+  if (smem > (size_t)dev_max) {
+    P = TilePlan();
+    return 0;
+  }
+  Arena A;
+  struct Up {
+    size_t off;
+    const void* src;
+    size_t bytes;
+  };
+  std::vector<Up> ups;
+  auto cpy = [&](const auto& vec) {
+    using V = typename std::decay<decltype(vec)>::type::value_type;
+    size_t o = A.take(sizeof(V) * std::max<size_t>(vec.size(), 1));
+    if (!vec.empty()) ups.push_back({o, vec.data(), sizeof(V) * vec.size()});
+    return o;
+  };
+  const size_t o_info = cpy(P.info), o_halo = cpy(P.halo), o_h1t3 = cpy(P.h1_t3), o_h1st = cpy(P.h1_st);
+  const size_t o_lt3 = cpy(P.lt3), o_lst = cpy(P.lst), o_lfe = cpy(P.lfe), o_eloc = cpy(P.eloc);
+  const size_t o_be = cpy(P.be), o_beloc = cpy(P.beloc);
+  cudaError_t e = cudaMalloc(&h->tile_buf, A.off);
+  if (e != cudaSuccess)
+    return set_error(e == cudaErrorMemoryAllocation ? STORM_ERR_NOMEM : STORM_ERR_CUDA,
+                     std::string("device allocation of the tile plan: ") + cudaGetErrorString(e));
+  for (const Up& u : ups) CK(cudaMemcpy(static_cast<char*>(h->tile_buf) + u.off, u.src, u.bytes, cudaMemcpyHostToDevice));
+  void* B = h->tile_buf;
+  t.info = at<int32_t>(B, o_info); t.halo = at<int32_t>(B, o_halo);
+  t.h1_t3 = at<uint16_t>(B, o_h1t3); t.h1_st = at<uint16_t>(B, o_h1st);
+  t.lt3 = at<uint16_t>(B, o_lt3); t.lst = at<uint16_t>(B, o_lst); t.lfe = at<uint16_t>(B, o_lfe);
+  t.eloc = at<uint32_t>(B, o_eloc); t.be = at<int32_t>(B, o_be); t.beloc = at<uint32_t>(B, o_beloc);
+  h->tile_smem = smem;
+  if (smem > 48 * 1024) set_tile_smem_limit((int)smem);
+  CK(cudaGetLastError());
+  // the host copy of the plan is not needed after the upload
+  P.halo = {}; P.h1_t3 = {}; P.h1_st = {}; P.lt3 = {}; P.lst = {}; P.lfe = {}; P.eloc = {}; P.be = {}; P.beloc = {};
+  h->tiles_ok = true;
+  return 0;
 }
 
 int upload(StormFvtHandle* h) {
@@ -332,13 +454,27 @@ int upload(StormFvtHandle* h) {
   size_t o_rsc = cpy(L.rs_cells, std::max<size_t>(L.rs_cells.size(), 1));
   size_t o_phi = A.take(rsavg ? 8 * 3 * (size_t)T : 8), o_phi0 = A.take(rsavg ? 8 * 3 * (size_t)T : 8);
   const size_t ne1 = std::max(L.ne, 1);
-  size_t o_eL = cpy(L.eL, ne1), o_eR = cpy(L.eR, ne1), o_es = cpy(L.eslot, ne1);
+  // edges with a cell that has an open-boundary face: the fused kernel hands their
+  // fluxes to k_flux_bc through the edge-flux arrays
+  std::vector<uint8_t> eslot = L.eslot;
+  for (int32_t e = 0; e < L.ne; e++)
+    if ((L.forder[L.eL[e]] & kOrderHasBc) || (L.forder[L.eR[e]] & kOrderHasBc)) eslot[e] |= kEdgeExport;
+  // vertex minus centroid of each cell vertex (the differences bed_slope_STD forms)
+  std::vector<double> vox(T3), voy(T3);
+  for (size_t q = 0; q < T3; q++) {
+    const int32_t c = (int32_t)(q % (size_t)T), v = L.vert[q];
+    vox[q] = L.node_x[v] - L.xc[c];
+    voy[q] = L.node_y[v] - L.yc[c];
+  }
+  size_t o_vox = cpy(vox, T3), o_voy = cpy(voy, T3);
+  size_t o_eL = cpy(L.eL, ne1), o_eR = cpy(L.eR, ne1), o_es = cpy(eslot, ne1);
   size_t o_enx = cpy(L.enx, ne1), o_eny = cpy(L.eny, ne1), o_el = cpy(L.elen, ne1), o_ez0 = cpy(L.ez0, ne1);
   // state
   const size_t TL = (size_t)(K + 1) * T;
   size_t o_rkh = A.take(8 * TL), o_rku = A.take(8 * TL), o_rkv = A.take(8 * TL);
   size_t o_ua = A.take(8 * (size_t)T), o_va = A.take(8 * (size_t)T), o_ub = A.take(8 * (size_t)T),
          o_vb = A.take(8 * (size_t)T);
+  size_t o_ua2 = A.take(8 * (size_t)T), o_va2 = A.take(8 * (size_t)T);
   size_t o_g[6];
   for (int i = 0; i < 6; i++) o_g[i] = A.take(8 * (size_t)T);
   size_t o_dra = A.take(T), o_drb = A.take(T), o_hv = A.take(8 * (size_t)N), o_vw = A.take(N);
@@ -405,6 +541,8 @@ int upload(StormFvtHandle* h) {
   d.nscen = h->nscen;
   d.rkh = at<double>(B, o_rkh); d.rku = at<double>(B, o_rku); d.rkv = at<double>(B, o_rkv);
   d.u_a = at<double>(B, o_ua); d.v_a = at<double>(B, o_va); d.u_b = at<double>(B, o_ub); d.v_b = at<double>(B, o_vb);
+  h->u_a2 = at<double>(B, o_ua2); h->v_a2 = at<double>(B, o_va2);
+  d.vox = at<double>(B, o_vox); d.voy = at<double>(B, o_voy);
   d.delh_x = at<double>(B, o_g[0]); d.delh_y = at<double>(B, o_g[1]); d.delu_x = at<double>(B, o_g[2]);
   d.delu_y = at<double>(B, o_g[3]); d.delv_x = at<double>(B, o_g[4]); d.delv_y = at<double>(B, o_g[5]);
   d.dry_a = at<uint8_t>(B, o_dra); d.dry_b = at<uint8_t>(B, o_drb); d.hvtx = at<double>(B, o_hv);
@@ -502,6 +640,8 @@ int upload(StormFvtHandle* h) {
     x.blk_cnt = I.blk_cnt;
   }
   CK(cudaMemcpy(d.sc, s0.data(), sizeof(Scalars) * s0.size(), cudaMemcpyHostToDevice));
+  int rct = upload_tiles(h);
+  if (rct) return rct;
   int maxcnt = 1;
   for (int b = 0; b < L.nbdr; b++) maxcnt = std::max(maxcnt, L.bdr_cnt[b]);
   h->bc_smem = (size_t)maxcnt * 2 * sizeof(double) + (((size_t)maxcnt + 7) & ~(size_t)7);
@@ -1085,6 +1225,62 @@ int storm_fvt_autotune(StormFvtHandle* h, int32_t iters, int32_t* chosen) {
   h->exec = nullptr;
   h->graph = nullptr;
   return capture_graph(h);
+}
+
+int storm_fvt_set_stage_path(StormFvtHandle* h, int32_t path) {
+  clear_error();
+  if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_set_stage_path: null handle");
+  if (path != STORM_STAGE_PHASES && path != STORM_STAGE_FUSED)
+    return set_error(STORM_ERR_ARG, "storm_fvt_set_stage_path: path must be STORM_STAGE_PHASES or STORM_STAGE_FUSED");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  h->want_tiles = path == STORM_STAGE_FUSED;
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->exec = nullptr;
+  h->graph = nullptr;
+  return capture_graph(h);
+}
+
+int32_t storm_fvt_stage_path(const StormFvtHandle* h) {
+  return (h && h->use_tiles) ? STORM_STAGE_FUSED : STORM_STAGE_PHASES;
+}
+
+int storm_fvt_tile_check(const StormFvtMesh* const* meshes, int32_t n, int32_t tile_cells, int64_t* stats) {
+  clear_error();
+  if (!meshes || n < 1 || !stats || tile_cells < 32 || tile_cells > 4096)
+    return set_error(STORM_ERR_ARG, "storm_fvt_tile_check: bad argument");
+  StormFvtOptions o;
+  storm_fvt_default_options(&o);
+  std::vector<HostLayout> parts(n);
+  std::vector<ScenarioInfo> info;
+  HostLayout L;
+  TilePlan P;
+  try {
+    for (int32_t i = 0; i < n; i++) {
+      if (!meshes[i]) return set_error(STORM_ERR_ARG, "storm_fvt_tile_check: null mesh");
+      int rc = build_layout(*meshes[i], o, parts[i]);
+      if (rc) return rc;
+    }
+    merge_layouts(parts, kRed, L, info);
+    if (build_tiles(L, tile_cells, P) != 0) return set_error(STORM_ERR_UNSUPPORTED, "storm_fvt_tile_check: tile too large");
+  } catch (const std::bad_alloc&) {
+    return set_error(STORM_ERR_NOMEM, "storm_fvt_tile_check: host out of memory");
+  }
+  int64_t s1 = 0, s2 = 0;
+  for (int32_t t = 0; t < P.ntiles; t++) {
+    s1 += P.info[(size_t)t * TI_N + TI_N1];
+    s2 += P.info[(size_t)t * TI_N + TI_N2];
+  }
+  stats[0] = P.ntiles;
+  stats[1] = P.ns_max;
+  stats[2] = P.ng_max;
+  stats[3] = P.ne_max;
+  stats[4] = s1;
+  stats[5] = s2;
+  stats[6] = (int64_t)P.be.size();
+  stats[7] = check_tiles(L, P);
+  return 0;
 }
 
 int storm_fvt_link_partitions(StormFvtHandle* h, int32_t n_halo, const int32_t* dst_scen, const int32_t* dst_elem,

@@ -51,6 +51,7 @@ struct Dev {
   double alpha[4][4], beta[4];
   // cells
   const double *area, *perim, *xc, *yc, *z, *delz_x, *delz_y, *zmax, *cd;
+  const double *vox, *voy;  // [3][T] vertex minus centroid of each cell vertex (bed_slope_STD)
   const double *wcoef1, *wcoef2;  // wind stress terms per cell (null: no wind)
   // linked partitions of one mesh: halo cell slots and their owners' slots, the halo
   // mask (null: no halo), the scenario holding element n_elems of the whole mesh
@@ -116,9 +117,21 @@ struct Geo {
   R* efx;  // [3][ne]
 };
 
+// Device view of the tile plan of the fused stage kernel (TilePlan in storm_internal.h).
+struct TileDev {
+  int32_t tc, ntiles, kst, ns_max, ng_max, ne_max;
+  const int32_t* info;                 // [ntiles][TI_N]
+  const int32_t* halo;                 // H1 then H2 slots per tile
+  const uint16_t *h1_t3, *h1_st;       // local topology of the H1 cells
+  const uint16_t *lt3, *lst, *lfe;     // local topology of every cell in its own tile
+  const uint32_t* eloc;                // [ne] local L | R << 16 (range edges)
+  const int32_t* be;                   // back edges
+  const uint32_t* beloc;               // their local L | R << 16
+};
+
 // One launch of a templated stage kernel (see launch_stage in fvt_kernels.cu).
 enum StageKernel { STAGE_GRAD, STAGE_BC, STAGE_EFLUX, STAGE_FLUX, STAGE_FLUX_BC, STAGE_PHI, STAGE_PHI_BC,
-                   STAGE_UPDATE, STAGE_CULVERT };
+                   STAGE_UPDATE, STAGE_CULVERT, STAGE_GRAD_BC, STAGE_TILE };
 struct StageLaunch {
   int which;
   dim3 grid, block;
@@ -129,7 +142,14 @@ struct StageLaunch {
   const uint8_t* dry;
   uint8_t* dry_next;
   double *rku_prev, *rkv_prev;
+  // stage-input velocities and where the stage writes its new ones (the same arrays
+  // for the phase kernels; ping-pong buffers for the fused tile kernel)
+  const double *u_in, *v_in;
+  double *u_out, *v_out;
+  const TileDev* tiles;  // STAGE_TILE only
 };
+size_t tile_smem_bytes(const TileDev& t, bool mixed);
+void set_tile_smem_limit(int bytes);
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed);
 void set_bc_smem_limit(int bytes);
 // Linked partitions: halo exchange of one level (+ up to two flag arrays), the shared
@@ -139,7 +159,7 @@ void launch_link_fric(const Dev& d, cudaStream_t st);
 void launch_link(const Dev& d, cudaStream_t st);
 void launch_link_dt(const Dev& d, cudaStream_t st);
 // Friction, hvalve and the iteration partials (halo cells left out when linked).
-void launch_fric(const Dev& d, cudaStream_t st);
+void launch_fric(const Dev& d, const double* u_src, const double* v_src, cudaStream_t st);
 void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st);
 
 // The output pass (to_vertices, ctr2vtx of cd, error_est(2)) after an iteration.

@@ -299,6 +299,48 @@ __device__ __forceinline__ double block_min(double x, double* sm) {
   return r;
 }
 
+// The five iteration reductions in one pass: sums of st, sb, tm, the max of rm and the
+// min of dt, each by the same xor-shuffle tree and the same serial warp order as
+// block_sum / block_max / block_min (so the same bits), with one barrier.
+template <int NT>
+__device__ __forceinline__ void block_reduce5(double st, double sb, double tm, double rm, double dt, double* sm,
+                                              double* out) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    st = st + __shfl_xor_sync(0xffffffffu, st, o);
+    sb = sb + __shfl_xor_sync(0xffffffffu, sb, o);
+    tm = tm + __shfl_xor_sync(0xffffffffu, tm, o);
+    rm = fmax2(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+    dt = fmin2(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  constexpr int NW = NT / 32;
+  __syncthreads();
+  if (l == 0) {
+    sm[w] = st;
+    sm[NW + w] = sb;
+    sm[2 * NW + w] = tm;
+    sm[3 * NW + w] = rm;
+    sm[4 * NW + w] = dt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = sm[0], b = sm[NW], c = sm[2 * NW], m = sm[3 * NW], n = sm[4 * NW];
+    for (int i = 1; i < NW; i++) {
+      a = a + sm[i];
+      b = b + sm[NW + i];
+      c = c + sm[2 * NW + i];
+      m = fmax2(m, sm[3 * NW + i]);
+      n = fmin2(n, sm[4 * NW + i]);
+    }
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+    out[3] = m;
+    out[4] = n;
+  }
+}
+
 // get_time_bcs.f90:31-77 for scenario `sid` (one thread)
 __device__ void time_bcs(const Dev& d, int sid, double time) {
   Scalars* sc = &d.sc[sid];
@@ -464,26 +506,54 @@ __device__ __forceinline__ float limited_r(double q0, double qn, float g_x, floa
   return (fabsf(num) >= fabsf(delq)) ? 1.0f : qdiv(num, delq);
 }
 
+// Neighbour values of the gradient and flux arithmetic: read from global memory by
+// slot (the phase kernels) or from a tile's shared-memory copy by local id (k_tile).
+struct NbGlobal {
+  const double* __restrict__ hs;
+  const double* __restrict__ z;
+  const double* __restrict__ u;
+  const double* __restrict__ v;
+  const uint8_t* __restrict__ dry;
+  __device__ __forceinline__ double H(int i) const { return hs[i]; }
+  __device__ __forceinline__ double Z(int i) const { return z[i]; }
+  __device__ __forceinline__ double U(int i) const { return u[i]; }
+  __device__ __forceinline__ double V(int i) const { return v[i]; }
+  __device__ __forceinline__ bool D(int i) const { return dry[i] != 0; }
+};
+struct NbShared {
+  const double *h, *z, *u, *v;
+  const uint8_t* dry;
+  __device__ __forceinline__ double H(int i) const { return h[i]; }
+  __device__ __forceinline__ double Z(int i) const { return z[i]; }
+  __device__ __forceinline__ double U(int i) const { return u[i]; }
+  __device__ __forceinline__ double V(int i) const { return v[i]; }
+  __device__ __forceinline__ bool D(int i) const { return dry[i] != 0; }
+};
+
+// Limited LSQ gradients of one cell, with hgradfix2 and the partially-wet velocity
+// zeroing (lsq_grad_array.f90:60-73, limiterBJ.f90:42-81 with beta = one,
+// cell_grads.f90:72-75, hgradfix2.f90:48-98, to_vertices.f90:44-55).  `c` is the cell
+// slot (geometry), `self` its index in `nb`, t3 its face neighbours in `nb` (-1: none)
+// and st(k) its k-th stencil neighbour in `nb`.  Differences of the FP64 fields are
+// taken in double and then rounded to R.  With the BJ limiter the three rc offsets
+// are read here and returned in rcx/rcy (when given).
 template <class R>
-__global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* __restrict__ hs,
-                                              const uint8_t* __restrict__ dry, double* __restrict__ rku_prev,
-                                              double* __restrict__ rkv_prev) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.T) return;
-  const int sid = d.cell_sid[c];
-  if (sid < 0 || d.sc[sid].converged) return;
+struct GradOut {
+  R hx, hy, ux, uy, vx, vy;
+  double ub, vb;
+  bool fix;  // hgradfix2 set the gradient: the previous RK level's momentum is zeroed
+};
+
+template <class R, class NB, class ST>
+__device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>& G, const NB& nb, int c, int self,
+                                                     const int (&t3)[3], ST st, R* rcx, R* rcy) {
   const int T = d.T;
-  const double zeta_c = hs[c] + d.z[c];
-  const double u_c = d.u_a[c], v_c = d.v_a[c];
-  // face neighbours and vertices first: their loads (and the flags read through them
-  // below) are in flight while the stencil is gathered
-  int t3[3], vt[3];
+  const double zeta_c = nb.H(self) + nb.Z(self);
+  const double u_c = nb.U(self), v_c = nb.V(self);
+  int vt[3];
 #pragma unroll
-  for (int j = 0; j < 3; j++) {
-    t3[j] = d.t2t3[(size_t)j * T + c];
-    vt[j] = d.vert[(size_t)j * T + c];
-  }
-  const bool dry_c = dry[c];
+  for (int j = 0; j < 3; j++) vt[j] = d.vert[(size_t)j * T + c];
+  const bool dry_c = nb.D(self);
   R hx = R(0), hy = R(0), ux = R(0), uy = R(0), vx = R(0), vy = R(0);
   if (d.lim == 1 || d.lim == 2) {
     R dz = R(0), ez = R(0), du = R(0), eu = R(0), dv = R(0), ev = R(0);
@@ -495,16 +565,16 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
 #pragma unroll
       for (int k = 0; k < 3; k++) {
         const size_t q = (size_t)k * T + c;
-        jj[k] = d.st_id[q];
+        jj[k] = st(k);
         w[k] = G.st_w[q];
         dx[k] = G.st_dx[q];
         dy[k] = G.st_dy[q];
       }
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        pz[k] = (R)((hs[jj[k]] + d.z[jj[k]]) - zeta_c);
-        pu[k] = (R)(d.u_a[jj[k]] - u_c);
-        pv[k] = (R)(d.v_a[jj[k]] - v_c);
+        pz[k] = (R)((nb.H(jj[k]) + nb.Z(jj[k])) - zeta_c);
+        pu[k] = (R)(nb.U(jj[k]) - u_c);
+        pv[k] = (R)(nb.V(jj[k]) - v_c);
       }
 #pragma unroll
       for (int k = 0; k < 3; k++) {
@@ -519,11 +589,11 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
     }
     for (int k = k0; k < n; k++) {
       const size_t q = (size_t)k * T + c;
-      const int j = d.st_id[q];
+      const int j = st(k);
       const R w = G.st_w[q], dx = G.st_dx[q], dy = G.st_dy[q];
-      const R pz = (R)((hs[j] + d.z[j]) - zeta_c);
-      const R pu = (R)(d.u_a[j] - u_c);
-      const R pv = (R)(d.v_a[j] - v_c);
+      const R pz = (R)((nb.H(j) + nb.Z(j)) - zeta_c);
+      const R pu = (R)(nb.U(j) - u_c);
+      const R pv = (R)(nb.V(j) - v_c);
       dz = dz + w * pz * dx;
       ez = ez + w * pz * dy;
       du = du + w * pu * dx;
@@ -546,9 +616,13 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
       const size_t q = (size_t)j * T + c;
       const int k = t3[j];
       const R rx = G.rc_x[q], ry = G.rc_y[q];
-      const double qz = k < 0 ? zeta_c : hs[k] + d.z[k];
-      const double qu = k < 0 ? u_c : d.u_a[k];
-      const double qv = k < 0 ? v_c : d.v_a[k];
+      if (rcx) {
+        rcx[j] = rx;
+        rcy[j] = ry;
+      }
+      const double qz = k < 0 ? zeta_c : nb.H(k) + nb.Z(k);
+      const double qu = k < 0 ? u_c : nb.U(k);
+      const double qv = k < 0 ? v_c : nb.V(k);
       rz[j] = limited_r(zeta_c, qz, hx, hy, rx, ry);
       ru[j] = limited_r(u_c, qu, ux, uy, rx, ry);
       rv[j] = limited_r(v_c, qv, vx, vy, rx, ry);
@@ -563,6 +637,7 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
   hx = hx - G.delz_x[c];
   hy = hy - G.delz_y[c];
   double ub = u_c, vb = v_c;
+  bool fix = false;
   if (!dry_c) {
     // hgradfix2.f90:48-98
     bool setgrad = zeta_c < d.zmax[c];
@@ -570,15 +645,14 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
     for (int j = 0; j < 3; j++) {
       const int l = t3[j];
       if (l < 0) continue;
-      if (dry[l] && d.z[l] < zeta_c) setgrad = false;
+      if (nb.D(l) && nb.Z(l) < zeta_c) setgrad = false;
     }
     if (setgrad) {
       hx = -G.delz_x[c];
       hy = -G.delz_y[c];
       ub = kZero;
       vb = kZero;
-      rku_prev[c] = kZero;
-      rkv_prev[c] = kZero;
+      fix = true;
       ux = R(0); uy = R(0); vx = R(0); vy = R(0);
     }
     // to_vertices.f90:44-55
@@ -590,11 +664,47 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
       vb = kZero;
     }
   }
-  G.delh_x[c] = hx; G.delh_y[c] = hy;
-  G.delu_x[c] = ux; G.delu_y[c] = uy;
-  G.delv_x[c] = vx; G.delv_y[c] = vy;
-  d.u_b[c] = ub;
-  d.v_b[c] = vb;
+  GradOut<R> o;
+  o.hx = hx; o.hy = hy; o.ux = ux; o.uy = uy; o.vx = vx; o.vy = vy;
+  o.ub = ub; o.vb = vb; o.fix = fix;
+  return o;
+}
+
+// Gradients of every cell (list == nullptr) or of the listed cells (the cells with an
+// open-boundary face, ahead of the boundary kernel), stored for the phase kernels.
+template <class R>
+__global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, double* __restrict__ rku_prev,
+                                              double* __restrict__ rkv_prev, const double* __restrict__ u_in,
+                                              const double* __restrict__ v_in, const int32_t* __restrict__ list,
+                                              int nlist) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int c;
+  if (list) {
+    if (i >= nlist) return;
+    c = list[i];
+  } else {
+    if (i >= d.T) return;
+    c = i;
+  }
+  const int sid = d.cell_sid[c];
+  if (sid < 0 || d.sc[sid].converged) return;
+  const int T = d.T;
+  const NbGlobal nb{hs, d.z, u_in, v_in, dry};
+  int t3[3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) t3[j] = d.t2t3[(size_t)j * T + c];
+  const GradOut<R> g = cell_gradients<R>(d, G, nb, c, c, t3, [&](int k) { return d.st_id[(size_t)k * T + c]; },
+                                         (R*)nullptr, (R*)nullptr);
+  if (g.fix) {
+    rku_prev[c] = kZero;
+    rkv_prev[c] = kZero;
+  }
+  G.delh_x[c] = g.hx; G.delh_y[c] = g.hy;
+  G.delu_x[c] = g.ux; G.delu_y[c] = g.uy;
+  G.delv_x[c] = g.vx; G.delv_y[c] = g.vy;
+  d.u_b[c] = g.ub;
+  d.v_b[c] = g.vb;
 }
 
 // ---------------------------------------------------------------------------
@@ -888,23 +998,22 @@ __device__ __forceinline__ EdgeState edge_state(const Dev& d, const Geo<R>& G, c
   return s;
 }
 
-// invisc_fluxes.f90:39-147 for the interior edge between L=e(1) (slot ml) and
-// R=e(2) (slot mr); returns false when the edge is skipped.  The wet/dry tests and
-// the I1 stage comparison run on the FP64 face states; the flux function in R.
+// invisc_fluxes.f90:39-147 for an interior edge from its two face states: left =
+// e(1), right = e(2), dl/dr their dry flags, zl/zr their bed elevations and hl/hr
+// their cell depths (Rusanov's cell celerities); returns false when the edge is
+// skipped.  The wet/dry tests and the I1 stage comparison run on the FP64 face
+// states; the flux function in R.
 template <class R>
-__device__ __forceinline__ bool interior_flux(const Dev& d, const Geo<R>& G, const double* __restrict__ hs,
-                                              const uint8_t* __restrict__ dry, int L, int ml, int Rc, int mr, R nx,
-                                              R ny, double z0e, R* f, bool* bad) {
-  const bool dl = dry[L], dr = dry[Rc];
+__device__ __forceinline__ bool edge_flux(const Dev& d, bool dl, bool dr, const EdgeState& sl, const EdgeState& sr,
+                                          double zl, double zr, double hl, double hr, R nx, R ny, double z0e, R* f,
+                                          bool* bad) {
   if (dl && dr) return false;
   double hleft = kZero, uleft = kZero, vleft = kZero, hright = kZero, uright = kZero, vright = kZero;
   if (!dl) {
-    EdgeState s = edge_state(d, G, hs, L, ml);
-    hleft = s.h; uleft = s.u; vleft = s.v;
+    hleft = sl.h; uleft = sl.u; vleft = sl.v;
   }
   if (!dr) {
-    EdgeState s = edge_state(d, G, hs, Rc, mr);
-    hright = s.h; uright = s.u; vright = s.v;
+    hright = sr.h; uright = sr.u; vright = sr.v;
   }
   if (hleft < d.h_dry && hright < d.h_dry) return false;
   bool set_wall = false;
@@ -912,9 +1021,9 @@ __device__ __forceinline__ bool interior_flux(const Dev& d, const Geo<R>& G, con
     double h0 = fmax2(hright, hleft);
     h0 = h0 + z0e;
     if (dl)
-      if (d.z[L] + d.h_wet > h0) { set_wall = true; hleft = hright; }
+      if (zl + d.h_wet > h0) { set_wall = true; hleft = hright; }
     if (dr)
-      if (d.z[Rc] + d.h_wet > h0) { set_wall = true; hright = hleft; }
+      if (zr + d.h_wet > h0) { set_wall = true; hright = hleft; }
   }
   if (set_wall) {
     f[0] = R(kZero);
@@ -924,13 +1033,27 @@ __device__ __forceinline__ bool interior_flux(const Dev& d, const Geo<R>& G, con
   } else if (d.flux == STORM_FLUX_HLL) {
     flux_hll<R>(nx, ny, (R)hleft, (R)uleft, (R)vleft, (R)hright, (R)uright, (R)vright, (R)d.h_dry, f, bad);
   } else if (d.flux == STORM_FLUX_RUSANOV) {
-    const R cl = dl ? R(kZero) : (R)sqrt(kG * hs[L]);  // wavec (solverFVT.f90:180-181)
-    const R cr = dr ? R(kZero) : (R)sqrt(kG * hs[Rc]);
+    const R cl = dl ? R(kZero) : (R)sqrt(kG * hl);  // wavec (solverFVT.f90:180-181)
+    const R cr = dr ? R(kZero) : (R)sqrt(kG * hr);
     flux_rusanov<R>(nx, ny, (R)hleft, (R)uleft, (R)vleft, cl, (R)hright, (R)uright, (R)vright, cr, f);
   } else {
     flux_roe<R>(nx, ny, (R)hleft, (R)uleft, (R)vleft, (R)hright, (R)uright, (R)vright, f);
   }
   return true;
+}
+
+// The same for the edge between L=e(1) (slot ml) and R=e(2) (slot mr), with the face
+// states reconstructed from the stored gradients.
+template <class R>
+__device__ __forceinline__ bool interior_flux(const Dev& d, const Geo<R>& G, const double* __restrict__ hs,
+                                              const uint8_t* __restrict__ dry, int L, int ml, int Rc, int mr, R nx,
+                                              R ny, double z0e, R* f, bool* bad) {
+  const bool dl = dry[L], dr = dry[Rc];
+  if (dl && dr) return false;
+  EdgeState sl{kZero, kZero, kZero}, sr{kZero, kZero, kZero};
+  if (!dl) sl = edge_state(d, G, hs, L, ml);
+  if (!dr) sr = edge_state(d, G, hs, Rc, mr);
+  return edge_flux<R>(d, dl, dr, sl, sr, d.z[L], d.z[Rc], hs[L], hs[Rc], nx, ny, z0e, f, bad);
 }
 
 // Interior-edge fluxes of one stage (invisc_fluxes.f90:39-147), one thread per edge:
@@ -961,19 +1084,19 @@ __global__ void __launch_bounds__(128, 8) k_eflux(Dev d, Geo<R> G, const double*
 }
 
 // bed_slope_STD.f90:23-70 with adjustZb.f90:41-70: the amounts g*h*gradzb*area that
-// are subtracted from phi(i,2:3).  The adjust test (a negative reconstructed vertex
-// depth) and the adjusted gradient run in double on both paths.
-__device__ __forceinline__ void bed_source(const Dev& d, const Geo<double>& G, int c, double h_c, double* s2,
-                                           double* s3) {
+// are subtracted from phi(i,2:3), from the cell's depth gradient (dhx, dhy).  The
+// vertex offsets from the centroid (node - centroid, the reference's own differences)
+// are precomputed per cell; the adjust test (a negative reconstructed vertex depth)
+// and the adjusted gradient run in double on both paths.
+__device__ __forceinline__ void bed_source(const Dev& d, const Geo<double>& G, int c, double h_c, double dhx,
+                                           double dhy, double* s2, double* s3) {
   const int T = d.T;
-  const double dhx = G.delh_x[c], dhy = G.delh_y[c], xc = d.xc[c], yc = d.yc[c];
-  int vid[3];
   double hp[3];
   bool adjust = false;
 #pragma unroll
   for (int i = 0; i < 3; i++) {
-    vid[i] = d.vert[(size_t)i * T + c];
-    hp[i] = h_c + dhx * (d.node_x[vid[i]] - xc) + dhy * (d.node_y[vid[i]] - yc);
+    const size_t q = (size_t)i * T + c;
+    hp[i] = h_c + dhx * d.vox[q] + dhy * d.voy[q];
     if (hp[i] < kZero) adjust = true;
   }
   double gx, gy;
@@ -981,10 +1104,11 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<double>& G, i
     double zp[3], x[3], y[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
+      const int vid = d.vert[(size_t)i * T + c];
       hp[i] = fmin2(kZero, hp[i]);
-      zp[i] = d.zvtx[vid[i]] + hp[i];
-      x[i] = d.node_x[vid[i]];
-      y[i] = d.node_y[vid[i]];
+      zp[i] = d.zvtx[vid] + hp[i];
+      x[i] = d.node_x[vid];
+      y[i] = d.node_y[vid];
     }
     const double b1 = y[1] - y[2], c1 = x[2] - x[1];
     const double b2 = y[2] - y[0], c2 = x[0] - x[2];
@@ -999,27 +1123,25 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<double>& G, i
   *s2 = kG * h_c * gx * d.area[c];
   *s3 = kG * h_c * gy * d.area[c];
 }
-__device__ __forceinline__ void bed_source(const Dev& d, const Geo<float>& G, int c, double h_c, double* s2,
-                                           double* s3) {
+__device__ __forceinline__ void bed_source(const Dev& d, const Geo<float>& G, int c, double h_c, float dhx,
+                                           float dhy, double* s2, double* s3) {
   const int T = d.T;
-  const float dhx = G.delh_x[c], dhy = G.delh_y[c];
-  const double xc = d.xc[c], yc = d.yc[c];
-  int vid[3];
   double hp[3];
   bool adjust = false;
 #pragma unroll
   for (int i = 0; i < 3; i++) {
-    vid[i] = d.vert[(size_t)i * T + c];
-    hp[i] = h_c + (double)(dhx * (float)(d.node_x[vid[i]] - xc) + dhy * (float)(d.node_y[vid[i]] - yc));
+    const size_t q = (size_t)i * T + c;
+    hp[i] = h_c + (double)(dhx * (float)d.vox[q] + dhy * (float)d.voy[q]);
     if (hp[i] < kZero) adjust = true;
   }
   if (adjust) {
     double zp[3], x[3], y[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-      zp[i] = d.zvtx[vid[i]] + fmin2(kZero, hp[i]);
-      x[i] = d.node_x[vid[i]];
-      y[i] = d.node_y[vid[i]];
+      const int vid = d.vert[(size_t)i * T + c];
+      zp[i] = d.zvtx[vid] + fmin2(kZero, hp[i]);
+      x[i] = d.node_x[vid];
+      y[i] = d.node_y[vid];
     }
     const double a = kHalf / d.area[c];
     const double gx = a * ((y[1] - y[2]) * zp[0] + (y[2] - y[0]) * zp[1] + (y[0] - y[1]) * zp[2]);
@@ -1033,28 +1155,86 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<float>& G, in
   }
 }
 
-// Fluxes, sources and the RK update of stage s (1-based) for cell c: the faces are
-// added to phi in the order invisc_fluxes.f90 visits them (phi = zero first,
-// solverFVT.f90:194), then the bed slope, then the RK update.  phi and the RK
-// combination are FP64 on both paths.
+// Where the face contributions of a cell come from: the phase kernels' global arrays
+// (edge fluxes of k_eflux, stored gradients) ...
 template <class R>
-__device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int c, const double* __restrict__ hs,
-                                             const uint8_t* __restrict__ dry, double* p1o, double* p2o, double* p3o) {
+struct FacesGlobal {
+  const Dev& d;
+  const Geo<R>& G;
+  const double* __restrict__ hs;
+  int c;
+  // flux*length of the interior face in slot j, and whether the edge produced one
+  __device__ __forceinline__ bool iface(int j, R* f) const {
+    const int e = d.fref[(size_t)j * d.T + c];
+    f[0] = G.efx[e];
+    f[1] = G.efx[d.ne + e];
+    f[2] = G.efx[2 * d.ne + e];
+    return d.eok[e] != 0;
+  }
+  // the cell's own reconstructed state at face j (weslp2 walls)
+  __device__ __forceinline__ EdgeState own(int j) const {
+    const size_t q = (size_t)j * d.T + c;
+    EdgeState s;
+    s.h = recon(hs[c], G.delh_x[c], G.rc_x[q], G.delh_y[c], G.rc_y[q]);
+    s.u = recon(d.u_b[c], G.delu_x[c], G.rc_x[q], G.delu_y[c], G.rc_y[q]);
+    s.v = recon(d.v_b[c], G.delv_x[c], G.rc_x[q], G.delv_y[c], G.rc_y[q]);
+    return s;
+  }
+  __device__ __forceinline__ void dh(R* x, R* y) const {
+    *x = G.delh_x[c];
+    *y = G.delh_y[c];
+  }
+};
+
+// ... or a tile's shared memory (k_tile): edge fluxes by local edge, face states and
+// depth gradients by local cell.
+template <class R>
+struct FacesTile {
+  const uint16_t* __restrict__ lfe;
+  int T, c, l, ngm, nem;
+  const R* sf;             // [3][nem]
+  const uint8_t* seok;     // [nem]
+  const double *sfh, *sfu, *sfv;  // [3][ngm]
+  const R *sdhx, *sdhy;    // [owned]
+  __device__ __forceinline__ bool iface(int j, R* f) const {
+    const int le = lfe[(size_t)j * T + c];
+    f[0] = sf[le];
+    f[1] = sf[nem + le];
+    f[2] = sf[2 * nem + le];
+    return seok[le] != 0;
+  }
+  // the face state is clipped at zero depth; weslp2 skips any face state below
+  // h_dry > 0, so the clip never changes its result
+  __device__ __forceinline__ EdgeState own(int j) const {
+    EdgeState s;
+    s.h = sfh[j * ngm + l];
+    s.u = sfu[j * ngm + l];
+    s.v = sfv[j * ngm + l];
+    return s;
+  }
+  __device__ __forceinline__ void dh(R* x, R* y) const {
+    *x = sdhx[l];
+    *y = sdhy[l];
+  }
+};
+
+// Fluxes and sources of stage s for cell c: the faces are added to phi in the order
+// invisc_fluxes.f90 visits them (phi = zero first, solverFVT.f90:194), then the bed
+// slope, wind and culvert terms.  phi is FP64 on both paths.
+template <class R, class FS>
+__device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, const FS& fs, int c, double h_c,
+                                             bool dry_c, double* p1o, double* p2o, double* p3o) {
   const int T = d.T;
-  const bool dry_c = dry[c];
-  const double h_c = hs[c];
   double p1 = kZero, p2 = kZero, p3 = kZero;
   const uint8_t ord = d.forder[c];
   // Issue the loads of all three faces before the (ordered) accumulation: face
-  // descriptors first, then the edge fluxes of the interior faces, so the gathers
-  // overlap instead of forming one dependent chain per face.
-  int fj[3], fkd[3], fre[3];
+  // descriptors first, then the fluxes of the interior faces, so the gathers overlap
+  // instead of forming one dependent chain per face.
+  int fj[3], fkd[3];
 #pragma unroll
   for (int t = 0; t < 3; t++) {
     fj[t] = (ord >> (2 * t)) & 3;
-    const size_t q = (size_t)fj[t] * T + c;
-    fkd[t] = d.fkind[q] & 7;
-    fre[t] = d.fref[q];
+    fkd[t] = d.fkind[(size_t)fj[t] * T + c] & 7;
   }
   bool fok[3];
   R fv[3][3];
@@ -1062,13 +1242,7 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
   for (int t = 0; t < 3; t++) {
     fok[t] = false;
     fv[t][0] = fv[t][1] = fv[t][2] = R(0);
-    if (fkd[t] == FACE_LEFT || fkd[t] == FACE_RIGHT) {
-      const int e = fre[t];  // flux*length of the edge, evaluated once by k_eflux
-      fok[t] = d.eok[e];
-      fv[t][0] = G.efx[e];
-      fv[t][1] = G.efx[d.ne + e];
-      fv[t][2] = G.efx[2 * d.ne + e];
-    }
+    if (fkd[t] == FACE_LEFT || fkd[t] == FACE_RIGHT) fok[t] = fs.iface(fj[t], fv[t]);
   }
 #pragma unroll
   for (int t = 0; t < 3; t++) {
@@ -1092,7 +1266,7 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
       if (dry_c) continue;
       const double nx = d.fnx[q], ny = d.fny[q], len = d.flen[q];
       if (d.btype == 0) {  // wenslp3_fluxes.f90:34-67
-        const int w = fre[t];
+        const int w = d.fref[q];
         const double h1 = d.hvtx[d.wall_p1[w]], h2 = d.hvtx[d.wall_p2[w]];
         double hedge = qsqrt((h1 * h1 + h1 * h2 + h2 * h2) * kOneThird);
         if (hedge < kZero) hedge = kZero;
@@ -1100,11 +1274,11 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
         p2 = p2 - kHalf * kG * hedge * hedge * nx * len;
         p3 = p3 - kHalf * kG * hedge * hedge * ny * len;
       } else {  // weslp2_fluxes.f90:34-76
-        const size_t qc = (size_t)j * T + c;
-        const double hleft = recon(h_c, G.delh_x[c], G.rc_x[qc], G.delh_y[c], G.rc_y[qc]);
+        const EdgeState o = fs.own(j);
+        const double hleft = o.h;
         if (hleft < d.h_dry) continue;
-        const double uleft = recon(d.u_b[c], G.delu_x[c], G.rc_x[qc], G.delu_y[c], G.rc_y[qc]);
-        const double vleft = recon(d.v_b[c], G.delv_x[c], G.rc_x[qc], G.delv_y[c], G.rc_y[qc]);
+        const double uleft = o.u;
+        const double vleft = o.v;
         const double tx = -ny, ty = nx;  // edges%tang flipped with the normal
         double uright = uleft * tx + vleft * ty;
         uright = uright + 2.0 * sqrt(kG * hleft);
@@ -1116,7 +1290,7 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
         p3 = p3 - (f3 + dh * ny) * len;
       }
     } else if (kind == FACE_BC) {
-      const int e = fre[t];
+      const int e = d.fref[q];
       p1 = p1 - d.bc_c[e];
       p2 = p2 - d.bc_c[d.nbce + e];
       p3 = p3 - d.bc_c[2 * d.nbce + e];
@@ -1124,7 +1298,9 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
   }
   if (!dry_c) {
     double s2, s3;
-    bed_source(d, G, c, h_c, &s2, &s3);
+    R dhx, dhy;
+    fs.dh(&dhx, &dhy);
+    bed_source(d, G, c, h_c, dhx, dhy, &s2, &s3);
     p2 = p2 - s2;
     p3 = p3 - s3;
     if (d.wcoef1) {  // wind forcing (solverFVT.f90:218-224)
@@ -1152,10 +1328,12 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, int 
 
 // The RK update of stage s (1-based) for cell c from its phi (solverFVT.f90:259-325).
 __device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c, bool dry_c, double p1, double p2,
-                                          double p3, uint8_t* __restrict__ dry_next) {
+                                          double p3, uint8_t* __restrict__ dry_next, const double* __restrict__ u_in,
+                                          const double* __restrict__ v_in, double* __restrict__ u_out,
+                                          double* __restrict__ v_out) {
   const int T = d.T;
   // RK update (solverFVT.f90:259-283)
-  const double u_c = d.u_a[c], v_c = d.v_a[c];
+  const double u_c = u_in[c], v_c = v_in[c];
   double delt;
   if (d.steady) {
     const double um = (h_c < d.h_dry) ? kZero : qsqrt(u_c * u_c + v_c * v_c);
@@ -1202,8 +1380,8 @@ __device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c
   d.rkh[qs] = rh;
   d.rku[qs] = ru;
   d.rkv[qs] = rv;
-  d.u_a[c] = un;
-  d.v_a[c] = vn;
+  u_out[c] = un;
+  v_out[c] = vn;
   if (s < d.K) {
     double um;
     dry_next[c] = dry_flag(rh, un, vn, d.h_dry, d.h_wet, &um);
@@ -1214,10 +1392,14 @@ __device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c
 
 template <class R>
 __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, int c, const double* __restrict__ hs,
-                                          const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+                                          const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next,
+                                          const double* __restrict__ u_in, const double* __restrict__ v_in,
+                                          double* __restrict__ u_out, double* __restrict__ v_out) {
   double p1, p2, p3;
-  assemble_phi<R>(d, G, c, hs, dry, &p1, &p2, &p3);
-  rk_update(d, s, c, hs[c], dry[c] != 0, p1, p2, p3, dry_next);
+  const double h_c = hs[c];
+  const bool dry_c = dry[c] != 0;
+  assemble_phi<R>(d, G, FacesGlobal<R>{d, G, hs, c}, c, h_c, dry_c, &p1, &p2, &p3);
+  rk_update(d, s, c, h_c, dry_c, p1, p2, p3, dry_next, u_in, v_in, u_out, v_out);
 }
 
 // Residual smoothing (solverFVT.f90:238-256, activateRSAVG): the stage's phi is
@@ -1241,7 +1423,7 @@ __global__ void __launch_bounds__(128) k_flux_phi(Dev d, Geo<R> G, const double*
   const int sid = d.cell_sid[c];
   if (sid < 0 || d.sc[sid].converged) return;
   double p1, p2, p3;
-  assemble_phi<R>(d, G, c, hs, dry, &p1, &p2, &p3);
+  assemble_phi<R>(d, G, FacesGlobal<R>{d, G, hs, c}, c, hs[c], dry[c] != 0, &p1, &p2, &p3);
   const size_t T = d.T;
   d.phi[c] = p1;
   d.phi[T + c] = p2;
@@ -1273,39 +1455,263 @@ __global__ void __launch_bounds__(128) k_update(Dev d, int s, const double* __re
   const int sid = d.cell_sid[c];
   if (sid < 0 || d.sc[sid].converged) return;
   const size_t T = d.T;
-  rk_update(d, s, c, hs[c], dry[c] != 0, d.phi[c], d.phi[T + c], d.phi[2 * T + c], dry_next);
+  rk_update(d, s, c, hs[c], dry[c] != 0, d.phi[c], d.phi[T + c], d.phi[2 * T + c], dry_next, d.u_a, d.v_a, d.u_a,
+            d.v_a);
 }
 
 // All cells without an open-boundary face (those wait for k_bc in k_flux_bc).
 template <class R>
 __global__ void __launch_bounds__(128, 10) k_flux(Dev d, Geo<R> G, int s, const double* __restrict__ hs,
-                                              const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+                                              const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next,
+                                              const double* __restrict__ u_in, const double* __restrict__ v_in,
+                                              double* __restrict__ u_out, double* __restrict__ v_out) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.T) return;
   const int sid = d.cell_sid[c];
   if (sid < 0 || d.sc[sid].converged) return;
   if (d.forder[c] & kOrderHasBc) return;
-  flux_cell<R>(d, G, s, c, hs, dry, dry_next);
+  flux_cell<R>(d, G, s, c, hs, dry, dry_next, u_in, v_in, u_out, v_out);
 }
 
 // The cells with an open-boundary face, after k_bc.
 template <class R>
 __global__ void __launch_bounds__(128) k_flux_bc(Dev d, Geo<R> G, int s, const double* __restrict__ hs,
-                                                 const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
+                                                 const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next,
+                                                 const double* __restrict__ u_in, const double* __restrict__ v_in,
+                                                 double* __restrict__ u_out, double* __restrict__ v_out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.nbc_cells) return;
   const int c = d.bc_cells[i];
   if (d.sc[d.cell_sid[c]].converged) return;
-  flux_cell<R>(d, G, s, c, hs, dry, dry_next);
+  flux_cell<R>(d, G, s, c, hs, dry, dry_next, u_in, v_in, u_out, v_out);
+}
+
+// ---------------------------------------------------------------------------
+// The fused RK stage over Morton tiles (one CTA per tile of kTileCells cell slots):
+//   A  the stage-input state (h, z, u, v, dry flag) of the tile's owned, H1 and H2
+//      cells into shared memory (owned cells: coalesced; halo: gathered);
+//   B  gradients, limiter, hgradfix2 and velocity zeroing of the owned and H1 cells
+//      (cell_gradients, the phase kernels' arithmetic) and their three face states;
+//   C  the flux of every edge of an owned cell, once, in the reference's orientation
+//      (edge_flux); the fluxes the boundary cells' update needs go to global memory;
+//   D  the ordered face gather, sources and SSP-RK update of every owned cell
+//      without an open-boundary face (assemble_phi + rk_update).
+// The boundary cells keep the phase path: their gradients (k_grad over the
+// boundary-cell list) and k_bc run on the side stream beside this kernel, and
+// k_flux_bc updates them afterwards.  Velocities ping-pong between two buffers: a
+// tile may still read a neighbour's stage-input velocity while the neighbour's own
+// tile writes its new one.
+constexpr int kTileCells = 256;
+constexpr int kTileThreads = 256;
+
+struct TileSmem {
+  size_t h, z, u, v, fh, fu, fv, dhx, dhy, f, dry, eok, total;
+};
+__host__ __device__ inline TileSmem tile_smem_layout(int ns, int ng, int ne, int tc, int rsz) {
+  TileSmem m;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t r = o;
+    o += (bytes + 15) & ~(size_t)15;
+    return r;
+  };
+  m.h = take(8 * (size_t)ns);
+  m.z = take(8 * (size_t)ns);
+  m.u = take(8 * (size_t)ns);
+  m.v = take(8 * (size_t)ns);
+  m.fh = take(8 * 3 * (size_t)ng);
+  m.fu = take(8 * 3 * (size_t)ng);
+  m.fv = take(8 * 3 * (size_t)ng);
+  m.dhx = take((size_t)rsz * tc);
+  m.dhy = take((size_t)rsz * tc);
+  m.f = take((size_t)rsz * 3 * ne);
+  m.dry = take(ns);
+  m.eok = take(ne);
+  m.total = o;
+  return m;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kTileThreads, 3)
+    k_tile(Dev d, Geo<R> G, TileDev tp, int s, const double* __restrict__ hs, const uint8_t* __restrict__ dry,
+           uint8_t* __restrict__ dry_next, const double* __restrict__ u_in, const double* __restrict__ v_in,
+           double* __restrict__ u_out, double* __restrict__ v_out, double* __restrict__ rku_prev,
+           double* __restrict__ rkv_prev) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  const int t = blockIdx.x;
+  const int* I = tp.info + (size_t)t * TI_N;
+  const int tsid = I[TI_SID];
+  if (tsid >= 0 && d.sc[tsid].converged) return;
+  const int nown = I[TI_NOWN], n1 = I[TI_N1], n2 = I[TI_N2], hoff = I[TI_HOFF], h1off = I[TI_H1OFF];
+  const int er0 = I[TI_ER0], nr = I[TI_NR], nb = I[TI_NB], boff = I[TI_BOFF];
+  const int nS = nown + n1 + n2, nG = nown + n1, nE = nr + nb;
+  const int ngm = tp.ng_max, nem = tp.ne_max;
+  const int T = d.T, c0 = t * tp.tc;
+  const TileSmem L = tile_smem_layout(tp.ns_max, ngm, nem, tp.tc, (int)sizeof(R));
+  double* s_h = reinterpret_cast<double*>(tsm + L.h);
+  double* s_z = reinterpret_cast<double*>(tsm + L.z);
+  double* s_u = reinterpret_cast<double*>(tsm + L.u);
+  double* s_v = reinterpret_cast<double*>(tsm + L.v);
+  double* s_fh = reinterpret_cast<double*>(tsm + L.fh);
+  double* s_fu = reinterpret_cast<double*>(tsm + L.fu);
+  double* s_fv = reinterpret_cast<double*>(tsm + L.fv);
+  R* s_dhx = reinterpret_cast<R*>(tsm + L.dhx);
+  R* s_dhy = reinterpret_cast<R*>(tsm + L.dhy);
+  R* s_f = reinterpret_cast<R*>(tsm + L.f);
+  uint8_t* s_dry = tsm + L.dry;
+  uint8_t* s_eok = tsm + L.eok;
+
+  // A: stage-input state of every local cell
+  for (int l = threadIdx.x; l < nS; l += blockDim.x) {
+    const int g = l < nown ? c0 + l : tp.halo[hoff + l - nown];
+    s_h[l] = hs[g];
+    s_z[l] = d.z[g];
+    s_u[l] = u_in[g];
+    s_v[l] = v_in[g];
+    s_dry[l] = dry[g];
+  }
+  __syncthreads();
+
+  // B: gradients and face states of the owned and H1 cells
+  const NbShared nbs{s_h, s_z, s_u, s_v, s_dry};
+  for (int l = threadIdx.x; l < nG; l += blockDim.x) {
+    const bool own = l < nown;
+    const int g = own ? c0 + l : tp.halo[hoff + l - nown];
+    const int sid = d.cell_sid[g];
+    if (sid < 0 || d.sc[sid].converged) continue;
+    int t3[3];
+    const uint16_t* st;
+    size_t sst;
+    if (own) {
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const uint16_t x = tp.lt3[(size_t)j * T + g];
+        t3[j] = x == kNoLocal ? -1 : (int)x;
+      }
+      st = tp.lst + g;
+      sst = (size_t)T;
+    } else {
+      const size_t r = (size_t)(h1off + l - nown);
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        const uint16_t x = tp.h1_t3[3 * r + j];
+        t3[j] = x == kNoLocal ? -1 : (int)x;
+      }
+      st = tp.h1_st + (size_t)tp.kst * r;
+      sst = 1;
+    }
+    R rx[3], ry[3];
+    const GradOut<R> gr = cell_gradients<R>(d, G, nbs, g, l, t3, [&](int k) { return (int)st[(size_t)k * sst]; },
+                                            rx, ry);
+    if (d.lim != 2) {
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        rx[j] = G.rc_x[(size_t)j * T + g];
+        ry[j] = G.rc_y[(size_t)j * T + g];
+      }
+    }
+    if (own) {
+      // the boundary cells' previous-level momentum is zeroed by their k_grad pass
+      if (gr.fix && !(d.forder[g] & kOrderHasBc)) {
+        rku_prev[g] = kZero;
+        rkv_prev[g] = kZero;
+      }
+      s_dhx[l] = gr.hx;
+      s_dhy[l] = gr.hy;
+    }
+    const double h_c = s_h[l];
+#pragma unroll
+    for (int m = 0; m < 3; m++) {  // edge_state of the three faces (invisc_fluxes.f90:53-81)
+      double fh = recon(h_c, gr.hx, rx[m], gr.hy, ry[m]);
+      if (fh < kZero) fh = kZero;
+      s_fh[m * ngm + l] = fh;
+      s_fu[m * ngm + l] = recon(gr.ub, gr.ux, rx[m], gr.uy, ry[m]);
+      s_fv[m * ngm + l] = recon(gr.vb, gr.vx, rx[m], gr.vy, ry[m]);
+    }
+  }
+  __syncthreads();
+
+  // C: the flux of every edge of an owned cell
+  for (int le = threadIdx.x; le < nE; le += blockDim.x) {
+    int e;
+    uint32_t lo;
+    if (le < nr) {
+      e = er0 + le;
+      lo = tp.eloc[e];
+    } else {
+      e = tp.be[boff + le - nr];
+      lo = tp.beloc[boff + le - nr];
+    }
+    const int sid = d.edge_sid[e];
+    bool ok = false;
+    if (!d.sc[sid].converged) {
+      const int a = lo & 0xFFFF, b = lo >> 16;
+      const uint8_t sl = d.eslot[e];
+      const int ml = sl & 3, mr = (sl >> 2) & 3;
+      const bool dl = s_dry[a], dr = s_dry[b];
+      const EdgeState fa{s_fh[ml * ngm + a], s_fu[ml * ngm + a], s_fv[ml * ngm + a]};
+      const EdgeState fb{s_fh[mr * ngm + b], s_fu[mr * ngm + b], s_fv[mr * ngm + b]};
+      R f[3];
+      bool bad = false;
+      ok = edge_flux<R>(d, dl, dr, fa, fb, s_z[a], s_z[b], s_h[a], s_h[b], G.enx[e], G.eny[e],
+                        (dl || dr) ? d.ez0[e] : kZero, f, &bad);
+      if (ok) {
+        const R len = G.elen[e];
+        f[0] = f[0] * len;
+        f[1] = f[1] * len;
+        f[2] = f[2] * len;
+        s_f[le] = f[0];
+        s_f[nem + le] = f[1];
+        s_f[2 * nem + le] = f[2];
+      }
+      if ((sl & kEdgeExport) && le < nr) {  // a boundary cell's face: k_flux_bc reads it
+        d.eok[e] = ok;
+        if (ok) {
+          G.efx[e] = f[0];
+          G.efx[d.ne + e] = f[1];
+          G.efx[2 * d.ne + e] = f[2];
+        }
+      }
+      if (bad) atomicOr(&d.sc[sid].status, 2);
+    }
+    s_eok[le] = ok;
+  }
+  __syncthreads();
+
+  // D: ordered gather, sources and RK update of the owned cells
+  for (int l = threadIdx.x; l < nown; l += blockDim.x) {
+    const int c = c0 + l;
+    const int sid = d.cell_sid[c];
+    if (sid < 0 || d.sc[sid].converged) continue;
+    if (d.forder[c] & kOrderHasBc) continue;
+    const double h_c = s_h[l];
+    const bool dry_c = s_dry[l] != 0;
+    const FacesTile<R> fs{tp.lfe, T, c, l, ngm, nem, s_f, s_eok, s_fh, s_fu, s_fv, s_dhx, s_dhy};
+    double p1, p2, p3;
+    assemble_phi<R>(d, G, fs, c, h_c, dry_c, &p1, &p2, &p3);
+    rk_update(d, s, c, h_c, dry_c, p1, p2, p3, dry_next, u_in, v_in, u_out, v_out);
+  }
+}
+
+size_t tile_smem_bytes(const TileDev& t, bool mixed) {
+  return tile_smem_layout(t.ns_max, t.ng_max, t.ne_max, t.tc, mixed ? 4 : 8).total;
+}
+
+void set_tile_smem_limit(int bytes) {
+  cudaFuncSetAttribute(k_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 // ---------------------------------------------------------------------------
 // After the RK stages: find_dry_cells, fric_terms_impl, hvalve, rk level copy and the
 // block partials of the iteration's reductions (solverFVT.f90:335-386, 407-445).
 // kHalo: the handle links partitions, and halo cells stay out of the partials.
+// u_src/v_src: the velocities of the last stage (the fused path's ping-pong buffer);
+// the friction step writes the next iteration's start into d.u_a/d.v_a.
 template <bool kHalo>
-__global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
-  __shared__ double sm[kRedThreads / 32];
+__global__ void __launch_bounds__(kRedThreads) k_fric(Dev d, const double* __restrict__ u_src,
+                                                      const double* __restrict__ v_src) {
+  __shared__ double sm[5 * (kRedThreads / 32)];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int T = d.T, K = d.K;
   const int sid = c < T ? d.cell_sid[c] : -1;
@@ -1315,7 +1721,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
   if (sid >= 0) {
     const size_t qk = (size_t)K * T + c;
     const double h = d.rkh[qk];
-    double u = d.u_a[c], v = d.v_a[c];
+    double u = u_src[c], v = v_src[c];
     double ru = d.rku[qk], rv = d.rkv[qk];
     const double h0 = d.rkh[c];  // rkh(i,0), the iteration's starting depth
     double um;
@@ -1395,38 +1801,46 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d) {
       atomicOr(&d.sc[sid].status, 1);
     }
   }
-  double* pb = d.part + 8 * blockIdx.x;
-  double r0 = block_sum<kRedThreads>(st, sm);
-  if (threadIdx.x == 0) pb[0] = r0;
-  double r1 = block_sum<kRedThreads>(sb, sm);
-  if (threadIdx.x == 0) pb[1] = r1;
-  double r2 = block_sum<kRedThreads>(tm, sm);
-  if (threadIdx.x == 0) pb[2] = r2;
-  double r3 = block_max<kRedThreads>(rm, sm);
-  if (threadIdx.x == 0) pb[3] = r3;
-  double r4 = block_min<kRedThreads>(dtc, sm);
-  if (threadIdx.x == 0) pb[4] = r4;
+  block_reduce5<kRedThreads>(st, sb, tm, rm, dtc, sm, d.part + 8 * blockIdx.x);
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
-  __shared__ double sm[kRedThreads / 32];
+  __shared__ double sm[5 * (kRedThreads / 32)];
+  __shared__ double red[5];
   const int sid = blockIdx.x;
   Scalars* sc = &d.sc[sid];
   if (sc->converged) return;
   double a0 = kZero, a1 = kZero, a2 = kZero, a3 = kZero, a4 = kVlarge;
-  for (int b = threadIdx.x; b < sc->blk_cnt; b += blockDim.x) {
-    const double* pb = d.part + 8 * (sc->blk_off + b);
+  const int cnt = sc->blk_cnt;
+  const double* p0 = d.part + 8 * (size_t)sc->blk_off;
+  int b = threadIdx.x;
+  // four partial records in flight per thread; each thread still adds its records in
+  // increasing order, so the sums round as in a one-at-a-time loop
+  for (; b + 3 * kRedThreads < cnt; b += 4 * kRedThreads) {
+    double r[4][5];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int j = 0; j < 5; j++) r[k][j] = p0[8 * (size_t)(b + k * kRedThreads) + j];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      a0 = a0 + r[k][0];
+      a1 = a1 + r[k][1];
+      a2 = a2 + r[k][2];
+      a3 = fmax2(a3, r[k][3]);
+      a4 = fmin2(a4, r[k][4]);
+    }
+  }
+  for (; b < cnt; b += kRedThreads) {
+    const double* pb = p0 + 8 * (size_t)b;
     a0 = a0 + pb[0];
     a1 = a1 + pb[1];
     a2 = a2 + pb[2];
     a3 = fmax2(a3, pb[3]);
     a4 = fmin2(a4, pb[4]);
   }
-  const double sumtop = block_sum<kRedThreads>(a0, sm);
-  const double sumbot = block_sum<kRedThreads>(a1, sm);
-  const double tmass = block_sum<kRedThreads>(a2, sm);
-  const double rmax_phi = block_max<kRedThreads>(a3, sm);
-  const double dtmin = block_min<kRedThreads>(a4, sm);
+  block_reduce5<kRedThreads>(a0, a1, a2, a3, a4, sm, red);
+  const double sumtop = red[0], sumbot = red[1], tmass = red[2], rmax_phi = red[3], dtmin = red[4];
   if (threadIdx.x == 0) {
     sc->sumtop = sumtop;
     sc->sumbot = sumbot;
@@ -1800,9 +2214,9 @@ void launch_halo(const Dev& d, int level, uint8_t* f1, uint8_t* f2, cudaStream_t
   k_halo<<<(d.nhalo + 255) / 256, 256, 0, st>>>(d, level, f1, f2);
 }
 void launch_link_fric(const Dev& d, cudaStream_t st) { k_link_fric<<<1, 32, 0, st>>>(d); }
-void launch_fric(const Dev& d, cudaStream_t st) {
-  if (d.nhalo > 0) k_fric<true><<<d.nblk_red, kRedThreads, 0, st>>>(d);
-  else k_fric<false><<<d.nblk_red, kRedThreads, 0, st>>>(d);
+void launch_fric(const Dev& d, const double* u_src, const double* v_src, cudaStream_t st) {
+  if (d.nhalo > 0) k_fric<true><<<d.nblk_red, kRedThreads, 0, st>>>(d, u_src, v_src);
+  else k_fric<false><<<d.nblk_red, kRedThreads, 0, st>>>(d, u_src, v_src);
 }
 void launch_link_dt(const Dev& d, cudaStream_t st) { k_link_dt<<<1, 32, 0, st>>>(d); }
 void launch_link(const Dev& d, cudaStream_t st) { k_link<<<1, 32, 0, st>>>(d); }
@@ -1813,7 +2227,12 @@ template <class R>
 static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) {
   switch (L.which) {
     case STAGE_GRAD:
-      k_grad<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev);
+      k_grad<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev, L.u_in, L.v_in,
+                                                   nullptr, 0);
+      break;
+    case STAGE_GRAD_BC:
+      k_grad<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev, L.u_in, L.v_in,
+                                                   d.bc_cells, d.nbc_cells);
       break;
     case STAGE_BC:
       k_bc<R><<<L.grid, L.block, L.smem, L.stream>>>(d, G, L.hs, L.dry);
@@ -1822,10 +2241,12 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
       k_eflux<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry);
       break;
     case STAGE_FLUX:
-      k_flux<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.s, L.hs, L.dry, L.dry_next);
+      k_flux<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.s, L.hs, L.dry, L.dry_next, L.u_in, L.v_in, L.u_out,
+                                                   L.v_out);
       break;
     case STAGE_FLUX_BC:
-      k_flux_bc<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.s, L.hs, L.dry, L.dry_next);
+      k_flux_bc<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.s, L.hs, L.dry, L.dry_next, L.u_in, L.v_in, L.u_out,
+                                                      L.v_out);
       break;
     case STAGE_PHI:
       k_flux_phi<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, 0);
@@ -1838,6 +2259,10 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
       break;
     case STAGE_CULVERT:
       k_culvert<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry);
+      break;
+    case STAGE_TILE:
+      k_tile<R><<<L.grid, L.block, L.smem, L.stream>>>(d, G, *L.tiles, L.s, L.hs, L.dry, L.dry_next, L.u_in, L.v_in,
+                                                        L.u_out, L.v_out, L.rku_prev, L.rkv_prev);
       break;
   }
 }

@@ -30,9 +30,11 @@ EXPORTS = (
     "storm_fvt_cfl_dt_noalloc", "storm_fvt_create_batch", "storm_fvt_num_scenarios",
     "storm_fvt_set_scenario_state", "storm_fvt_get_scenario_state", "storm_fvt_scenario_stats",
     "storm_fvt_autotune", "storm_fvt_output_vertices", "storm_fvt_link_partitions",
+    "storm_fvt_set_stage_path", "storm_fvt_stage_path", "storm_fvt_tile_check",
 )
 
-KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux")
+KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux", "tile")
+STAGE_PHASES, STAGE_FUSED = 0, 1
 
 
 class StormError(RuntimeError):
@@ -84,6 +86,11 @@ def lib():
     L.storm_fvt_autotune.argtypes = [C.c_void_p, C.c_int32, ip]
     L.storm_fvt_output_vertices.argtypes = [C.c_void_p, C.POINTER(abi.OutputBoundary), C.c_int32] + [dp] * 5
     L.storm_fvt_link_partitions.argtypes = [C.c_void_p, C.c_int32, ip, ip, ip, ip, C.c_int32]
+    L.storm_fvt_set_stage_path.argtypes = [C.c_void_p, C.c_int32]
+    L.storm_fvt_stage_path.argtypes = [C.c_void_p]
+    L.storm_fvt_stage_path.restype = C.c_int32
+    L.storm_fvt_tile_check.argtypes = [C.POINTER(C.POINTER(abi.Mesh)), C.c_int32, C.c_int32,
+                                       C.POINTER(C.c_int64)]
     _lib = L
     return L
 
@@ -91,6 +98,16 @@ def lib():
 def _chk(rc: int):
     if rc != 0:
         raise StormError(rc, lib().storm_fvt_last_error().decode())
+
+
+def tile_check(meshes, tile_cells: int = 256) -> dict:
+    """Host-only build and check of the fused kernel's tile plan (storm_fvt_tile_check)."""
+    ms = [m.mesh if isinstance(m, PreparedMesh) else m for m in meshes]
+    arr = (C.POINTER(abi.Mesh) * len(ms))(*[C.pointer(m) for m in ms])
+    st = (C.c_int64 * 8)()
+    _chk(lib().storm_fvt_tile_check(arr, len(ms), int(tile_cells), st))
+    keys = ("tiles", "ns_max", "ng_max", "ne_max", "h1_cells", "h2_cells", "back_edges", "check")
+    return dict(zip(keys, [int(x) for x in st]))
 
 
 def default_options(**kw) -> abi.Options:
@@ -216,6 +233,14 @@ class Solver:
         ch = np.zeros(4, dtype=np.int32)
         _chk(lib().storm_fvt_autotune(self._h, int(iters), abi.iptr(ch)))
         return dict(zip(("node", "grad", "eflux", "flux"), ch.tolist()))
+
+    def set_stage_path(self, path: int):
+        """STAGE_FUSED (one tile kernel per stage, the default where it applies) or
+        STAGE_PHASES (k_grad, k_eflux, k_flux); re-captures the iteration graph."""
+        _chk(lib().storm_fvt_set_stage_path(self._h, int(path)))
+
+    def stage_path(self) -> int:
+        return int(lib().storm_fvt_stage_path(self._h))
 
     def kernel_times(self) -> dict:
         """Per-kernel device ms and launch counts of the last step in timing mode."""

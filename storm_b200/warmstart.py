@@ -420,9 +420,12 @@ def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, dev
     preds = predict(net, norm, inps, dev, timing=tm)
     infer_ms = tm["device_ms"]
     warm_states = [state_from_prediction(i, p) for i, p in zip(inps, preds)]
+    # the analytic prior alone: zero network output through the same mapping
+    prior_states = [state_from_prediction(i, np.zeros((len(i.d0), 3), dtype=np.float32)) for i in inps]
     cold64 = run_steady_batch(ev, istop=istop, precision=abi.PREC_FP64, device=device)
     cold_mx = run_steady_batch(ev, istop=istop, precision=abi.PREC_MIXED, device=device)
     warm_mx = run_steady_batch(ev, states=warm_states, istop=istop, precision=abi.PREC_MIXED, device=device)
+    prior_mx = run_steady_batch(ev, states=prior_states, istop=istop, precision=abi.PREC_MIXED, device=device)
     # the steady state itself: FP64 run on from the cold-start result to RMS dh < 1e-10
     # (without it, depths are compared with the cold FP64 run's own stop state)
     if reference:
@@ -443,7 +446,12 @@ def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, dev
                 "device_s_batch": r["device_ms"] / 1e3, "device_ms_per_scenario": r["device_ms"] / len(ev),
                 "wall_s_batch": r["wall_s"]}
 
+    dh_prior = dmax(prior_mx["states"])
     out = {"cold_fp64": summ(cold64), "cold_mixed": summ(cold_mx), "warm_mixed": summ(warm_mx),
+           "prior_mixed": dict(summ(prior_mx), depth_err_vs_steady_max_m=max(dh_prior),
+                               depth_err_vs_steady_median_m=float(np.median(dh_prior)),
+                               within_1cm=int(sum(x <= 0.01 for x in dh_prior))),
+           "network_vs_prior_iters": float(prior_mx["iters"].mean() / max(warm_mx["iters"].mean(), 1)),
                    "inference_ms_batch": infer_ms, "inference_host_s_batch": tm["host_s"],
                    "features_host_s_batch": feat_s,
                    "speedup_per_scenario_vs_cold_fp64": (cold64["device_ms"]) / (warm_mx["device_ms"] + infer_ms),
@@ -459,14 +467,16 @@ def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, dev
                                                     "cold_mixed": float(np.median(dh_cold)),
                                                     "cold_fp64": float(np.median(dh_cold64)),
                                                     "prediction": float(np.median(dh_pred))}}
+    # the same tighter stop tests from the warm start, the prior alone and the cold start
     for rs in warm_rstops:
-        w = run_steady_batch(ev, states=warm_states, istop=istop, precision=abi.PREC_MIXED, device=device,
-                             rstop=rs)
-        dw = dmax(w["states"])
-        out[f"warm_mixed_rstop_{rs:g}"] = dict(summ(w), depth_err_vs_steady_median_m=float(np.median(dw)),
+        for name, st0 in (("warm_mixed", warm_states), ("prior_mixed", prior_states), ("cold_mixed", None)):
+            w = run_steady_batch(ev, states=st0, istop=istop, precision=abi.PREC_MIXED, device=device, rstop=rs)
+            dw = dmax(w["states"])
+            out[f"{name}_rstop_{rs:g}"] = dict(summ(w), depth_err_vs_steady_median_m=float(np.median(dw)),
                                                 depth_err_vs_steady_max_m=max(dw),
                                                 within_1cm=int(sum(x <= 0.01 for x in dw)))
     out["within_1cm"] = {"warm_mixed": int(sum(x <= 0.01 for x in dh_warm)),
+                         "prior_mixed": int(sum(x <= 0.01 for x in dh_prior)),
                          "cold_fp64": int(sum(x <= 0.01 for x in dh_cold64)), "of": len(ev)}
     plain = []
     for sc in ev[:plain_n]:
@@ -493,10 +503,14 @@ def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, dev
         out["speedup_per_scenario_vs_plain_fp64_single_cold"] = w_plain / warm_wall
         out["warm_batched_wall_s_per_scenario_incl_network"] = warm_wall
         for rs in warm_rstops:
+            for name, extra in (("warm_mixed", infer_ms / 1e3 + tm["host_s"] + feat_s), ("prior_mixed", feat_s),
+                                ("cold_mixed", 0.0)):
+                r = out[f"{name}_rstop_{rs:g}"]
+                ww = (r["wall_s_batch"] + extra) / len(ev)
+                r["wall_s_per_scenario_incl_preparation"] = ww
+                r["speedup_per_scenario_vs_plain_fp64_single_cold"] = w_plain / ww
             r = out[f"warm_mixed_rstop_{rs:g}"]
-            ww = (r["wall_s_batch"] + infer_ms / 1e3 + tm["host_s"] + feat_s) / len(ev)
-            r["wall_s_per_scenario_incl_network"] = ww
-            r["speedup_per_scenario_vs_plain_fp64_single_cold"] = w_plain / ww
+            r["wall_s_per_scenario_incl_network"] = r["wall_s_per_scenario_incl_preparation"]
     return out
 
 

@@ -1,0 +1,82 @@
+"""The fused stage kernel (k_tile) against the phase kernels (k_grad, k_eflux,
+k_flux), through the C-ABI.  Both paths run the same device functions for the
+gradient, edge-flux and update arithmetic, so every state array, RK level, vertex
+depth and iteration statistic must agree to the last bit, in FP64 and in mixed
+precision, with and without open boundaries, for single meshes and batches.  The
+oracle comparisons of test_gpu_parity.py run on the fused path (the default)."""
+import numpy as np
+import pytest
+
+from storm_b200 import abi, fvt, scenarios
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float64).view(np.uint64)
+
+
+def _run(pm, opts, sc, path, steps):
+    g = fvt.Solver(pm, opts, keep=pm)
+    if path == fvt.STAGE_PHASES:
+        g.set_stage_path(path)
+    assert g.stage_path() == path
+    g.set_state(sc.h0, sc.u0, sc.v0)
+    st = None
+    for n in (steps // 2, steps - steps // 2):
+        st = g.step(n)
+    out = g.state(), st
+    g.close()
+    return out
+
+
+@pytest.mark.parametrize("name,make,steps", [
+    ("channel-hll", lambda: scenarios.channel(flux=abi.FLUX_HLL), 60),
+    ("channel-roe-btype1", lambda: scenarios.channel(nx=60, ny=8, btype=1), 40),
+    ("channel-lim0-rk2", lambda: scenarios.channel(nx=60, ny=8, opt_limiter=0, rkorder=2), 40),
+    ("meander", lambda: scenarios.meander(n_target=40_000, seed=5), 40),
+    ("dambreak", lambda: scenarios.dambreak(n_target=30_000, seed=4), 40),
+])
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_fused_equals_phases(name, make, steps, precision, storm_lib):
+    sc = make()
+    sc.options.precision = precision
+    pm = fvt.build_mesh(sc.problem)
+    (a, sa) = _run(pm, sc.options, sc, fvt.STAGE_FUSED, steps)
+    (b, sb) = _run(pm, sc.options, sc, fvt.STAGE_PHASES, steps)
+    for k in ("h", "u", "v", "rkh", "rku", "rkv", "hvtx"):
+        if not np.array_equal(_bits(a[k]), _bits(b[k])):
+            d = np.abs(a[k] - b[k])
+            raise AssertionError(f"{name} {k}: {np.count_nonzero(_bits(a[k]) != _bits(b[k]))} differ, max {d.max():.3e}")
+    assert sa == sb
+
+
+def test_fused_batch_equals_phases(storm_lib):
+    scs = scenarios.batch_channels(6, 1500, 5000, seed=9, opt_limiter=0, precision=abi.PREC_MIXED)
+    pms = [fvt.build_mesh(s.problem) for s in scs]
+    outs = []
+    for path in (fvt.STAGE_FUSED, fvt.STAGE_PHASES):
+        b = fvt.BatchSolver(pms, scs[0].options, keep=pms)
+        if path == fvt.STAGE_PHASES:
+            b.set_stage_path(path)
+        assert b.stage_path() == path
+        for i, s in enumerate(scs):
+            b.set_scenario_state(i, s.h0, s.u0, s.v0)
+        b.step(300)
+        outs.append([(b.scenario_state(i), b.scenario_stats(i)) for i in range(len(scs))])
+        b.close()
+    for i, ((a, sa), (c, sc_)) in enumerate(zip(*outs)):
+        for k in ("h", "u", "v", "hvtx"):
+            assert np.array_equal(_bits(a[k]), _bits(c[k])), (i, k)
+        assert sa == sc_, i
+
+
+def test_fused_not_used_for_culverts_or_smoothing(storm_lib):
+    sc = scenarios.channel(nx=40, ny=6)
+    sc.options.rsavg_passes = 2
+    sc.options.rsavg_eps = 0.5
+    sc.options.rsavg_order = 1
+    pm = fvt.build_mesh(sc.problem)
+    g = fvt.Solver(pm, sc.options, keep=pm)
+    assert g.stage_path() == fvt.STAGE_PHASES
+    g.close()

@@ -31,6 +31,12 @@ def test_warm_start_needs_fewer_iterations(storm_lib):
     warm = warmstart.run_steady_batch(scs, states=states, istop=40000, precision=abi.PREC_MIXED)
     assert cold["converged"].all() and warm["converged"].all()
     assert warm["iters"].mean() < 0.67 * cold["iters"].mean(), (warm["iters"], cold["iters"])
+    # what the network adds over its analytic prior (zero network output through the
+    # same mapping to h, hu, hv): fewer iterations to the same stop test
+    prior = [warmstart.state_from_prediction(i, np.zeros((len(i.d0), 3), dtype=np.float32)) for i in inps]
+    pri = warmstart.run_steady_batch(scs, states=prior, istop=40000, precision=abi.PREC_MIXED)
+    assert pri["converged"].all()
+    assert warm["iters"].mean() < 0.8 * pri["iters"].mean(), (warm["iters"], pri["iters"])
     for a, b in zip(warm["states"], cold["states"]):
         # both runs stop at RMS dh < 1e-6, a few cm short of the steady state
         assert np.abs(a["h"] - b["h"]).max() < 0.25
