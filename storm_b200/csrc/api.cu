@@ -563,6 +563,7 @@ int upload(StormFvtHandle* h) {
   gd.rc_x = d.rc_x; gd.rc_y = d.rc_y; gd.st_w = d.st_w; gd.st_dx = d.st_dx; gd.st_dy = d.st_dy;
   gd.lsq_a = d.lsq_a; gd.lsq_b = d.lsq_b; gd.lsq_c = d.lsq_c; gd.lsq_det = d.lsq_det;
   gd.delz_x = d.delz_x; gd.delz_y = d.delz_y; gd.enx = d.enx; gd.eny = d.eny; gd.elen = d.elen;
+  gd.vox = d.vox; gd.voy = d.voy;
   gd.delh_x = d.delh_x; gd.delh_y = d.delh_y; gd.delu_x = d.delu_x; gd.delu_y = d.delu_y;
   gd.delv_x = d.delv_x; gd.delv_y = d.delv_y; gd.efx = d.efx;
   // FP32 copies for the mixed-precision path: the gradients and edge fluxes reuse the
@@ -597,6 +598,8 @@ int upload(StormFvtHandle* h) {
     fc.push_back({&gf.enx, f32(L.enx)});
     fc.push_back({&gf.eny, f32(L.eny)});
     fc.push_back({&gf.elen, f32(L.elen)});
+    fc.push_back({&gf.vox, f32(vox)});
+    fc.push_back({&gf.voy, f32(voy)});
     size_t total = 0;
     for (auto& c : fc) total += (c.host.size() * 4 + 255) & ~(size_t)255;
     cudaError_t ef = cudaMalloc(&h->arena32, std::max<size_t>(total, 256));
@@ -644,7 +647,12 @@ int upload(StormFvtHandle* h) {
   if (rct) return rct;
   int maxcnt = 1;
   for (int b = 0; b < L.nbdr; b++) maxcnt = std::max(maxcnt, L.bdr_cnt[b]);
-  h->bc_smem = (size_t)maxcnt * 2 * sizeof(double) + (((size_t)maxcnt + 7) & ~(size_t)7);
+  // per edge: two sums' terms (16 B) and a flag; with the fixed point's invariants
+  // cached, four more doubles and two flags (up to about 4,000 edges per boundary)
+  const size_t plain = (size_t)maxcnt * 2 * sizeof(double) + (((size_t)maxcnt + 7) & ~(size_t)7);
+  const size_t cached = (size_t)maxcnt * 6 * sizeof(double) + (((size_t)2 * maxcnt + 7) & ~(size_t)7);
+  d.bc_cache = cached <= 200 * 1024;
+  h->bc_smem = d.bc_cache ? cached : plain;
   if (h->bc_smem > 48 * 1024) set_bc_smem_limit((int)h->bc_smem);
   return 0;
 }

@@ -98,6 +98,7 @@ struct Dev {
   double *phi, *phi0;
   const int32_t* rs_cells;
   double rs_fac1, rs_fac2;
+  int32_t bc_cache;         // k_bc keeps the inflow fixed point's invariants in shared memory
   double* bc_c;             // [3][nbce] boundary contributions to phi
   double* bc_rec;           // [3][nbce] reconstructed boundary-edge h, u, v
   double* part;             // [nblk][8] reduction partials (blocks never span scenarios)
@@ -113,6 +114,7 @@ template <class R>
 struct Geo {
   const R *rc_x, *rc_y, *st_w, *st_dx, *st_dy, *lsq_a, *lsq_b, *lsq_c, *lsq_det, *delz_x, *delz_y;
   const R *enx, *eny, *elen;
+  const R *vox, *voy;  // [3][T] vertex minus centroid (bed_slope_STD), in R
   R *delh_x, *delh_y, *delu_x, *delu_y, *delv_x, *delv_y;
   R* efx;  // [3][ne]
 };

@@ -744,6 +744,137 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
     d.bc_c[NB + off + e] = c2;
     d.bc_c[2 * NB + off + e] = c3;
   };
+  if ((kind == BC_QBYH || kind == BC_QBYH_WET) && d.bc_cache) {
+    // inflowQbyH.f90:31-212 / :221-402 with the per-edge terms that do not depend on
+    // the iterate (edge depth and velocity, the Riemann invariant 2 sqrt(g h) + u.n,
+    // normal, length, the wet-only mask) computed once: every fixed-point iteration
+    // then evaluates only the qfrac-dependent part, with the same operations in the
+    // same order, and thread 0 adds the sums serially in string order.
+    const bool wet_only = kind == BC_QBYH_WET;
+    const double qin = sc->qin[slot];
+    if (qin < kVsmall) {
+      for (int e = threadIdx.x; e < cnt; e += blockDim.x) put(e, kZero, kZero, kZero);
+      if (threadIdx.x == 0) sc->cqin3[slot] = kZero;
+      return;
+    }
+    double* cb = smb + 2 * cnt;   // [cnt] 2 sqrt(g hleft) + uleft
+    double* cnx = cb + cnt;       // [cnt] normal x
+    double* cny = cnx + cnt;      // [cnt] normal y
+    double* cln = cny + cnt;      // [cnt] edge length
+    uint8_t* okc = (uint8_t*)(cln + cnt);  // [cnt] accumulation mask
+    uint8_t* v0 = okc + cnt;               // [cnt] wet-only mask
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+      const int i = d.bce_cell[off + e];
+      const bool dr = dry[i];
+      v0[e] = !(wet_only && dr);
+      const double hleft = dr ? kZero : fmax2(d.bc_rec[off + e], kZero);
+      tA[e] = hleft * d.bce_len[off + e];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double at = kZero;
+      for (int e = 0; e < cnt; e++)
+        if (v0[e]) at = at + tA[e];
+      s_atotal = at;
+      s_null = equals(at, kZero);
+      s_done = 0;
+    }
+    __syncthreads();
+    const bool null_area = s_null;
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+      double hleft = null_area ? sc->bch_max : d.bc_rec[off + e], uedg, vedg;
+      if (hleft < h_dry) {
+        hleft = fmax2(hleft, kZero);
+        uedg = kZero;
+        vedg = kZero;
+      } else {
+        uedg = d.bc_rec[NB + off + e];
+        vedg = d.bc_rec[2 * NB + off + e];
+      }
+      const double nx = d.bce_nx[off + e], ny = d.bce_ny[off + e];
+      const double uleft = uedg * nx + vedg * ny;
+      const double sq = sqrt(kG * hleft);
+      cb[e] = 2.0 * sq + uleft;
+      cnx[e] = nx;
+      cny[e] = ny;
+      cln[e] = d.bce_len[off + e];
+    }
+    __syncthreads();
+    // fixed-point iteration on the total flow area (:61-126)
+    double newatotal = kZero;
+    for (int counter = 0;; counter++) {
+      const double atotal = s_atotal;
+      const double qfrac = qin / atotal;
+      for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+        const double nx = cnx[e], ny = cny[e], len = cln[e];
+        double uright = -qfrac;
+        double hright = cb[e] - uright;
+        hright = hright * hright / 4.0 / kG;
+        uright = -qfrac * nx;
+        const double vright = -qfrac * ny;
+        okc[e] = v0[e] && !(hright < h_dry);
+        tA[e] = hright * len;
+        tB[e] = (uright * nx + vright * ny) * hright * len;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double na = kZero, qt = kZero;
+        int e = 0;
+        for (; e + 4 <= cnt; e += 4) {  // loads ahead of the two serial chains
+          const uint8_t o0 = okc[e], o1 = okc[e + 1], o2 = okc[e + 2], o3 = okc[e + 3];
+          const double a0 = tA[e], a1 = tA[e + 1], a2 = tA[e + 2], a3 = tA[e + 3];
+          const double b0 = tB[e], b1 = tB[e + 1], b2 = tB[e + 2], b3 = tB[e + 3];
+          if (o0) { na = na + a0; qt = qt + b0; }
+          if (o1) { na = na + a1; qt = qt + b1; }
+          if (o2) { na = na + a2; qt = qt + b2; }
+          if (o3) { na = na + a3; qt = qt + b3; }
+        }
+        for (; e < cnt; e++)
+          if (okc[e]) {
+            na = na + tA[e];
+            qt = qt + tB[e];
+          }
+        qt = fabs(qt);
+        if (fabs(qt - qin) / qin < 0.005 || counter > 50) s_done = 1;
+        else s_atotal = na;
+        tA[0] = na;  // hand newatotal to every thread through shared memory
+      }
+      __syncthreads();
+      newatotal = tA[0];
+      const int done = s_done;
+      __syncthreads();
+      if (done) break;
+    }
+    const double atotal = newatotal;  // :130
+    const double qfrac = qin / atotal;
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+      const double nx = cnx[e], ny = cny[e], len = cln[e];
+      double uright = -qfrac;
+      double hright = cb[e] - uright;
+      hright = hright * hright / 4.0 / kG;
+      uright = -qfrac * nx;
+      const double vright = -qfrac * ny;
+      const bool valid = v0[e] && !(hright < h_dry);
+      okc[e] = valid;
+      if (valid) {
+        const double f1 = hright * (uright * nx + vright * ny);
+        const double f2 = hright * uright * (uright * nx + vright * ny) + kHalf * kG * hright * hright * nx;
+        const double f3 = hright * vright * (uright * nx + vright * ny) + kHalf * kG * hright * hright * ny;
+        tA[e] = f1 * len;
+        put(e, f1 * len, f2 * len, f3 * len);
+      } else {
+        put(e, kZero, kZero, kZero);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double cq = kZero;
+      for (int e = 0; e < cnt; e++)
+        if (okc[e]) cq = cq + tA[e];
+      sc->cqin3[slot] = cq;
+    }
+    return;
+  }
   if (kind == BC_QBYH || kind == BC_QBYH_WET) {  // inflowQbyH.f90:31-212 / :221-402
     const bool wet_only = kind == BC_QBYH_WET;
     const double qin = sc->qin[slot];
@@ -1131,7 +1262,7 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<float>& G, in
 #pragma unroll
   for (int i = 0; i < 3; i++) {
     const size_t q = (size_t)i * T + c;
-    hp[i] = h_c + (double)(dhx * (float)d.vox[q] + dhy * (float)d.voy[q]);
+    hp[i] = h_c + (double)(dhx * G.vox[q] + dhy * G.voy[q]);
     if (hp[i] < kZero) adjust = true;
   }
   if (adjust) {
