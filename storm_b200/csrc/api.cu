@@ -83,6 +83,7 @@ struct StormFvtHandle {
   TileDev td{};
   void* tile_buf = nullptr;
   size_t tile_smem = 0;
+  int tile_grid = 0;        // persistent grid of k_tile: resident CTAs on all SMs
   bool tiles_ok = false;    // plan built and within the shared-memory limit
   bool want_tiles = true;   // storm_fvt_set_stage_path
   bool use_tiles = false;   // the captured iteration runs k_tile
@@ -212,7 +213,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     k_node<<<gN, h->bs_node, 0, h->stream>>>(d, hs, dry);
     if (done()) return STORM_ERR_CUDA;
     if (fused) {
-      const int nt = h->td.ntiles;
+      const int nt = h->tile_grid;
       if (gB > 0 && !timing) {
         // the boundary cells' gradients and k_bc on the side stream beside k_tile;
         // k_flux_bc updates those cells once both are done
@@ -394,6 +395,10 @@ int upload_tiles(StormFvtHandle* h) {
   t.eloc = at<uint32_t>(B, o_eloc); t.be = at<int32_t>(B, o_be); t.beloc = at<uint32_t>(B, o_beloc);
   h->tile_smem = smem;
   if (smem > 48 * 1024) set_tile_smem_limit((int)smem);
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+  const int per_sm = std::max(1, tile_blocks_per_sm(h->mixed, smem));
+  h->tile_grid = std::max(1, std::min(P.ntiles, nsm * per_sm));
   CK(cudaGetLastError());
   // the host copy of the plan is not needed after the upload
   P.halo = {}; P.h1_t3 = {}; P.h1_st = {}; P.lt3 = {}; P.lst = {}; P.lfe = {}; P.eloc = {}; P.be = {}; P.beloc = {};

@@ -151,6 +151,7 @@ struct StageLaunch {
   const TileDev* tiles;  // STAGE_TILE only
 };
 size_t tile_smem_bytes(const TileDev& t, bool mixed);
+int tile_blocks_per_sm(bool mixed, size_t smem);  // resident CTAs of k_tile per SM
 void set_tile_smem_limit(int bytes);
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed);
 void set_bc_smem_limit(int bytes);

@@ -672,17 +672,16 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
 
 // Gradients of every cell (list == nullptr) or of the listed cells (the cells with an
 // open-boundary face, ahead of the boundary kernel), stored for the phase kernels.
-template <class R>
+template <class R, bool kList>
 __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* __restrict__ hs,
                                               const uint8_t* __restrict__ dry, double* __restrict__ rku_prev,
                                               double* __restrict__ rkv_prev, const double* __restrict__ u_in,
-                                              const double* __restrict__ v_in, const int32_t* __restrict__ list,
-                                              int nlist) {
+                                              const double* __restrict__ v_in) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   int c;
-  if (list) {
-    if (i >= nlist) return;
-    c = list[i];
+  if (kList) {
+    if (i >= d.nbc_cells) return;
+    c = d.bc_cells[i];
   } else {
     if (i >= d.T) return;
     c = i;
@@ -1669,10 +1668,11 @@ __global__ void __launch_bounds__(kTileThreads, 3)
            double* __restrict__ u_out, double* __restrict__ v_out, double* __restrict__ rku_prev,
            double* __restrict__ rkv_prev) {
   extern __shared__ __align__(16) unsigned char tsm[];
-  const int t = blockIdx.x;
+  // persistent: each CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+  for (int t = blockIdx.x; t < tp.ntiles; t += gridDim.x) {
   const int* I = tp.info + (size_t)t * TI_N;
   const int tsid = I[TI_SID];
-  if (tsid >= 0 && d.sc[tsid].converged) return;
+  if (tsid >= 0 && d.sc[tsid].converged) continue;  // uniform over the CTA
   const int nown = I[TI_NOWN], n1 = I[TI_N1], n2 = I[TI_N2], hoff = I[TI_HOFF], h1off = I[TI_H1OFF];
   const int er0 = I[TI_ER0], nr = I[TI_NR], nb = I[TI_NB], boff = I[TI_BOFF];
   const int nS = nown + n1 + n2, nG = nown + n1, nE = nr + nb;
@@ -1822,10 +1822,19 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     assemble_phi<R>(d, G, fs, c, h_c, dry_c, &p1, &p2, &p3);
     rk_update(d, s, c, h_c, dry_c, p1, p2, p3, dry_next, u_in, v_in, u_out, v_out);
   }
+  __syncthreads();  // the next tile reuses the shared memory
+  }
 }
 
 size_t tile_smem_bytes(const TileDev& t, bool mixed) {
   return tile_smem_layout(t.ns_max, t.ng_max, t.ne_max, t.tc, mixed ? 4 : 8).total;
+}
+
+int tile_blocks_per_sm(bool mixed, size_t smem) {
+  int n = 0;
+  if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile<float>, kTileThreads, smem);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile<double>, kTileThreads, smem);
+  return n;
 }
 
 void set_tile_smem_limit(int bytes) {
@@ -2358,12 +2367,10 @@ template <class R>
 static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) {
   switch (L.which) {
     case STAGE_GRAD:
-      k_grad<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev, L.u_in, L.v_in,
-                                                   nullptr, 0);
+      k_grad<R, false><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev, L.u_in, L.v_in);
       break;
     case STAGE_GRAD_BC:
-      k_grad<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev, L.u_in, L.v_in,
-                                                   d.bc_cells, d.nbc_cells);
+      k_grad<R, true><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev, L.u_in, L.v_in);
       break;
     case STAGE_BC:
       k_bc<R><<<L.grid, L.block, L.smem, L.stream>>>(d, G, L.hs, L.dry);
