@@ -346,7 +346,8 @@ def _member_list(n, lo, hi, seed, limiter):
 
 
 def pipeline(train_n=4096, eval_n=64, lo=2000, hi=8000, gen_batch=512, istop=40000, epochs=30,
-             cells_per_batch=400_000, lr=1e-3, limiter=0, device=0, seed=7, log=print, weights_out=None):
+             cells_per_batch=400_000, lr=1e-3, limiter=0, device=0, seed=7, log=print, weights_out=None,
+             warm_rstops=(), plain_n=8):
     """Generate `train_n` steady states with the solver (mixed precision), train the
     network on them, then run the `eval_n` held-out scenarios (seeds disjoint) to
     steady state cold in FP64, cold in mixed precision and warm in mixed precision.
@@ -393,7 +394,8 @@ def pipeline(train_n=4096, eval_n=64, lo=2000, hi=8000, gen_batch=512, istop=400
         np.savez(weights_out, params=net.params_numpy(), **norm.arrays())
     del batches
     # 3. evaluation on held-out scenarios
-    res["eval"] = evaluate(net, norm, eval_n, lo, hi, istop, limiter, device, seed)
+    res["eval"] = evaluate(net, norm, eval_n, lo, hi, istop, limiter, device, seed, plain_n=plain_n,
+                           warm_rstops=warm_rstops)
     return res
 
 
@@ -532,7 +534,7 @@ def main(argv=None):
     ap.add_argument("--model", default=None, help="evaluate this trained model (.npz) instead of training")
     ap.add_argument("--plain-n", type=int, default=8)
     ap.add_argument("--warm-rstop", type=float, nargs="*", default=[],
-                    help="also run the warm start to these residuals (evaluation of --model)")
+                    help="also run the warm start, the prior alone and the cold start to these residuals")
     a = ap.parse_args(argv)
     from . import build
     build.build()
@@ -549,7 +551,8 @@ def main(argv=None):
                 f.write(s + "\n")
         return
     res = pipeline(a.train_n, a.eval_n, a.lo, a.hi, a.gen_batch, a.istop, a.epochs, a.cells_per_batch, a.lr,
-                   weights_out=a.weights_out, log=lambda m: print(m, flush=True))
+                   weights_out=a.weights_out, log=lambda m: print(m, flush=True), warm_rstops=a.warm_rstop,
+                   plain_n=a.plain_n)
     s = json.dumps(res)
     print(s)
     if a.json_out:
