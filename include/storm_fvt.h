@@ -354,15 +354,17 @@ STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t*
  * same either way):
  *   STORM_STAGE_PHASES  k_node, k_grad, k_eflux, k_flux per stage (gradients and edge
  *                       fluxes pass through device memory between the kernels);
- *   STORM_STAGE_FUSED   k_node, then one fused kernel per stage over Morton tiles of
- *                       256 cells (gradients, edge fluxes and the RK update of a tile
- *                       in shared memory), the default wherever it applies.
+ *   STORM_STAGE_FUSED   one fused kernel per stage over Morton tiles of 256 cells
+ *                       (vertex depths, gradients, edge fluxes and the RK update of a
+ *                       tile in shared memory), the default wherever it applies;
+ *   STORM_STAGE_FUSED_NODE_KERNEL  the same with the vertex depths computed by k_node
+ *                       before it (for measurement).
  * The fused path does not apply to culverts, residual smoothing or linked partitions
  * (those run the phase kernels whatever is set), nor to a mesh whose tiles do not fit
  * in shared memory.  Setting re-captures the iteration graph. */
-enum { STORM_STAGE_PHASES = 0, STORM_STAGE_FUSED = 1 };
+enum { STORM_STAGE_PHASES = 0, STORM_STAGE_FUSED = 1, STORM_STAGE_FUSED_NODE_KERNEL = 2 };
 STORM_FVT_API int storm_fvt_set_stage_path(StormFvtHandle* hd, int32_t path);
-/* The path the captured iteration runs (STORM_STAGE_PHASES or STORM_STAGE_FUSED). */
+/* The path the captured iteration runs (one of the STORM_STAGE_* values). */
 STORM_FVT_API int32_t storm_fvt_stage_path(const StormFvtHandle* hd);
 
 /* Host-only check of the fused kernel's tile plan for a batch of prepared meshes

@@ -23,7 +23,6 @@ namespace storm {
 
 __global__ void k_init(Dev d, int c0);
 __global__ void k_init_final(Dev d, int sid);
-__global__ void k_node(Dev d, const double* hs, const uint8_t* dry);
 __global__ void k_final(Dev d);
 
 static thread_local std::string g_err;
@@ -87,6 +86,9 @@ struct StormFvtHandle {
   bool tiles_ok = false;    // plan built and within the shared-memory limit
   bool want_tiles = true;   // storm_fvt_set_stage_path
   bool use_tiles = false;   // the captured iteration runs k_tile
+  bool fuse_nodes = true;   // k_tile computes the vertex depths (else k_node runs before it)
+  int32_t* bc_nodes = nullptr;  // vertices of the boundary cells (device, in tile_buf)
+  int n_bc_nodes = 0;
   double *u_a2 = nullptr, *v_a2 = nullptr;
 };
 
@@ -145,15 +147,14 @@ T* at(void* base, size_t off) {
 enum { KT_NODE = 0, KT_GRAD, KT_BC, KT_FLUX, KT_FRIC, KT_FINAL, KT_EFLUX, KT_TILE, KT_COUNT };
 static_assert(KT_COUNT <= 8, "per-class timing arrays hold 8 classes");
 
-constexpr int kTileCellsHost = 256;   // k_tile's tile (kTileCells in fvt_kernels.cu)
+constexpr int kTileCellsHost = 256;   // cell slots per tile of k_tile
 constexpr int kTileThreadsHost = 256;
 
 int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
   const Dev& d = h->d;
-  const int T = d.T, N = d.N, K = d.K;
+  const int T = d.T, K = d.K;
   const int gT = (T + h->bs_grad - 1) / h->bs_grad;
   const int gF = (T + h->bs_flux - 1) / h->bs_flux;
-  const int gN = (N + h->bs_node - 1) / h->bs_node;
   const int gE = (d.ne + h->bs_eflux - 1) / h->bs_eflux;
   // in timing mode every launch is bracketed by an event pair tagged with its class
   auto mark = [&](int cls) -> int {
@@ -209,16 +210,21 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
       u_out = (s & 1) ? h->u_a2 : d.u_a;
       v_out = (s & 1) ? h->v_a2 : d.v_a;
     }
-    if (mark(KT_NODE)) return STORM_ERR_CUDA;
-    k_node<<<gN, h->bs_node, 0, h->stream>>>(d, hs, dry);
-    if (done()) return STORM_ERR_CUDA;
+    const bool tile_nodes = fused && h->td.nodes;
+    if (!tile_nodes) {
+      if (mark(KT_NODE)) return STORM_ERR_CUDA;
+      launch_node(d, hs, dry, nullptr, 0, h->bs_node, h->stream);
+      if (done()) return STORM_ERR_CUDA;
+    }
     if (fused) {
       const int nt = h->tile_grid;
       if (gB > 0 && !timing) {
-        // the boundary cells' gradients and k_bc on the side stream beside k_tile;
-        // k_flux_bc updates those cells once both are done
+        // the boundary cells' vertex depths (when the tiles compute the others), their
+        // gradients and k_bc on the side stream beside k_tile; k_flux_bc updates those
+        // cells once both are done
         CK(cudaEventRecord(h->fork_ev[s], h->stream));
         CK(cudaStreamWaitEvent(h->side, h->fork_ev[s], 0));
+        if (tile_nodes) launch_node(d, hs, dry, h->bc_nodes, h->n_bc_nodes, 128, h->side);
         launch(STAGE_GRAD_BC, gB, kFluxThreads, 0, h->side, s, hs, dry, dry_next);
         if (d.nbdr > 0) launch(STAGE_BC, d.nbdr, 128, h->bc_smem, h->side, s, hs, dry, dry_next);
         CK(cudaEventRecord(h->join_ev[s], h->side));
@@ -227,6 +233,11 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
         launch(STAGE_FLUX_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
       } else {
         if (gB > 0) {
+          if (tile_nodes) {
+            if (mark(KT_NODE)) return STORM_ERR_CUDA;
+            launch_node(d, hs, dry, h->bc_nodes, h->n_bc_nodes, 128, h->stream);
+            if (done()) return STORM_ERR_CUDA;
+          }
           if (mark(KT_GRAD)) return STORM_ERR_CUDA;
           launch(STAGE_GRAD_BC, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
           if (done()) return STORM_ERR_CUDA;
@@ -347,6 +358,22 @@ void release(StormFvtHandle* h) {
   delete h;
 }
 
+// Shared memory and persistent grid of k_tile for the chosen variant (vertex depths in
+// the tile or by k_node).
+int configure_tiles(StormFvtHandle* h) {
+  TileDev& t = h->td;
+  t.nodes = h->fuse_nodes ? 1 : 0;
+  const size_t smem = tile_smem_bytes(t, h->mixed);
+  h->tile_smem = smem;
+  if (smem > 48 * 1024) set_tile_smem_limit((int)smem);
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+  const int per_sm = std::max(1, tile_blocks_per_sm(h->mixed, smem));
+  h->tile_grid = std::max(1, std::min(t.ntiles, nsm * per_sm));
+  CK(cudaGetLastError());
+  return 0;
+}
+
 // The tile plan of the fused stage kernel and its device copy.  A mesh whose tiles do
 // not fit (more than 65,534 local cells or edges, or more shared memory than a block
 // may have) keeps the phase kernels.
@@ -359,7 +386,8 @@ int upload_tiles(StormFvtHandle* h) {
   }
   TileDev& t = h->td;
   t.tc = P.tc; t.ntiles = P.ntiles; t.kst = P.kst;
-  t.ns_max = P.ns_max; t.ng_max = P.ng_max; t.ne_max = P.ne_max;
+  t.ns_max = P.ns_max; t.ng_max = P.ng_max; t.ne_max = P.ne_max; t.nn_max = P.nn_max;
+  t.nodes = 1;
   const size_t smem = tile_smem_bytes(t, h->mixed);
   int dev_max = 0;
   CK(cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
@@ -383,6 +411,8 @@ int upload_tiles(StormFvtHandle* h) {
   const size_t o_info = cpy(P.info), o_halo = cpy(P.halo), o_h1t3 = cpy(P.h1_t3), o_h1st = cpy(P.h1_st);
   const size_t o_lt3 = cpy(P.lt3), o_lst = cpy(P.lst), o_lfe = cpy(P.lfe), o_eloc = cpy(P.eloc);
   const size_t o_be = cpy(P.be), o_beloc = cpy(P.beloc);
+  const size_t o_tn = cpy(P.tnode), o_tns = cpy(P.tn_start), o_tno = cpy(P.tn_own), o_tnc = cpy(P.tn_cells);
+  const size_t o_lvt = cpy(P.lvt), o_h1vt = cpy(P.h1_vt), o_lw = cpy(P.lwall), o_bcn = cpy(P.bc_nodes);
   cudaError_t e = cudaMalloc(&h->tile_buf, A.off);
   if (e != cudaSuccess)
     return set_error(e == cudaErrorMemoryAllocation ? STORM_ERR_NOMEM : STORM_ERR_CUDA,
@@ -393,17 +423,17 @@ int upload_tiles(StormFvtHandle* h) {
   t.h1_t3 = at<uint16_t>(B, o_h1t3); t.h1_st = at<uint16_t>(B, o_h1st);
   t.lt3 = at<uint16_t>(B, o_lt3); t.lst = at<uint16_t>(B, o_lst); t.lfe = at<uint16_t>(B, o_lfe);
   t.eloc = at<uint32_t>(B, o_eloc); t.be = at<int32_t>(B, o_be); t.beloc = at<uint32_t>(B, o_beloc);
-  h->tile_smem = smem;
-  if (smem > 48 * 1024) set_tile_smem_limit((int)smem);
-  int nsm = 0;
-  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
-  const int per_sm = std::max(1, tile_blocks_per_sm(h->mixed, smem));
-  h->tile_grid = std::max(1, std::min(P.ntiles, nsm * per_sm));
-  CK(cudaGetLastError());
+  t.tnode = at<int32_t>(B, o_tn); t.tn_start = at<int32_t>(B, o_tns); t.tn_own = at<uint8_t>(B, o_tno);
+  t.tn_cells = at<uint16_t>(B, o_tnc); t.lvt = at<uint16_t>(B, o_lvt); t.h1_vt = at<uint16_t>(B, o_h1vt);
+  t.lwall = at<uint32_t>(B, o_lw);
+  h->bc_nodes = at<int32_t>(B, o_bcn);
+  h->n_bc_nodes = h->L.bc_cells.empty() ? 0 : (int)P.bc_nodes.size();
   // the host copy of the plan is not needed after the upload
   P.halo = {}; P.h1_t3 = {}; P.h1_st = {}; P.lt3 = {}; P.lst = {}; P.lfe = {}; P.eloc = {}; P.be = {}; P.beloc = {};
+  P.tnode = {}; P.tn_start = {}; P.tn_own = {}; P.tn_cells = {}; P.lvt = {}; P.h1_vt = {}; P.lwall = {};
+  P.bc_nodes = {};
   h->tiles_ok = true;
-  return 0;
+  return configure_tiles(h);
 }
 
 int upload(StormFvtHandle* h) {
@@ -1243,11 +1273,16 @@ int storm_fvt_autotune(StormFvtHandle* h, int32_t iters, int32_t* chosen) {
 int storm_fvt_set_stage_path(StormFvtHandle* h, int32_t path) {
   clear_error();
   if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_set_stage_path: null handle");
-  if (path != STORM_STAGE_PHASES && path != STORM_STAGE_FUSED)
-    return set_error(STORM_ERR_ARG, "storm_fvt_set_stage_path: path must be STORM_STAGE_PHASES or STORM_STAGE_FUSED");
+  if (path != STORM_STAGE_PHASES && path != STORM_STAGE_FUSED && path != STORM_STAGE_FUSED_NODE_KERNEL)
+    return set_error(STORM_ERR_ARG, "storm_fvt_set_stage_path: unknown path");
   CK(cudaSetDevice(h->device));
   CK(cudaStreamSynchronize(h->stream));
-  h->want_tiles = path == STORM_STAGE_FUSED;
+  h->want_tiles = path != STORM_STAGE_PHASES;
+  h->fuse_nodes = path == STORM_STAGE_FUSED;
+  if (h->tiles_ok) {
+    int rc = configure_tiles(h);
+    if (rc) return rc;
+  }
   if (h->exec) cudaGraphExecDestroy(h->exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   h->exec = nullptr;
@@ -1256,7 +1291,8 @@ int storm_fvt_set_stage_path(StormFvtHandle* h, int32_t path) {
 }
 
 int32_t storm_fvt_stage_path(const StormFvtHandle* h) {
-  return (h && h->use_tiles) ? STORM_STAGE_FUSED : STORM_STAGE_PHASES;
+  if (!h || !h->use_tiles) return STORM_STAGE_PHASES;
+  return h->td.nodes ? STORM_STAGE_FUSED : STORM_STAGE_FUSED_NODE_KERNEL;
 }
 
 int storm_fvt_tile_check(const StormFvtMesh* const* meshes, int32_t n, int32_t tile_cells, int64_t* stats) {

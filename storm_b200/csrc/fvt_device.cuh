@@ -121,7 +121,8 @@ struct Geo {
 
 // Device view of the tile plan of the fused stage kernel (TilePlan in storm_internal.h).
 struct TileDev {
-  int32_t tc, ntiles, kst, ns_max, ng_max, ne_max;
+  int32_t tc, ntiles, kst, ns_max, ng_max, ne_max, nn_max;
+  int32_t nodes;                       // the tile computes its vertex depths (else k_node does)
   const int32_t* info;                 // [ntiles][TI_N]
   const int32_t* halo;                 // H1 then H2 slots per tile
   const uint16_t *h1_t3, *h1_st;       // local topology of the H1 cells
@@ -129,6 +130,11 @@ struct TileDev {
   const uint32_t* eloc;                // [ne] local L | R << 16 (range edges)
   const int32_t* be;                   // back edges
   const uint32_t* beloc;               // their local L | R << 16
+  const int32_t *tnode, *tn_start;     // nodes per tile; start of their incident cells in tn_cells
+  const uint8_t* tn_own;               // the tile writes the node's depth out
+  const uint16_t* tn_cells;            // local incident cells (n2t order)
+  const uint16_t *lvt, *h1_vt;         // local vertex ids of owned / H1 cells
+  const uint32_t* lwall;               // [3][T] local ends of wall faces
 };
 
 // One launch of a templated stage kernel (see launch_stage in fvt_kernels.cu).
@@ -164,6 +170,9 @@ void launch_link_dt(const Dev& d, cudaStream_t st);
 // Friction, hvalve and the iteration partials (halo cells left out when linked).
 void launch_fric(const Dev& d, const double* u_src, const double* v_src, cudaStream_t st);
 void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st);
+// k_node over every node (list == nullptr) or the n listed nodes
+void launch_node(const Dev& d, const double* hs, const uint8_t* dry, const int32_t* list, int n, int block,
+                 cudaStream_t st);
 
 // The output pass (to_vertices, ctr2vtx of cd, error_est(2)) after an iteration.
 struct OutputArgs {

@@ -435,20 +435,21 @@ __global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int sid) {
 }
 
 // ---------------------------------------------------------------------------
-// Vertex water surface and depth of one stage.
-__global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= d.N) return;
-  const int sid = d.node_sid[n];
-  if (d.sc[sid].converged) return;
-  const int b0 = d.n2t_off[n], b1 = d.n2t_off[n + 1];
+// Vertex water surface and depth of one stage (to_vertices.f90:26-41: ctr2vtxWSE type
+// 3, cap at the highest wet neighbour, positivity_vtx; enforce_bcs.f90:37-56 for the
+// stage nodes).  cell(q, &dry, &h, &z) gives the q-th incident cell (n2t order).
+template <class CellF>
+__device__ __forceinline__ void node_depth(const Dev& d, int n, int b0, int b1, CellF cell, double* hv_out,
+                                           bool* wet_out) {
   const double zv0 = d.zvtx[n];
   double id = kZero, a = kZero, zetaref = zv0;
   int counter = 0;
   for (int q = b0; q < b1; q++) {
-    const int k = d.n2t_cell[q];
-    if (dry[k]) continue;
-    const double zeta = hs[k] + d.z[k];
+    bool dk;
+    double hk, zk;
+    cell(q, &dk, &hk, &zk);
+    if (dk) continue;
+    const double zeta = hk + zk;
     const double w = d.n2t_w[q];
     counter++;
     id = id + w;
@@ -459,9 +460,38 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ 
   zv = fmin2(zv, zetaref);
   double hv = zv - zv0;
   if (hv < kZero) hv = kZero;
-  d.vwet[n] = hv > d.h_dry;
+  *wet_out = hv > d.h_dry;
   const int b = d.node_hbc[n];
-  if (b >= 0) hv = fmax2(kZero, d.sc[sid].hbc[b] - zv0);
+  if (b >= 0) hv = fmax2(kZero, d.sc[d.node_sid[n]].hbc[b] - zv0);
+  *hv_out = hv;
+}
+
+// Every node, or the listed nodes (the vertices of the cells with an open-boundary
+// face, ahead of their gradients on the side stream of the fused path).
+__global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry,
+                                              const int32_t* __restrict__ list, int nlist) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int n;
+  if (list) {
+    if (i >= nlist) return;
+    n = list[i];
+  } else {
+    if (i >= d.N) return;
+    n = i;
+  }
+  const int sid = d.node_sid[n];
+  if (d.sc[sid].converged) return;
+  double hv;
+  bool wet;
+  node_depth(d, n, d.n2t_off[n], d.n2t_off[n + 1],
+             [&](int q, bool* dk, double* hk, double* zk) {
+               const int k = d.n2t_cell[q];
+               *dk = dry[k] != 0;
+               *hk = hs[k];
+               *zk = d.z[k];
+             },
+             &hv, &wet);
+  d.vwet[n] = wet;
   d.hvtx[n] = hv;
 }
 
@@ -544,15 +574,12 @@ struct GradOut {
   bool fix;  // hgradfix2 set the gradient: the previous RK level's momentum is zeroed
 };
 
-template <class R, class NB, class ST>
+template <class R, class NB, class ST, class VW>
 __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>& G, const NB& nb, int c, int self,
-                                                     const int (&t3)[3], ST st, R* rcx, R* rcy) {
+                                                     const int (&t3)[3], ST st, VW vwet, R* rcx, R* rcy) {
   const int T = d.T;
   const double zeta_c = nb.H(self) + nb.Z(self);
   const double u_c = nb.U(self), v_c = nb.V(self);
-  int vt[3];
-#pragma unroll
-  for (int j = 0; j < 3; j++) vt[j] = d.vert[(size_t)j * T + c];
   const bool dry_c = nb.D(self);
   R hx = R(0), hy = R(0), ux = R(0), uy = R(0), vx = R(0), vy = R(0);
   if (d.lim == 1 || d.lim == 2) {
@@ -658,7 +685,7 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
     // to_vertices.f90:44-55
     bool flag = true;
 #pragma unroll
-    for (int j = 0; j < 3; j++) flag = flag && d.vwet[vt[j]];
+    for (int j = 0; j < 3; j++) flag = flag && vwet(j);
     if (!flag) {
       ub = kZero;
       vb = kZero;
@@ -694,6 +721,7 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
 #pragma unroll
   for (int j = 0; j < 3; j++) t3[j] = d.t2t3[(size_t)j * T + c];
   const GradOut<R> g = cell_gradients<R>(d, G, nb, c, c, t3, [&](int k) { return d.st_id[(size_t)k * T + c]; },
+                                         [&](int j) { return d.vwet[d.vert[(size_t)j * T + c]] != 0; },
                                          (R*)nullptr, (R*)nullptr);
   if (g.fix) {
     rku_prev[c] = kZero;
@@ -1314,6 +1342,12 @@ struct FacesGlobal {
     *x = G.delh_x[c];
     *y = G.delh_y[c];
   }
+  // vertex depths at the two ends (walledg1 order) of the wall face in slot j
+  __device__ __forceinline__ void hwall(int j, double* h1, double* h2) const {
+    const int w = d.fref[(size_t)j * d.T + c];
+    *h1 = d.hvtx[d.wall_p1[w]];
+    *h2 = d.hvtx[d.wall_p2[w]];
+  }
 };
 
 // ... or a tile's shared memory (k_tile): edge fluxes by local edge, face states and
@@ -1326,6 +1360,24 @@ struct FacesTile {
   const uint8_t* seok;     // [nem]
   const double *sfh, *sfu, *sfv;  // [3][ngm]
   const R *sdhx, *sdhy;    // [owned]
+  const uint32_t* __restrict__ lwall;  // [3][T] local node ids of the wall ends
+  const double* shv;       // vertex depths of the tile's nodes
+  const double* __restrict__ hvtx;  // or the global ones (nodes not fused)
+  const int32_t* __restrict__ wall_p1;
+  const int32_t* __restrict__ wall_p2;
+  const int32_t* __restrict__ fref;
+  __device__ __forceinline__ void hwall(int j, double* h1, double* h2) const {
+    const size_t q = (size_t)j * T + c;
+    if (shv) {
+      const uint32_t w = lwall[q];
+      *h1 = shv[w & 0xFFFF];
+      *h2 = shv[w >> 16];
+    } else {
+      const int w = fref[q];
+      *h1 = hvtx[wall_p1[w]];
+      *h2 = hvtx[wall_p2[w]];
+    }
+  }
   __device__ __forceinline__ bool iface(int j, R* f) const {
     const int le = lfe[(size_t)j * T + c];
     f[0] = sf[le];
@@ -1396,8 +1448,8 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, cons
       if (dry_c) continue;
       const double nx = d.fnx[q], ny = d.fny[q], len = d.flen[q];
       if (d.btype == 0) {  // wenslp3_fluxes.f90:34-67
-        const int w = d.fref[q];
-        const double h1 = d.hvtx[d.wall_p1[w]], h2 = d.hvtx[d.wall_p2[w]];
+        double h1, h2;
+        fs.hwall(j, &h1, &h2);
         double hedge = qsqrt((h1 * h1 + h1 * h2 + h2 * h2) * kOneThird);
         if (hedge < kZero) hedge = kZero;
         if (hedge < d.h_dry) continue;
@@ -1631,13 +1683,12 @@ __global__ void __launch_bounds__(128) k_flux_bc(Dev d, Geo<R> G, int s, const d
 // k_flux_bc updates them afterwards.  Velocities ping-pong between two buffers: a
 // tile may still read a neighbour's stage-input velocity while the neighbour's own
 // tile writes its new one.
-constexpr int kTileCells = 256;
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = 256;  // tiles of 256 cell slots (the host's tile plan)
 
 struct TileSmem {
-  size_t h, z, u, v, fh, fu, fv, dhx, dhy, f, dry, eok, total;
+  size_t h, z, u, v, fh, fu, fv, dhx, dhy, f, hv, dry, eok, vw, total;
 };
-__host__ __device__ inline TileSmem tile_smem_layout(int ns, int ng, int ne, int tc, int rsz) {
+__host__ __device__ inline TileSmem tile_smem_layout(int ns, int ng, int ne, int tc, int rsz, int nn) {
   TileSmem m;
   size_t o = 0;
   auto take = [&](size_t bytes) {
@@ -1655,8 +1706,10 @@ __host__ __device__ inline TileSmem tile_smem_layout(int ns, int ng, int ne, int
   m.dhx = take((size_t)rsz * tc);
   m.dhy = take((size_t)rsz * tc);
   m.f = take((size_t)rsz * 3 * ne);
+  m.hv = take(8 * (size_t)nn);
   m.dry = take(ns);
   m.eok = take(ne);
+  m.vw = take(nn);
   m.total = o;
   return m;
 }
@@ -1675,10 +1728,11 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   if (tsid >= 0 && d.sc[tsid].converged) continue;  // uniform over the CTA
   const int nown = I[TI_NOWN], n1 = I[TI_N1], n2 = I[TI_N2], hoff = I[TI_HOFF], h1off = I[TI_H1OFF];
   const int er0 = I[TI_ER0], nr = I[TI_NR], nb = I[TI_NB], boff = I[TI_BOFF];
-  const int nS = nown + n1 + n2, nG = nown + n1, nE = nr + nb;
+  const int noff = I[TI_NOFF], nn = tp.nodes ? I[TI_NN] : 0;
+  const int nS = nown + n1 + n2 + (tp.nodes ? I[TI_N3] : 0), nG = nown + n1, nE = nr + nb;
   const int ngm = tp.ng_max, nem = tp.ne_max;
   const int T = d.T, c0 = t * tp.tc;
-  const TileSmem L = tile_smem_layout(tp.ns_max, ngm, nem, tp.tc, (int)sizeof(R));
+  const TileSmem L = tile_smem_layout(tp.ns_max, ngm, nem, tp.tc, (int)sizeof(R), tp.nodes ? tp.nn_max : 0);
   double* s_h = reinterpret_cast<double*>(tsm + L.h);
   double* s_z = reinterpret_cast<double*>(tsm + L.z);
   double* s_u = reinterpret_cast<double*>(tsm + L.u);
@@ -1691,6 +1745,8 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   R* s_f = reinterpret_cast<R*>(tsm + L.f);
   uint8_t* s_dry = tsm + L.dry;
   uint8_t* s_eok = tsm + L.eok;
+  double* s_hv = reinterpret_cast<double*>(tsm + L.hv);
+  uint8_t* s_vw = tsm + L.vw;
 
   // A: stage-input state of every local cell
   for (int l = threadIdx.x; l < nS; l += blockDim.x) {
@@ -1703,6 +1759,34 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   }
   __syncthreads();
 
+  // A2: vertex depths of the tile's nodes from their incident cells (node_depth, the
+  // arithmetic of k_node); the tile owning a node's first incident cell writes it out
+  if (tp.nodes) {
+    for (int ln = threadIdx.x; ln < nn; ln += blockDim.x) {
+      const int n = tp.tnode[noff + ln];
+      if (d.sc[d.node_sid[n]].converged) continue;
+      const int b0 = d.n2t_off[n], b1 = d.n2t_off[n + 1];
+      const uint16_t* lc = tp.tn_cells + tp.tn_start[noff + ln] - b0;
+      double hv;
+      bool wet;
+      node_depth(d, n, b0, b1,
+                 [&](int q, bool* dk, double* hk, double* zk) {
+                   const int k = lc[q];
+                   *dk = s_dry[k] != 0;
+                   *hk = s_h[k];
+                   *zk = s_z[k];
+                 },
+                 &hv, &wet);
+      s_hv[ln] = hv;
+      s_vw[ln] = wet;
+      if (tp.tn_own[noff + ln]) {
+        d.hvtx[n] = hv;
+        d.vwet[n] = wet;
+      }
+    }
+    __syncthreads();
+  }
+
   // B: gradients and face states of the owned and H1 cells
   const NbShared nbs{s_h, s_z, s_u, s_v, s_dry};
   for (int l = threadIdx.x; l < nG; l += blockDim.x) {
@@ -1711,8 +1795,8 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     const int sid = d.cell_sid[g];
     if (sid < 0 || d.sc[sid].converged) continue;
     int t3[3];
-    const uint16_t* st;
-    size_t sst;
+    const uint16_t *st, *vt;
+    size_t sst, svt;
     if (own) {
 #pragma unroll
       for (int j = 0; j < 3; j++) {
@@ -1721,6 +1805,8 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       }
       st = tp.lst + g;
       sst = (size_t)T;
+      vt = tp.lvt + g;
+      svt = (size_t)T;
     } else {
       const size_t r = (size_t)(h1off + l - nown);
 #pragma unroll
@@ -1730,10 +1816,14 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       }
       st = tp.h1_st + (size_t)tp.kst * r;
       sst = 1;
+      vt = tp.h1_vt + 3 * r;
+      svt = 1;
     }
     R rx[3], ry[3];
-    const GradOut<R> gr = cell_gradients<R>(d, G, nbs, g, l, t3, [&](int k) { return (int)st[(size_t)k * sst]; },
-                                            rx, ry);
+    const GradOut<R> gr = cell_gradients<R>(
+        d, G, nbs, g, l, t3, [&](int k) { return (int)st[(size_t)k * sst]; },
+        [&](int j) { return tp.nodes ? s_vw[vt[(size_t)j * svt]] != 0 : d.vwet[d.vert[(size_t)j * T + g]] != 0; },
+        rx, ry);
     if (d.lim != 2) {
 #pragma unroll
       for (int j = 0; j < 3; j++) {
@@ -1817,7 +1907,8 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     if (d.forder[c] & kOrderHasBc) continue;
     const double h_c = s_h[l];
     const bool dry_c = s_dry[l] != 0;
-    const FacesTile<R> fs{tp.lfe, T, c, l, ngm, nem, s_f, s_eok, s_fh, s_fu, s_fv, s_dhx, s_dhy};
+    const FacesTile<R> fs{tp.lfe, T, c, l, ngm, nem, s_f, s_eok, s_fh, s_fu, s_fv, s_dhx, s_dhy,
+                          tp.lwall, tp.nodes ? s_hv : nullptr, d.hvtx, d.wall_p1, d.wall_p2, d.fref};
     double p1, p2, p3;
     assemble_phi<R>(d, G, fs, c, h_c, dry_c, &p1, &p2, &p3);
     rk_update(d, s, c, h_c, dry_c, p1, p2, p3, dry_next, u_in, v_in, u_out, v_out);
@@ -1827,7 +1918,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 }
 
 size_t tile_smem_bytes(const TileDev& t, bool mixed) {
-  return tile_smem_layout(t.ns_max, t.ng_max, t.ne_max, t.tc, mixed ? 4 : 8).total;
+  return tile_smem_layout(t.ns_max, t.ng_max, t.ne_max, t.tc, mixed ? 4 : 8, t.nodes ? t.nn_max : 0).total;
 }
 
 int tile_blocks_per_sm(bool mixed, size_t smem) {
@@ -2408,6 +2499,12 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed) {
   if (mixed) launch_stage_t<float>(L, d, Gf);
   else launch_stage_t<double>(L, d, Gd);
+}
+
+void launch_node(const Dev& d, const double* hs, const uint8_t* dry, const int32_t* list, int n, int block,
+                 cudaStream_t st) {
+  const int cnt = list ? n : d.N;
+  if (cnt > 0) k_node<<<(cnt + block - 1) / block, block, 0, st>>>(d, hs, dry, list, n);
 }
 
 void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st) {

@@ -110,17 +110,23 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
 // local cells are the owned ones (local id = slot - t*tc), then H1 (face neighbours
 // of owned cells in other tiles: their gradients and face states are recomputed in
 // the tile), then H2 (stencil and face neighbours of H1 cells outside owned and H1:
-// state only).  Its edges are the interior edges whose smaller cell slot is owned (a
-// contiguous range of the edge arrays, sorted by that slot) followed by the "back"
-// edges whose larger slot is owned.  Local ids are 16-bit; kNoLocal marks none.
+// state only), then H3 (the other cells around the tile's nodes: state only).  Its
+// nodes are the vertices of its owned and H1 cells; each node's vertex depth is
+// computed in the tile from its incident cells, and the tile owning the node's
+// smallest incident cell slot writes it out.  Its edges are the interior edges whose
+// smaller cell slot is owned (a contiguous range of the edge arrays, sorted by that
+// slot) followed by the "back" edges whose larger slot is owned.  Local ids are
+// 16-bit; kNoLocal marks none.
 constexpr uint16_t kNoLocal = 0xFFFF;
 constexpr uint8_t kEdgeExport = 0x10;  // eslot flag: the edge has a cell with an open-boundary face
-enum TileInfo { TI_NOWN = 0, TI_N1, TI_N2, TI_HOFF, TI_H1OFF, TI_ER0, TI_NR, TI_NB, TI_BOFF, TI_SID, TI_N };
+enum TileInfo { TI_NOWN = 0, TI_N1, TI_N2, TI_HOFF, TI_H1OFF, TI_ER0, TI_NR, TI_NB, TI_BOFF, TI_SID,
+                TI_N3, TI_NOFF, TI_NN, TI_N };
 struct TilePlan {
   int32_t tc = 0, ntiles = 0, kst = 0;
   int32_t ns_max = 0, ng_max = 0, ne_max = 0;  // largest local cell, gradient and edge counts
+  int32_t nn_max = 0;                           // largest node count
   std::vector<int32_t> info;    // [ntiles][TI_N]; TI_SID: the tile's one scenario, or -1 if several
-  std::vector<int32_t> halo;    // global slots of H1 then H2, per tile from info[TI_HOFF]
+  std::vector<int32_t> halo;    // global slots of H1, H2 then H3, per tile from info[TI_HOFF]
   std::vector<uint16_t> h1_t3;  // [sum n1][3]   local t2t3 of the H1 cells
   std::vector<uint16_t> h1_st;  // [sum n1][kst] local stencil of the H1 cells
   std::vector<uint16_t> lt3;    // [3][T]   local t2t3 of every cell in its own tile
@@ -129,6 +135,15 @@ struct TilePlan {
   std::vector<uint32_t> eloc;   // [ne]     local L | R << 16 of each edge in the tile of its smaller slot
   std::vector<int32_t> be;      // back edges (global edge ids), per tile from info[TI_BOFF]
   std::vector<uint32_t> beloc;  // local L | R << 16 of each back edge
+  // nodes, per tile from info[TI_NOFF]: global id, whether this tile writes its depth
+  // out, and where its incident cells (local ids, in the n2t order) start in tn_cells
+  std::vector<int32_t> tnode, tn_start;
+  std::vector<uint8_t> tn_own;
+  std::vector<uint16_t> tn_cells;
+  std::vector<uint16_t> lvt;    // [3][T]   local vertex ids of every cell in its own tile
+  std::vector<uint16_t> h1_vt;  // [sum n1][3] local vertex ids of the H1 cells
+  std::vector<uint32_t> lwall;  // [3][T]   local p1 | p2 << 16 of each wall face in its own tile
+  std::vector<int32_t> bc_nodes;  // vertices of the cells with an open-boundary face
 };
 // Returns 0, or -1 when a tile needs more than 65,534 local cells or edges.
 int build_tiles(const HostLayout& L, int tc, TilePlan& P);

@@ -34,7 +34,7 @@ EXPORTS = (
 )
 
 KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux", "tile")
-STAGE_PHASES, STAGE_FUSED = 0, 1
+STAGE_PHASES, STAGE_FUSED, STAGE_FUSED_NODE_KERNEL = 0, 1, 2
 
 
 class StormError(RuntimeError):

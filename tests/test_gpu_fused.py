@@ -18,7 +18,7 @@ def _bits(a):
 
 def _run(pm, opts, sc, path, steps):
     g = fvt.Solver(pm, opts, keep=pm)
-    if path == fvt.STAGE_PHASES:
+    if path != fvt.STAGE_FUSED:
         g.set_stage_path(path)
     assert g.stage_path() == path
     g.set_state(sc.h0, sc.u0, sc.v0)
@@ -38,11 +38,12 @@ def _run(pm, opts, sc, path, steps):
     ("dambreak", lambda: scenarios.dambreak(n_target=30_000, seed=4), 40),
 ])
 @pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
-def test_fused_equals_phases(name, make, steps, precision, storm_lib):
+@pytest.mark.parametrize("fused", [fvt.STAGE_FUSED, fvt.STAGE_FUSED_NODE_KERNEL])
+def test_fused_equals_phases(name, make, steps, precision, fused, storm_lib):
     sc = make()
     sc.options.precision = precision
     pm = fvt.build_mesh(sc.problem)
-    (a, sa) = _run(pm, sc.options, sc, fvt.STAGE_FUSED, steps)
+    (a, sa) = _run(pm, sc.options, sc, fused, steps)
     (b, sb) = _run(pm, sc.options, sc, fvt.STAGE_PHASES, steps)
     for k in ("h", "u", "v", "rkh", "rku", "rkv", "hvtx"):
         if not np.array_equal(_bits(a[k]), _bits(b[k])):
