@@ -690,7 +690,8 @@ def main():
     solver = fvt.Solver(pm, sc.options, keep=pm)
     if args.stage_path == "phases":
         solver.set_stage_path(fvt.STAGE_PHASES)
-    path_used = "fused" if solver.stage_path() == fvt.STAGE_FUSED else "phases"
+    path_used = {fvt.STAGE_PHASES: "phases", fvt.STAGE_FUSED: "fused",
+                 fvt.STAGE_FUSED_NODE_KERNEL: "fused-node-kernel"}[solver.stage_path()]
     setup = {"mesh_build_s": mesh_ratios.build_s, "create_s": time.perf_counter() - t0,
              "what": "storm_fvt_mesh_build (topology, edges, walls, boundary arrays, LSQ and IDW set-up: "
                      "read_data + dataprepFVT, host C++) and storm_fvt_create (layout, upload, graph capture)"}
@@ -769,29 +770,36 @@ def main():
         }
         s2.close()
 
-    # ---- the other stage path on the same mesh: speed and bitwise agreement ----
+    # ---- the other stage paths on the same mesh: speed and bitwise agreement ----
     ab = None
     if args.ab_steps > 0:
         n_ab = max(1, min(args.steps, args.ab_steps))
-        other_path = fvt.STAGE_PHASES if path_used == "fused" else fvt.STAGE_FUSED
-        s3 = fvt.Solver(pm, sc.options, keep=pm)
-        s3.set_stage_path(other_path)
-        if s3.stage_path() == other_path:
-            finals = []
-            for sv in (solver, s3):
-                sv.set_state(sc.h0, sc.u0, sc.v0)
-                sv.step(args.warmup)
+        names = {fvt.STAGE_PHASES: "phases", fvt.STAGE_FUSED: "fused",
+                 fvt.STAGE_FUSED_NODE_KERNEL: "fused, vertex depths by k_node"}
+        solver.set_state(sc.h0, sc.u0, sc.v0)
+        solver.step(args.warmup)
+        barrier()
+        solver.step(n_ab)
+        barrier()
+        ms_this, st_this = solver.last_timing()["step_ms"], solver.state()
+        ab = {"steps": n_ab, "this_path_ms_per_step": ms_this / n_ab, "others": []}
+        for other_path in names:
+            if other_path == solver.stage_path():
+                continue
+            s3 = fvt.Solver(pm, sc.options, keep=pm)
+            s3.set_stage_path(other_path)
+            if s3.stage_path() == other_path:
+                s3.set_state(sc.h0, sc.u0, sc.v0)
+                s3.step(args.warmup)
                 barrier()
-                sv.step(n_ab)
+                s3.step(n_ab)
                 barrier()
-                finals.append((sv.last_timing()["step_ms"], sv.state()))
-            same = all(np.array_equal(finals[0][1][k].view(np.uint64), finals[1][1][k].view(np.uint64))
-                       for k in ("h", "u", "v", "rku", "rkv", "hvtx"))
-            ab = {"stage_kernels": "phases" if path_used == "fused" else "fused", "steps": n_ab,
-                  "ms_per_step": finals[1][0] / n_ab, "this_path_ms_per_step": finals[0][0] / n_ab,
-                  "value": T * K_rk * n_ab / (finals[1][0] / 1e3),
-                  "bitwise_equal_states": bool(same)}
-        s3.close()
+                ms3, st3 = s3.last_timing()["step_ms"], s3.state()
+                same = all(np.array_equal(st_this[k].view(np.uint64), st3[k].view(np.uint64))
+                           for k in ("h", "u", "v", "rku", "rkv", "hvtx"))
+                ab["others"].append({"stage_kernels": names[other_path], "ms_per_step": ms3 / n_ab,
+                                     "value": T * K_rk * n_ab / (ms3 / 1e3), "bitwise_equal_states": bool(same)})
+            s3.close()
 
     # ---- per-kernel timing pass (roofline of the RK-stage kernel chain) ----
     solver.set_state(sc.h0, sc.u0, sc.v0)
@@ -814,8 +822,9 @@ def main():
     traffic = None
     if (args.config, path_used) in NCU_DRAM_BYTES_PER_CELL_STAGE:
         traffic = NCU_DRAM_BYTES_PER_CELL_STAGE[(args.config, path_used)] * T * K_rk
-    chain = ("K x [k_node, k_grad(boundary cells) -> k_bc || k_tile, k_flux_bc]" if path_used == "fused"
-             else "K x [k_node, k_grad, k_bc || k_eflux, k_flux, k_flux_bc]")
+    chain = {"fused": "K x [k_node(boundary-cell vertices) -> k_grad(boundary cells) -> k_bc || k_tile, k_flux_bc]",
+             "fused-node-kernel": "K x [k_node, k_grad(boundary cells) -> k_bc || k_tile, k_flux_bc]",
+             "phases": "K x [k_node, k_grad, k_bc || k_eflux, k_flux, k_flux_bc]"}[path_used]
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
         "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
@@ -825,7 +834,7 @@ def main():
                           "per cell-stage, scaled to this mesh" if traffic else None,
         "achieved_serialised_stage_chain": achieved_serial,
         "kernel_ms_share": {k: round(v[0] / iter_ms, 4) for k, v in kt.items()},
-        "stage_kernel_avg_ms": (kt["tile"][0] / max(1, kt["tile"][1]) if path_used == "fused"
+        "stage_kernel_avg_ms": (kt["tile"][0] / max(1, kt["tile"][1]) if path_used != "phases"
                                 else kt["flux"][0] / max(1, kt["flux"][1])),
     }
 
