@@ -1766,12 +1766,12 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       const int n = tp.tnode[noff + ln];
       if (d.sc[d.node_sid[n]].converged) continue;
       const int b0 = d.n2t_off[n], b1 = d.n2t_off[n + 1];
-      const uint16_t* lc = tp.tn_cells + tp.tn_start[noff + ln] - b0;
+      const int base = tp.tn_start[noff + ln] - b0;  // tn_cells[base + q] for q in [b0, b1)
       double hv;
       bool wet;
       node_depth(d, n, b0, b1,
                  [&](int q, bool* dk, double* hk, double* zk) {
-                   const int k = lc[q];
+                   const int k = tp.tn_cells[base + q];
                    *dk = s_dry[k] != 0;
                    *hk = s_h[k];
                    *zk = s_z[k];
