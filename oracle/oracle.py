@@ -52,6 +52,19 @@ def lib():
             [C.POINTER(C.c_double)] * 4
         L.orc_output_vertices.argtypes = [C.c_void_p, C.POINTER(abi.OutputBoundary), C.c_int] + \
             [C.POINTER(C.c_double)] * 5
+        dp = C.POINTER(C.c_double)
+        L.orc_iter_begin.argtypes = [C.c_void_p, dp]
+        L.orc_iter_set_dt.argtypes = [C.c_void_p, C.c_double]
+        L.orc_iter_set_dt.restype = None
+        L.orc_iter_stage.argtypes = [C.c_void_p, C.c_int, dp, C.POINTER(C.c_int)]
+        L.orc_iter_fric.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_uint8), dp]
+        L.orc_iter_finish.argtypes = [C.c_void_p, dp, C.POINTER(abi.StepStats)]
+        L.orc_get_level.argtypes = [C.c_void_p, C.c_int, dp]
+        L.orc_put_level.argtypes = [C.c_void_p, C.c_int, C.c_int32, C.POINTER(C.c_int32), dp]
+        L.orc_set_bch_max.argtypes = [C.c_void_p, C.c_double]
+        L.orc_set_bch_max.restype = None
+        L.orc_get_bch_max.argtypes = [C.c_void_p]
+        L.orc_get_bch_max.restype = C.c_double
         _lib = L
     return _lib
 
@@ -131,6 +144,48 @@ class Oracle:
         d = np.empty(self.T, dtype=np.int32)
         _chk(lib().orc_get_drycell(self._h, abi.iptr(d)))
         return d
+
+    # ---- one iteration in steps (one part of a mesh split over processes) ----
+    def iter_begin(self) -> float:
+        dt = C.c_double()
+        _chk(lib().orc_iter_begin(self._h, C.byref(dt)))
+        return dt.value
+
+    def iter_set_dt(self, dt: float):
+        lib().orc_iter_set_dt(self._h, float(dt))
+
+    def iter_stage(self, rkstep: int) -> float:
+        d, bad = C.c_double(), C.c_int(0)
+        _chk(lib().orc_iter_stage(self._h, int(rkstep), C.byref(d), C.byref(bad)))
+        return d.value
+
+    def iter_fric(self, dt: float, owned: np.ndarray) -> np.ndarray:
+        own = np.ascontiguousarray(owned, dtype=np.uint8)
+        sums = np.zeros(4)
+        _chk(lib().orc_iter_fric(self._h, float(dt), own.ctypes.data_as(C.POINTER(C.c_uint8)), abi.dptr(sums)))
+        return sums
+
+    def iter_finish(self, sums) -> dict:
+        s = np.ascontiguousarray(sums, dtype=np.float64)
+        st = abi.StepStats()
+        _chk(lib().orc_iter_finish(self._h, abi.dptr(s), C.byref(st)))
+        return st.as_dict()
+
+    def get_level(self, level: int) -> np.ndarray:
+        out = np.empty((6, self.T))
+        _chk(lib().orc_get_level(self._h, int(level), abi.dptr(out)))
+        return out
+
+    def put_level(self, level: int, elems, values):
+        e = np.ascontiguousarray(elems, dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        _chk(lib().orc_put_level(self._h, int(level), len(e), abi.iptr(e), abi.dptr(v)))
+
+    def set_bch_max(self, v: float):
+        lib().orc_set_bch_max(self._h, float(v))
+
+    def bch_max(self) -> float:
+        return float(lib().orc_get_bch_max(self._h))
 
     def stage_probe(self, rkstep: int = 1, upto: int = 4) -> dict:
         T, N = self.T, self.N

@@ -2292,6 +2292,149 @@ int orc_step(orc_t* o, int nsteps, StormFvtStepStats* st) {
   return 0;
 }
 
+/* ---- one iteration in steps, for one part of a mesh split over processes ----------
+ * orc_step's iteration cut where a part's halo takes its owners' values and where the
+ * parts agree on dt and on the stop test; the caller does the exchanges between the
+ * calls.  orc_iter_begin returns this part's CFL minimum (unsteady, dt_op = 1: the
+ * global dt is the minimum over the parts) or the dt the part would use. */
+int orc_iter_begin(orc_t* o, double* dt_local) {
+  if (!o->have_state) return set_err(STORM_ERR_ARG, "state not set");
+  const int32_t T = o->n_elems;
+  const StormFvtOptions* op = &o->opt;
+  const int K = op->rkorder;
+  o->iter++;
+  for (int32_t i = 1; i <= T; i++) { RKU(i, 0) = RKU(i, K); RKV(i, 0) = RKV(i, K); RKH(i, 0) = RKH(i, K); }
+  if (!op->steady) {
+    if (op->dt_op == 0) o->delt = op->cfl;
+    else {
+      for (int32_t i = 1; i <= T; i++) ZETA(i) = H(i) + Z(i);
+      find_dry_cells(o);
+      wave_celerity(o);
+      o->delt = deltat_fvt(o, op->cfl);
+    }
+  }
+  *dt_local = o->delt;
+  return 0;
+}
+
+/* The iteration's dt (unsteady: the minimum over the parts); advances ttime as
+ * orc_step does before its stages. */
+void orc_iter_set_dt(orc_t* o, double delt) {
+  if (!o->opt.steady) o->delt = delt;
+  o->ttime = o->ttime + o->delt;
+}
+
+/* RK stage `rkstep`; *delt_out: steady, the local dt of this part's last element (the
+ * friction dt when that element is element n_elems of the whole mesh). */
+int orc_iter_stage(orc_t* o, int rkstep, double* delt_out, int* bad) {
+  if (rkstep < 1 || rkstep > o->opt.rkorder) return set_err(STORM_ERR_ARG, "bad rkstep");
+  *bad |= rk_stage(o, rkstep, 5, &o->delt);
+  *delt_out = o->delt;
+  return 0;
+}
+
+/* Friction with dt `delt` (steady: the whole mesh's element n_elems dt), the valve,
+ * and this part's sums over its owned cells: sums[0..3] = sum (h - h0)^2, sum h0^2,
+ * sum h*area, max |phi| (owned[i] != 0: element i+1 is owned). */
+int orc_iter_fric(orc_t* o, double delt, const uint8_t* owned, double* sums) {
+  const int32_t T = o->n_elems;
+  const StormFvtOptions* op = &o->opt;
+  o->delt = delt;
+  find_dry_cells(o);
+  fric_terms_impl(o, o->delt);
+  double sumtop = zero, sumbot = zero;
+  for (int32_t i = 1; i <= T; i++) {
+    if (!owned[i - 1]) continue;
+    sumtop = sumtop + (H(i) - RKH(i, 0)) * (H(i) - RKH(i, 0));
+    sumbot = sumbot + RKH(i, 0) * RKH(i, 0);
+  }
+  if (op->hvalve)
+    for (int32_t j = 1; j <= o->n_bcedges; j++) {
+      if (!o->hbar[j - 1]) continue;
+      int32_t k = o->bcedges[j - 1];
+      int32_t i = EE(k, 1) < 1 ? EE(k, 2) : EE(k, 1);
+      int m = local_edge(o, i, k);
+      double ksign = GE(i, m) >= 0 ? one : -one;
+      double dotprod = ksign * (U(i) * ENRM(k, 1) + V(i) * ENRM(k, 2));
+      if (dotprod < 0) { U(i) = zero; V(i) = zero; }
+    }
+  for (int32_t i = 1; i <= T; i++)
+    if (DRY(i)) { PHI(i, 1) = zero; PHI(i, 2) = zero; PHI(i, 3) = zero; }
+  double rmax_phi = zero, tmass = zero;
+  for (int32_t i = 1; i <= T; i++) {
+    if (!owned[i - 1]) continue;
+    rmax_phi = fmax2(fmax2(fmax2(rmax_phi, fabs(PHI(i, 1))), fabs(PHI(i, 2))), fabs(PHI(i, 3)));
+    tmass = tmass + H(i) * AREA(i);
+  }
+  sums[0] = sumtop;
+  sums[1] = sumbot;
+  sums[2] = tmass;
+  sums[3] = rmax_phi;
+  return 0;
+}
+
+/* The iteration's scalars from the sums over all parts (as orc_iter_fric's), the
+ * stop test and the boundary time series, as the end of orc_step's iteration. */
+int orc_iter_finish(orc_t* o, const double* sums, StormFvtStepStats* st) {
+  const StormFvtOptions* op = &o->opt;
+  double sb = sums[1];
+  if (equals(sb, zero)) sb = one;
+  o->rms = sqrt(sums[0] / sb);
+  o->tmass = sums[2];
+  if (op->steady) {
+    o->rmax = (op->stop_cr == 0) ? sums[3] : o->rms;
+    o->stime = (double)o->iter;
+    if (o->rmax < op->rstop) o->converged = 1;
+  } else {
+    o->stime = o->stime + o->delt;
+    o->rmax = sums[3];
+    for (int32_t b = 0; b < o->n_in; b++) o->qin_it[b] = o->qin[b];
+    for (int32_t b = 0; b < o->n_out; b++) o->hbc_it[b] = o->hbc[b];
+    get_time_bcs(o, o->stime);
+  }
+  if (st) {
+    memset(st, 0, sizeof *st);
+    st->iter = o->iter; st->converged = o->converged; st->ttime = o->ttime; st->stime = o->stime;
+    st->delt = o->delt; st->rmax = o->rmax; st->rms_dh = o->rms; st->tmass = o->tmass;
+    for (int b = 0; b < STORM_MAX_BDR; b++) { st->cqin3[b] = o->cqin3[b]; st->cqout3[b] = o->cqout3[b]; }
+  }
+  return 0;
+}
+
+/* h, u, v and RK level `level` of every element (get) or of the listed elements
+ * (put: n entries, 1-based element ids, values in list order). */
+int orc_get_level(const orc_t* o, int level, double* out6) {
+  const int32_t T = o->n_elems;
+  if (level < 0 || level > o->opt.rkorder) return set_err(STORM_ERR_ARG, "bad level");
+  memcpy(out6, o->h, sizeof(double) * T);
+  memcpy(out6 + T, o->u, sizeof(double) * T);
+  memcpy(out6 + 2 * (size_t)T, o->v, sizeof(double) * T);
+  memcpy(out6 + 3 * (size_t)T, o->rkh + (size_t)level * T, sizeof(double) * T);
+  memcpy(out6 + 4 * (size_t)T, o->rku + (size_t)level * T, sizeof(double) * T);
+  memcpy(out6 + 5 * (size_t)T, o->rkv + (size_t)level * T, sizeof(double) * T);
+  return 0;
+}
+int orc_put_level(orc_t* o, int level, int32_t n, const int32_t* elems, const double* in6) {
+  const int32_t T = o->n_elems;
+  if (level < 0 || level > o->opt.rkorder) return set_err(STORM_ERR_ARG, "bad level");
+  for (int32_t k = 0; k < n; k++) {
+    const int32_t i = elems[k];
+    if (i < 1 || i > T) return set_err(STORM_ERR_ARG, "element out of range");
+    H(i) = in6[k];
+    U(i) = in6[n + k];
+    V(i) = in6[2 * (size_t)n + k];
+    RKH(i, level) = in6[3 * (size_t)n + k];
+    RKU(i, level) = in6[4 * (size_t)n + k];
+    RKV(i, level) = in6[5 * (size_t)n + k];
+  }
+  return 0;
+}
+
+/* The inflow safety-net elevation (dataprepFVT.f90:278-286) of the whole mesh, for a
+ * part that holds only some of its boundary. */
+void orc_set_bch_max(orc_t* o, double v) { o->bch_max = v; }
+double orc_get_bch_max(const orc_t* o) { return o->bch_max; }
+
 int orc_get_state(const orc_t* o, double* h, double* u, double* v, double* rkh, double* rku, double* rkv,
                   double* hvtx) {
   const int32_t T = o->n_elems, K = o->opt.rkorder;

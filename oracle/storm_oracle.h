@@ -57,6 +57,23 @@ int orc_output_vertices(orc_t* o, const StormFvtOutputBoundary* ob, int in_loop,
 int orc_stage_probe(orc_t* o, int rkstep, int upto, int32_t* dry, double* grads6,
                     double* uv2, double* hvtx, double* phi3);
 
+/* One iteration of orc_step in steps, for one part of a mesh split over processes
+ * (the caller exchanges halo values and reduces dt and sums between the calls):
+ * orc_iter_begin (level copy, this part's CFL dt), orc_iter_set_dt (the global dt),
+ * orc_iter_stage for each RK stage, orc_iter_fric (friction with the whole mesh's
+ * friction dt, this part's sums over its owned elements), orc_iter_finish (scalars
+ * and stop test from the sums of all parts).  orc_get_level / orc_put_level move h,
+ * u, v and one RK level ([6][n] blocks). */
+int orc_iter_begin(orc_t* o, double* dt_local);
+void orc_iter_set_dt(orc_t* o, double delt);
+int orc_iter_stage(orc_t* o, int rkstep, double* delt_out, int* bad);
+int orc_iter_fric(orc_t* o, double delt, const uint8_t* owned, double* sums);
+int orc_iter_finish(orc_t* o, const double* sums, StormFvtStepStats* st);
+int orc_get_level(const orc_t* o, int level, double* out6);
+int orc_put_level(orc_t* o, int level, int32_t n, const int32_t* elems, const double* in6);
+void orc_set_bch_max(orc_t* o, double v);
+double orc_get_bch_max(const orc_t* o);
+
 #ifdef __cplusplus
 }
 #endif

@@ -390,3 +390,119 @@ class PartitionedSolver:
             for k in out:
                 out[k][own] = s[k][P.owned]
         return out
+
+
+class DistributedPart:
+    """One part of a mesh per process: the multi-process form of the linked parts.
+
+    Every rank holds one extended part (its owned cells plus the halo rings that make
+    its prepared data equal to the whole mesh's, `check_part`) in its own `engine` and
+    steps it with the exchanges an undivided iteration implies (solverFVT.f90:148-154
+    for dt, :335-346 and :407-445 for the friction step, residual and stop test):
+
+    * unsteady with the CFL dt: the iteration's dt is the minimum of the parts' CFL
+      minima (all_reduce MIN), exactly the whole mesh's;
+    * after every RK stage but the last, and after the friction step, the halo takes
+      its owners' h, u, v and that RK level (`exchange_halo`, isend/irecv in (owner,
+      receiver) order; NCCL puts the values in this GPU's own buffers);
+    * steady: the friction step uses the local dt of element n_elems of the whole mesh
+      (N3), broadcast from the part that owns it;
+    * the residual sums, the mass (all_reduce SUM) and max |phi| (MAX) come from the
+      owned cells of every part, so the stop test is the whole mesh's.
+
+    The owned cells then read exactly the values they read undivided.  `engine` is
+    made by make_engine(problem, options) for this rank's part and provides
+    set_state, iter_begin, iter_set_dt, iter_stage, iter_fric, iter_finish,
+    get_level, put_level, set_bch_max and state.  Every rank takes the same
+    collective steps in the same order."""
+
+    def __init__(self, problem: abi.ProblemHolder, options: abi.Options, rank: int, world: int, dist, make_engine):
+        import torch
+        self.rank, self.world, self.dist = rank, world, dist
+        self.options = options
+        self.K = int(options.rkorder)
+        self.device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        gm = fvt.build_mesh(problem)
+        mn = gm.numpy()
+        self.T = int(mn["n_elems"])
+        self.part = partition_cells(problem, mn, world)
+        adj = _Adjacency(problem.tri.reshape(self.T, 3).astype(np.int64) - 1, int(mn["n_pts"]))
+        rings = 0
+        for r in range(3, 9):  # the smallest halo that reproduces the whole mesh's data here
+            P = extended_parts(problem, mn, self.part, rings=r, only=[rank])[0]
+            pm = fvt.build_mesh(P.problem)
+            ok = check_part(mn, pm.numpy(), P, adj) == 0
+            pm.close()
+            if ok:
+                rings = r
+                break
+        allr = torch.zeros(world, dtype=torch.int64, device=self.device)
+        allr[rank] = rings
+        dist.all_reduce(allr)
+        if int(allr.min()) == 0:
+            raise ValueError("a part has no halo depth that reproduces the whole mesh's data")
+        parts = [extended_parts(problem, mn, self.part, rings=int(allr[p]), only=[p])[0] for p in range(world)]
+        self.P = parts[rank]
+        self.plan = exchange_plan(parts, self.part)
+        self.halo_elems = (np.nonzero(~self.P.owned)[0] + 1).astype(np.int32)
+        self.fric_owner = int(self.part[self.T - 1])
+        self.engine = make_engine(self.P.problem, options)
+        self.engine.set_bch_max(gm.mesh.bch_max)  # the inflow safety net is a whole-mesh figure
+        gm.close()
+        self.converged = False
+
+    def _reduce(self, vals, op):
+        import torch
+        t = torch.tensor(vals, dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return t.cpu().numpy()
+
+    def _exchange(self, level: int):
+        f = self.engine.get_level(level)
+        fields = [np.ascontiguousarray(f[k]) for k in range(6)]
+        exchange_halo(self.rank, self.plan, fields, self.dist)
+        he = self.halo_elems
+        self.engine.put_level(level, he, np.stack([x[he - 1] for x in fields]))
+
+    def set_state(self, h, u, v):
+        c = self.P.cells
+        self.engine.set_state(np.asarray(h)[c], np.asarray(u)[c], np.asarray(v)[c])
+        self.converged = False
+
+    def step(self, n: int = 1) -> dict:
+        import torch
+        R = self.dist.ReduceOp
+        o = self.options
+        st = {}
+        for _ in range(n):
+            if self.converged:
+                break
+            dt = self.engine.iter_begin()
+            if not o.steady and o.dt_op != 0:
+                dt = float(self._reduce([dt], R.MIN)[0])
+            self.engine.iter_set_dt(dt)
+            d_last = dt
+            for s in range(1, self.K + 1):
+                d_last = self.engine.iter_stage(s)
+                if s < self.K:
+                    self._exchange(s)
+            if o.steady:
+                t = torch.tensor([d_last], dtype=torch.float64, device=self.device)
+                self.dist.broadcast(t, src=self.fric_owner)
+                dfric = float(t.cpu()[0])
+            else:
+                dfric = dt
+            sums = self.engine.iter_fric(dfric, self.P.owned)
+            self._exchange(self.K)
+            tot = np.concatenate([self._reduce(list(sums[:3]), R.SUM), self._reduce([sums[3]], R.MAX)])
+            st = self.engine.iter_finish(tot)
+            self.converged = bool(st["converged"])
+        return st
+
+    def owned_state(self) -> dict:
+        """The owned cells' state: global ids and h, u, v, rkh, rku, rkv."""
+        s = self.engine.state()
+        own = self.P.owned
+        out = {k: np.asarray(s[k])[own] for k in ("h", "u", "v", "rkh", "rku", "rkv")}
+        out["cells"] = self.P.cells[own]
+        return out

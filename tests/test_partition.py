@@ -260,3 +260,63 @@ def test_halo_exchange_over_two_gloo_ranks():
     for rank, ok, total, whole in res:
         assert ok, rank
         assert total == pytest.approx(whole, rel=1e-13)
+
+
+def _parts_rank(rank, world, port, which, steps, out):
+    """One rank of the one-part-per-process run: its part stepped through the oracle
+    with the real exchanges over gloo, then its owned cells against an undivided
+    oracle run of the same steps."""
+    import os
+    import torch.distributed as dist
+    from oracle.oracle import Oracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        if which == "meander":
+            sc = scenarios.meander(n_target=6000, seed=11)        # unsteady, CFL dt, wet/dry, Manning
+        else:
+            sc = scenarios.channel(nx=40, ny=6, rstop=2e-4, stop_cr=1)  # steady, stop test, friction dt
+        dp = partition.DistributedPart(sc.problem, sc.options, rank, world, dist, lambda p, o: Oracle(p, o))
+        dp.set_state(sc.h0, sc.u0, sc.v0)
+        st = dp.step(steps)
+        whole = Oracle(sc.problem, sc.options)
+        whole.set_state(sc.h0, sc.u0, sc.v0)
+        so = whole.step(steps)
+        mine, ref = dp.owned_state(), whole.state()
+        c = mine["cells"]
+        ok = {k: bool(np.array_equal(mine[k].view(np.uint64), ref[k][c].view(np.uint64)))
+              for k in ("h", "u", "v", "rkh", "rku", "rkv")}
+        out.put((rank, ok, st["iter"], so["iter"], bool(st["converged"]), bool(so["converged"]),
+                 st["tmass"], so["tmass"], len(c), len(dp.halo_elems)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("which,steps", [("meander", 30), ("channel", 3000)])
+def test_one_part_per_process_bitwise_vs_undivided(which, steps):
+    """The multi-process decomposition over two gloo ranks: halo exchange after every
+    stage and the friction step, global dt minimum, the friction dt of element
+    n_elems, global sums for the stop test.  Owned cells are bit for bit those of the
+    undivided run and both stop at the same iteration; the mass, summed per part,
+    agrees to round-off."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_parts_rank, args=(r, 2, port, which, steps, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=600) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+    owned = 0
+    for rank, ok, it, it_ref, conv, conv_ref, tm, tm_ref, n_own, n_halo in res:
+        assert all(ok.values()), (rank, ok)
+        assert it == it_ref and conv == conv_ref
+        assert tm == pytest.approx(tm_ref, rel=1e-13)
+        assert n_halo > 0
+        owned += n_own
+    if which == "channel":
+        assert res[0][4]  # the steady run reached its stop test
+    assert owned == scenarios.meander(n_target=6000, seed=11).n_elems if which == "meander" else owned == 480
