@@ -367,6 +367,41 @@ STORM_FVT_API int storm_fvt_set_stage_path(StormFvtHandle* hd, int32_t path);
 /* The path the captured iteration runs (one of the STORM_STAGE_* values). */
 STORM_FVT_API int32_t storm_fvt_stage_path(const StormFvtHandle* hd);
 
+/*
+ * One part of a mesh per process (one GPU each).  No counterpart in the reference,
+ * which runs one mesh in one process: these cut storm_fvt_step's iteration at the
+ * points where the parts exchange halo values and agree on dt and on the stop test,
+ * and the caller (storm_b200/partition.py, DistributedPart) does the exchanges
+ * between the calls.  Single-mesh handles whose mesh is an extended part:
+ *   storm_fvt_set_exchange   the part's elements (1-based) it sends to other parts and
+ *                            the halo elements it receives (left out of its sums);
+ *   storm_fvt_iter_begin     this part's CFL dt (unsteady: the global dt is the
+ *                            minimum over the parts) or the carried steady dt;
+ *   storm_fvt_iter_set_dt    the iteration's dt (unsteady);
+ *   storm_fvt_iter_stage     RK stage s; *delt_last: steady, the local dt of the part's
+ *                            last element (element n_elems of the mesh in its owner);
+ *   storm_fvt_iter_fric      friction with dt `delt` (steady: element n_elems's), then
+ *                            sums[4] = this part's sum (h-h0)^2, sum h0^2, mass, max|phi|;
+ *   storm_fvt_iter_finish    the iteration's scalars and stop test from the sums of all
+ *                            parts (SUM, SUM, SUM, MAX);
+ *   storm_fvt_pack_halo      h, u, v, rkh, rku, rkv ([6][n_send], device memory) of the
+ *                            sent elements after stage `level`, or after the friction
+ *                            step (after_fric = 1, level 0);
+ *   storm_fvt_unpack_halo    the received [6][n_recv] values into the halo elements,
+ *                            with their dry flags derived from them.
+ * pack/unpack synchronise the handle's stream before they return.
+ */
+STORM_FVT_API int storm_fvt_set_exchange(StormFvtHandle* hd, int32_t n_send, const int32_t* send_elems,
+                                         int32_t n_recv, const int32_t* recv_elems);
+STORM_FVT_API int storm_fvt_iter_begin(StormFvtHandle* hd, double* dt_local);
+STORM_FVT_API int storm_fvt_iter_set_dt(StormFvtHandle* hd, double dt);
+STORM_FVT_API int storm_fvt_iter_stage(StormFvtHandle* hd, int32_t s, double* delt_last);
+STORM_FVT_API int storm_fvt_iter_fric(StormFvtHandle* hd, double delt, double* sums);
+STORM_FVT_API int storm_fvt_iter_finish(StormFvtHandle* hd, const double* sums, StormFvtStepStats* stats);
+STORM_FVT_API int storm_fvt_pack_halo(StormFvtHandle* hd, int32_t level, int32_t after_fric, double* dev_out);
+STORM_FVT_API int storm_fvt_unpack_halo(StormFvtHandle* hd, int32_t level, int32_t after_fric,
+                                        const double* dev_in);
+
 /* Host-only check of the fused kernel's tile plan for a batch of prepared meshes
  * (no device needed; no counterpart in the reference).  stats[8] receives: tiles,
  * largest local cell count, largest gradient count, largest edge count, H1 cells,

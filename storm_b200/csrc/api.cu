@@ -89,6 +89,10 @@ struct StormFvtHandle {
   bool fuse_nodes = true;   // k_tile computes the vertex depths (else k_node runs before it)
   int32_t* bc_nodes = nullptr;  // vertices of the boundary cells (device, in tile_buf)
   int n_bc_nodes = 0;
+  // one part of a mesh per process: the cells this part sends / receives (device slots)
+  void* xchg_buf = nullptr;
+  int32_t *send_slots = nullptr, *recv_slots = nullptr;
+  int n_send = 0, n_recv = 0;
   double *u_a2 = nullptr, *v_a2 = nullptr;
 };
 
@@ -150,7 +154,9 @@ static_assert(KT_COUNT <= 8, "per-class timing arrays hold 8 classes");
 constexpr int kTileCellsHost = 256;   // cell slots per tile of k_tile
 constexpr int kTileThreadsHost = 256;
 
-int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
+// One iteration (only = -1), or only its RK stage `only` (1..K), or only its friction
+// step and reductions (only = 0: the iteration cut of storm_fvt_iter_*).
+int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used, int only = -1) {
   const Dev& d = h->d;
   const int T = d.T, K = d.K;
   const int gT = (T + h->bs_grad - 1) / h->bs_grad;
@@ -198,7 +204,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
     L.tiles = &h->td;
     launch_stage(L, d, h->gd, h->gf, h->mixed);
   };
-  if (linked && !d.steady && d.dt_op != 0) launch_link_dt(d, h->stream);
+  if (only < 0 && linked && !d.steady && d.dt_op != 0) launch_link_dt(d, h->stream);
   for (int s = 1; s <= K; s++) {
     const double* hs = d.rkh + (size_t)(s - 1) * T;
     uint8_t* dry = (s & 1) ? d.dry_a : d.dry_b;
@@ -210,6 +216,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
       u_out = (s & 1) ? h->u_a2 : d.u_a;
       v_out = (s & 1) ? h->v_a2 : d.v_a;
     }
+    if (only >= 0 && s != only) continue;
     const bool tile_nodes = fused && h->td.nodes;
     if (!tile_nodes) {
       if (mark(KT_NODE)) return STORM_ERR_CUDA;
@@ -300,13 +307,17 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used) {
       if (done()) return STORM_ERR_CUDA;
     }
     // halo cells of linked partitions take their owners' new level and flags
-    if (d.nhalo > 0 && s < K) launch_halo(d, s, dry_next, nullptr, h->stream);
+    if (linked && d.nhalo > 0 && s < K) launch_halo(d, s, dry_next, nullptr, h->stream);
+  }
+  if (only > 0) {
+    CK(cudaGetLastError());
+    return 0;
   }
   if (linked && d.steady) launch_link_fric(d, h->stream);
   if (mark(KT_FRIC)) return STORM_ERR_CUDA;
   launch_fric(d, u_out, v_out, h->stream);
   if (done()) return STORM_ERR_CUDA;
-  if (d.nhalo > 0) launch_halo(d, 0, d.dry_a, d.dry_out, h->stream);
+  if (linked && d.nhalo > 0) launch_halo(d, 0, d.dry_a, d.dry_out, h->stream);
   if (mark(KT_FINAL)) return STORM_ERR_CUDA;
   k_final<<<d.nscen, kRed, 0, h->stream>>>(d);
   if (done()) return STORM_ERR_CUDA;
@@ -354,6 +365,7 @@ void release(StormFvtHandle* h) {
   if (h->out_buf) cudaFree(h->out_buf);
   if (h->halo_buf) cudaFree(h->halo_buf);
   if (h->tile_buf) cudaFree(h->tile_buf);
+  if (h->xchg_buf) cudaFree(h->xchg_buf);
   if (h->io_host) cudaFreeHost(h->io_host);
   delete h;
 }
@@ -1293,6 +1305,173 @@ int storm_fvt_set_stage_path(StormFvtHandle* h, int32_t path) {
 int32_t storm_fvt_stage_path(const StormFvtHandle* h) {
   if (!h || !h->use_tiles) return STORM_STAGE_PHASES;
   return h->td.nodes ? STORM_STAGE_FUSED : STORM_STAGE_FUSED_NODE_KERNEL;
+}
+
+// ---- one part of a mesh per process ------------------------------------------------
+
+static int part_handle(StormFvtHandle* h, const char* who) {
+  if (!h) return set_error(STORM_ERR_ARG, std::string(who) + ": null handle");
+  if (h->nscen != 1 || h->d.linked) return set_error(STORM_ERR_ARG, std::string(who) + ": needs a single-mesh handle");
+  if (!h->have_state) return set_error(STORM_ERR_ARG, std::string(who) + ": state not set");
+  CK(cudaSetDevice(h->device));
+  return 0;
+}
+
+static int read_scalars(StormFvtHandle* h) {
+  CK(cudaMemcpyAsync(h->sc_host, h->d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int storm_fvt_set_exchange(StormFvtHandle* h, int32_t n_send, const int32_t* send_elems, int32_t n_recv,
+                           const int32_t* recv_elems) {
+  clear_error();
+  if (!h) return set_error(STORM_ERR_ARG, "storm_fvt_set_exchange: null handle");
+  if (h->nscen != 1 || h->d.linked) return set_error(STORM_ERR_ARG, "storm_fvt_set_exchange: needs a single-mesh handle");
+  if (n_send < 0 || n_recv < 0 || (n_send && !send_elems) || (n_recv && !recv_elems))
+    return set_error(STORM_ERR_ARG, "storm_fvt_set_exchange: bad element lists");
+  const HostLayout& P = h->parts[0];
+  const int32_t T = h->d.T;
+  std::vector<int32_t> ss(std::max(n_send, 1)), rs(std::max(n_recv, 1));
+  std::vector<uint8_t> mask(T, 0);
+  for (int32_t i = 0; i < n_send; i++) {
+    if (send_elems[i] < 1 || send_elems[i] > P.T) return set_error(STORM_ERR_ARG, "storm_fvt_set_exchange: element out of range");
+    ss[i] = P.cell_new[send_elems[i] - 1];
+  }
+  for (int32_t i = 0; i < n_recv; i++) {
+    if (recv_elems[i] < 1 || recv_elems[i] > P.T) return set_error(STORM_ERR_ARG, "storm_fvt_set_exchange: element out of range");
+    rs[i] = P.cell_new[recv_elems[i] - 1];
+    if (mask[rs[i]]) return set_error(STORM_ERR_ARG, "storm_fvt_set_exchange: a received element is listed twice");
+    mask[rs[i]] = 1;
+  }
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->xchg_buf) cudaFree(h->xchg_buf);
+  h->xchg_buf = nullptr;
+  const size_t a = (4 * ss.size() + 255) & ~(size_t)255, b = (4 * rs.size() + 255) & ~(size_t)255;
+  cudaError_t e = cudaMalloc(&h->xchg_buf, a + b + T);
+  if (e != cudaSuccess) return set_error(STORM_ERR_NOMEM, std::string("storm_fvt_set_exchange: ") + cudaGetErrorString(e));
+  char* B = static_cast<char*>(h->xchg_buf);
+  CK(cudaMemcpy(B, ss.data(), 4 * ss.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B + a, rs.data(), 4 * rs.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(B + a + b, mask.data(), T, cudaMemcpyHostToDevice));
+  h->send_slots = reinterpret_cast<int32_t*>(B);
+  h->recv_slots = reinterpret_cast<int32_t*>(B + a);
+  h->n_send = n_send;
+  h->n_recv = n_recv;
+  // the received (halo) cells stay out of this part's reductions
+  h->d.halo_mask = reinterpret_cast<uint8_t*>(B + a + b);
+  h->d.nhalo = n_recv;
+  return 0;
+}
+
+int storm_fvt_iter_begin(StormFvtHandle* h, double* dt_local) {
+  clear_error();
+  int rc = part_handle(h, "storm_fvt_iter_begin");
+  if (rc) return rc;
+  if (!dt_local) return set_error(STORM_ERR_ARG, "storm_fvt_iter_begin: null argument");
+  if ((rc = read_scalars(h))) return rc;
+  *dt_local = h->sc_host[0].delt;
+  return 0;
+}
+
+int storm_fvt_iter_set_dt(StormFvtHandle* h, double dt) {
+  clear_error();
+  int rc = part_handle(h, "storm_fvt_iter_set_dt");
+  if (rc) return rc;
+  if (!h->opt.steady) launch_part_scalar(h->d, 0, dt, h->stream);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int storm_fvt_iter_stage(StormFvtHandle* h, int32_t s, double* delt_last) {
+  clear_error();
+  int rc = part_handle(h, "storm_fvt_iter_stage");
+  if (rc) return rc;
+  if (s < 1 || s > h->d.K) return set_error(STORM_ERR_ARG, "storm_fvt_iter_stage: stage out of range");
+  size_t dummy = 0;
+  if ((rc = enqueue_step(h, false, &dummy, s))) return rc;
+  h->launches += h->kernels_per_step / std::max(1, h->d.K);
+  if ((rc = read_scalars(h))) return rc;
+  if (delt_last) *delt_last = h->opt.steady ? h->sc_host[0].delt_fric : h->sc_host[0].delt;
+  return 0;
+}
+
+int storm_fvt_iter_fric(StormFvtHandle* h, double delt, double* sums) {
+  clear_error();
+  int rc = part_handle(h, "storm_fvt_iter_fric");
+  if (rc) return rc;
+  if (!sums) return set_error(STORM_ERR_ARG, "storm_fvt_iter_fric: null argument");
+  if (h->opt.steady) launch_part_scalar(h->d, 1, delt, h->stream);
+  size_t dummy = 0;
+  if ((rc = enqueue_step(h, false, &dummy, 0))) return rc;
+  h->launches += 2;
+  if ((rc = read_scalars(h))) return rc;
+  const Scalars& sc = h->sc_host[0];
+  sums[0] = sc.sumtop;
+  sums[1] = sc.sumbot;
+  sums[2] = sc.tmass;
+  sums[3] = sc.rmax_phi;
+  return 0;
+}
+
+int storm_fvt_iter_finish(StormFvtHandle* h, const double* sums, StormFvtStepStats* stats) {
+  clear_error();
+  int rc = part_handle(h, "storm_fvt_iter_finish");
+  if (rc) return rc;
+  if (!sums) return set_error(STORM_ERR_ARG, "storm_fvt_iter_finish: null argument");
+  launch_part_finish(h->d, sums, h->stream);
+  h->launches += 1;
+  CK(cudaGetLastError());
+  if ((rc = read_scalars(h))) return rc;
+  if (stats) fill_stats(h, h->sc_host[0], stats);
+  return 0;
+}
+
+// velocity buffers and dry flags of the state after stage `level` (after_fric = 0) or
+// after the friction step (level 0)
+static void part_buffers(StormFvtHandle* h, int level, int after_fric, double** u, double** v, uint8_t** dry) {
+  const Dev& d = h->d;
+  if (after_fric || !h->use_tiles) {
+    *u = d.u_a;
+    *v = d.v_a;
+  } else {
+    *u = (level & 1) ? h->u_a2 : d.u_a;
+    *v = (level & 1) ? h->v_a2 : d.v_a;
+  }
+  *dry = after_fric ? d.dry_a : ((level & 1) ? d.dry_b : d.dry_a);
+}
+
+int storm_fvt_pack_halo(StormFvtHandle* h, int32_t level, int32_t after_fric, double* dev_out) {
+  clear_error();
+  int rc = part_handle(h, "storm_fvt_pack_halo");
+  if (rc) return rc;
+  if (level < 0 || level > h->d.K || (after_fric && level != 0))
+    return set_error(STORM_ERR_ARG, "storm_fvt_pack_halo: level out of range (0 after the friction step)");
+  if (h->n_send > 0 && !dev_out) return set_error(STORM_ERR_ARG, "storm_fvt_pack_halo: null buffer");
+  double *u, *v;
+  uint8_t* dry;
+  part_buffers(h, level, after_fric, &u, &v, &dry);
+  launch_pack(h->d, level, h->n_send, h->send_slots, u, v, dev_out, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int storm_fvt_unpack_halo(StormFvtHandle* h, int32_t level, int32_t after_fric, const double* dev_in) {
+  clear_error();
+  int rc = part_handle(h, "storm_fvt_unpack_halo");
+  if (rc) return rc;
+  if (level < 0 || level > h->d.K || (after_fric && level != 0))
+    return set_error(STORM_ERR_ARG, "storm_fvt_unpack_halo: level out of range (0 after the friction step)");
+  if (h->n_recv > 0 && !dev_in) return set_error(STORM_ERR_ARG, "storm_fvt_unpack_halo: null buffer");
+  double *u, *v;
+  uint8_t* dry;
+  part_buffers(h, level, after_fric, &u, &v, &dry);
+  launch_unpack(h->d, level, h->n_recv, h->recv_slots, dev_in, u, v, dry, h->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
 }
 
 int storm_fvt_tile_check(const StormFvtMesh* const* meshes, int32_t n, int32_t tile_cells, int64_t* stats) {

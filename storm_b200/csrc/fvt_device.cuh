@@ -170,6 +170,15 @@ void launch_link_dt(const Dev& d, cudaStream_t st);
 // Friction, hvalve and the iteration partials (halo cells left out when linked).
 void launch_fric(const Dev& d, const double* u_src, const double* v_src, cudaStream_t st);
 void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st);
+// One part of a mesh per process: set dt (which 0) or the friction dt (1), pack /
+// unpack [6][n] halo values of the listed slots, finish the iteration with the sums
+// of all parts {sumtop, sumbot, tmass, max |phi|}.
+void launch_part_scalar(const Dev& d, int which, double v, cudaStream_t st);
+void launch_pack(const Dev& d, int level, int n, const int32_t* slots, const double* u, const double* v,
+                 double* out, cudaStream_t st);
+void launch_unpack(const Dev& d, int level, int n, const int32_t* slots, const double* in, double* u, double* v,
+                   uint8_t* dry, cudaStream_t st);
+void launch_part_finish(const Dev& d, const double* sums, cudaStream_t st);
 // k_node over every node (list == nullptr) or the n listed nodes
 void launch_node(const Dev& d, const double* hs, const uint8_t* dry, const int32_t* list, int n, int block,
                  cudaStream_t st);

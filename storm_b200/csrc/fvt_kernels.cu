@@ -2441,6 +2441,88 @@ __global__ void k_link(Dev d) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// One part of a mesh per process (storm_fvt_iter_*): the caller moves the halo values
+// between the processes and reduces dt and the sums; these kernels set the agreed
+// scalars and pack / unpack the exchanged cells.
+
+// which 0: the iteration's dt; 1: the steady friction dt (element n_elems of the mesh)
+__global__ void k_part_scalar(Dev d, int which, double v) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  if (which == 0) d.sc[0].delt = v;
+  else d.sc[0].delt_fric = v;
+}
+
+// out[6][n]: h (= rkh of the level), u, v, rkh, rku, rkv of the listed slots
+__global__ void __launch_bounds__(256) k_pack(Dev d, int level, int n, const int32_t* __restrict__ slots,
+                                              const double* __restrict__ u, const double* __restrict__ v,
+                                              double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = slots[k];
+  const size_t q = (size_t)level * d.T + c;
+  out[k] = d.rkh[q];
+  out[n + k] = u[c];
+  out[2 * (size_t)n + k] = v[c];
+  out[3 * (size_t)n + k] = d.rkh[q];
+  out[4 * (size_t)n + k] = d.rku[q];
+  out[5 * (size_t)n + k] = d.rkv[q];
+}
+
+// The received values into the listed (halo) slots, and their dry flags as the owner
+// derived them from the same state (find_dry_cells, as rk_update and k_fric do)
+__global__ void __launch_bounds__(256) k_unpack(Dev d, int level, int n, const int32_t* __restrict__ slots,
+                                                const double* __restrict__ in, double* __restrict__ u,
+                                                double* __restrict__ v, uint8_t* __restrict__ dry) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = slots[k];
+  const size_t q = (size_t)level * d.T + c;
+  const double hh = in[3 * (size_t)n + k], uu = in[n + k], vv = in[2 * (size_t)n + k];
+  d.rkh[q] = hh;
+  d.rku[q] = in[4 * (size_t)n + k];
+  d.rkv[q] = in[5 * (size_t)n + k];
+  u[c] = uu;
+  v[c] = vv;
+  double um;
+  dry[c] = dry_flag(hh, uu, vv, d.h_dry, d.h_wet, &um);
+}
+
+// The iteration's residual, mass, max |phi| and stop test from the sums of all parts
+// (k_final's expressions with the whole mesh's sums).
+__global__ void k_part_finish(Dev d, double top, double bot, double tm, double rmx) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  Scalars* sc = &d.sc[0];
+  double sbot = bot;
+  if (equals(sbot, kZero)) sbot = kOne;
+  sc->rms = sqrt(top / sbot);
+  sc->tmass = tm;
+  sc->sumtop = top;
+  sc->sumbot = bot;
+  sc->rmax_phi = rmx;
+  if (d.steady) {
+    sc->rmax = (d.stop_cr == 0) ? rmx : sc->rms;
+    sc->converged = sc->rmax < d.rstop;
+  } else {
+    sc->rmax = rmx;
+  }
+}
+
+void launch_part_scalar(const Dev& d, int which, double v, cudaStream_t st) {
+  k_part_scalar<<<1, 32, 0, st>>>(d, which, v);
+}
+void launch_pack(const Dev& d, int level, int n, const int32_t* slots, const double* u, const double* v,
+                 double* out, cudaStream_t st) {
+  if (n > 0) k_pack<<<(n + 255) / 256, 256, 0, st>>>(d, level, n, slots, u, v, out);
+}
+void launch_unpack(const Dev& d, int level, int n, const int32_t* slots, const double* in, double* u, double* v,
+                   uint8_t* dry, cudaStream_t st) {
+  if (n > 0) k_unpack<<<(n + 255) / 256, 256, 0, st>>>(d, level, n, slots, in, u, v, dry);
+}
+void launch_part_finish(const Dev& d, const double* sums, cudaStream_t st) {
+  k_part_finish<<<1, 32, 0, st>>>(d, sums[0], sums[1], sums[2], sums[3]);
+}
+
 void launch_halo(const Dev& d, int level, uint8_t* f1, uint8_t* f2, cudaStream_t st) {
   k_halo<<<(d.nhalo + 255) / 256, 256, 0, st>>>(d, level, f1, f2);
 }

@@ -31,6 +31,8 @@ EXPORTS = (
     "storm_fvt_set_scenario_state", "storm_fvt_get_scenario_state", "storm_fvt_scenario_stats",
     "storm_fvt_autotune", "storm_fvt_output_vertices", "storm_fvt_link_partitions",
     "storm_fvt_set_stage_path", "storm_fvt_stage_path", "storm_fvt_tile_check",
+    "storm_fvt_set_exchange", "storm_fvt_iter_begin", "storm_fvt_iter_set_dt", "storm_fvt_iter_stage",
+    "storm_fvt_iter_fric", "storm_fvt_iter_finish", "storm_fvt_pack_halo", "storm_fvt_unpack_halo",
 )
 
 KERNEL_CLASSES = ("node", "grad", "bc", "flux", "fric", "final", "eflux", "tile")
@@ -91,6 +93,14 @@ def lib():
     L.storm_fvt_stage_path.restype = C.c_int32
     L.storm_fvt_tile_check.argtypes = [C.POINTER(C.POINTER(abi.Mesh)), C.c_int32, C.c_int32,
                                        C.POINTER(C.c_int64)]
+    L.storm_fvt_set_exchange.argtypes = [C.c_void_p, C.c_int32, ip, C.c_int32, ip]
+    L.storm_fvt_iter_begin.argtypes = [C.c_void_p, dp]
+    L.storm_fvt_iter_set_dt.argtypes = [C.c_void_p, C.c_double]
+    L.storm_fvt_iter_stage.argtypes = [C.c_void_p, C.c_int32, dp]
+    L.storm_fvt_iter_fric.argtypes = [C.c_void_p, C.c_double, dp]
+    L.storm_fvt_iter_finish.argtypes = [C.c_void_p, dp, C.POINTER(abi.StepStats)]
+    L.storm_fvt_pack_halo.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
+    L.storm_fvt_unpack_halo.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]
     _lib = L
     return L
 

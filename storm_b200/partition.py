@@ -411,10 +411,12 @@ class DistributedPart:
       owned cells of every part, so the stop test is the whole mesh's.
 
     The owned cells then read exactly the values they read undivided.  `engine` is
-    made by make_engine(problem, options) for this rank's part and provides
-    set_state, iter_begin, iter_set_dt, iter_stage, iter_fric, iter_finish,
-    get_level, put_level, set_bch_max and state.  Every rank takes the same
-    collective steps in the same order."""
+    made by make_engine(problem, options, bch_max) for this rank's part (bch_max: the
+    whole mesh's inflow safety-net elevation) and provides set_state, iter_begin,
+    iter_set_dt, iter_stage, iter_fric, iter_finish and state, and either get_level /
+    put_level (host arrays; the state after the friction step is RK level K) or
+    set_exchange / pack / unpack (device buffers, GpuPartEngine).  Every rank takes
+    the same collective steps in the same order."""
 
     def __init__(self, problem: abi.ProblemHolder, options: abi.Options, rank: int, world: int, dist, make_engine):
         import torch
@@ -446,9 +448,26 @@ class DistributedPart:
         self.plan = exchange_plan(parts, self.part)
         self.halo_elems = (np.nonzero(~self.P.owned)[0] + 1).astype(np.int32)
         self.fric_owner = int(self.part[self.T - 1])
-        self.engine = make_engine(self.P.problem, options)
-        self.engine.set_bch_max(gm.mesh.bch_max)  # the inflow safety net is a whole-mesh figure
+        # the inflow safety net is a whole-mesh figure
+        self.engine = make_engine(self.P.problem, options, float(gm.mesh.bch_max))
         gm.close()
+        self.device_exchange = hasattr(self.engine, "pack")
+        if self.device_exchange:
+            # this rank's sends in (receiver) order and receives in (owner) order
+            sends = [(p, src) for (q, p), (src, _) in sorted(self.plan.items()) if q == rank]
+            recvs = [(q, dst) for (q, p), (_, dst) in sorted(self.plan.items()) if p == rank]
+            self.send_off, self.recv_off, o = {}, {}, 0
+            for p, src in sends:
+                self.send_off[p] = (o, len(src))
+                o += len(src)
+            o = 0
+            for q, dst in recvs:
+                self.recv_off[q] = (o, len(dst))
+                o += len(dst)
+            cat = (lambda a: np.concatenate(a).astype(np.int32) if a else np.zeros(0, np.int32))
+            self.send_elems = cat([src for _, src in sends])
+            self.recv_elems = cat([dst for _, dst in recvs])
+            self.engine.set_exchange(self.send_elems, self.recv_elems)
         self.converged = False
 
     def _reduce(self, vals, op):
@@ -457,12 +476,44 @@ class DistributedPart:
         self.dist.all_reduce(t, op=op)
         return t.cpu().numpy()
 
-    def _exchange(self, level: int):
+    def _exchange(self, level: int, after_fric: bool = False):
+        if self.device_exchange:
+            return self._exchange_device(0 if after_fric else level, after_fric)
         f = self.engine.get_level(level)
         fields = [np.ascontiguousarray(f[k]) for k in range(6)]
         exchange_halo(self.rank, self.plan, fields, self.dist)
         he = self.halo_elems
         self.engine.put_level(level, he, np.stack([x[he - 1] for x in fields]))
+
+    def _exchange_device(self, level: int, after_fric: bool):
+        """Halo values packed on this GPU, sent per peer over the process group (device
+        tensors with NCCL, staged through the host with gloo) and unpacked on the GPU."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        host = self.device == "cpu"
+        sb = torch.empty((6, len(self.send_elems)), dtype=torch.float64, device=dev)
+        self.engine.pack(level, after_fric, sb)
+        if host:
+            sb = sb.cpu()
+        rb = torch.empty((6, len(self.recv_elems)), dtype=torch.float64, device="cpu" if host else dev)
+        reqs, inbox = [], []
+        for (q, p) in sorted(self.plan):
+            if q == self.rank:
+                o, n = self.send_off[p]
+                reqs.append(self.dist.isend(sb[:, o:o + n].contiguous(), dst=p))
+            if p == self.rank:
+                o, n = self.recv_off[q]
+                buf = torch.empty((6, n), dtype=torch.float64, device=rb.device)
+                reqs.append(self.dist.irecv(buf, src=q))
+                inbox.append((o, n, buf))
+        for r in reqs:
+            r.wait()
+        for o, n, buf in inbox:
+            rb[:, o:o + n] = buf
+        if host:
+            rb = rb.to(dev)
+        torch.cuda.synchronize()
+        self.engine.unpack(level, after_fric, rb)
 
     def set_state(self, h, u, v):
         c = self.P.cells
@@ -493,7 +544,7 @@ class DistributedPart:
             else:
                 dfric = dt
             sums = self.engine.iter_fric(dfric, self.P.owned)
-            self._exchange(self.K)
+            self._exchange(self.K, after_fric=True)
             tot = np.concatenate([self._reduce(list(sums[:3]), R.SUM), self._reduce([sums[3]], R.MAX)])
             st = self.engine.iter_finish(tot)
             self.converged = bool(st["converged"])
@@ -506,3 +557,60 @@ class DistributedPart:
         out = {k: np.asarray(s[k])[own] for k in ("h", "u", "v", "rkh", "rku", "rkv")}
         out["cells"] = self.P.cells[own]
         return out
+
+
+class GpuPartEngine:
+    """A part on this process's GPU through the library's per-process entry points
+    (storm_fvt_iter_*, storm_fvt_pack_halo / storm_fvt_unpack_halo)."""
+
+    def __init__(self, problem: abi.ProblemHolder, options: abi.Options, bch_max: float):
+        import ctypes as C
+        self._C = C
+        self.pm = fvt.build_mesh(problem)
+        self.pm.mesh.bch_max = bch_max
+        self.solver = fvt.Solver(self.pm, options, keep=self.pm)
+        self._h = self.solver._h
+
+    def close(self):
+        self.solver.close()
+
+    def set_exchange(self, send_elems, recv_elems):
+        s = np.ascontiguousarray(send_elems, dtype=np.int32)
+        r = np.ascontiguousarray(recv_elems, dtype=np.int32)
+        fvt._chk(fvt.lib().storm_fvt_set_exchange(self._h, len(s), abi.iptr(s), len(r), abi.iptr(r)))
+
+    def set_state(self, h, u, v):
+        self.solver.set_state(h, u, v)
+
+    def iter_begin(self) -> float:
+        d = self._C.c_double()
+        fvt._chk(fvt.lib().storm_fvt_iter_begin(self._h, self._C.byref(d)))
+        return d.value
+
+    def iter_set_dt(self, dt: float):
+        fvt._chk(fvt.lib().storm_fvt_iter_set_dt(self._h, float(dt)))
+
+    def iter_stage(self, s: int) -> float:
+        d = self._C.c_double()
+        fvt._chk(fvt.lib().storm_fvt_iter_stage(self._h, int(s), self._C.byref(d)))
+        return d.value
+
+    def iter_fric(self, dt: float, owned) -> np.ndarray:
+        sums = np.zeros(4)
+        fvt._chk(fvt.lib().storm_fvt_iter_fric(self._h, float(dt), abi.dptr(sums)))
+        return sums
+
+    def iter_finish(self, sums) -> dict:
+        s = np.ascontiguousarray(sums, dtype=np.float64)
+        st = abi.StepStats()
+        fvt._chk(fvt.lib().storm_fvt_iter_finish(self._h, abi.dptr(s), self._C.byref(st)))
+        return st.as_dict()
+
+    def pack(self, level: int, after_fric: bool, buf):
+        fvt._chk(fvt.lib().storm_fvt_pack_halo(self._h, int(level), int(bool(after_fric)), buf.data_ptr()))
+
+    def unpack(self, level: int, after_fric: bool, buf):
+        fvt._chk(fvt.lib().storm_fvt_unpack_halo(self._h, int(level), int(bool(after_fric)), buf.data_ptr()))
+
+    def state(self) -> dict:
+        return self.solver.state()

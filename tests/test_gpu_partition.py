@@ -94,3 +94,62 @@ def test_wind_meander_three_parts(storm_lib):
     sc.problem.cd[:] = 0.0
     sc = scenarios.with_wind(sc, scenarios.wind_fields(sc.problem, at_vertices=True, seed=3))
     _compare(sc, sc.options, 3, rounds=1, steps=30)
+
+
+def _gpu_parts_rank(rank, world, port, which, steps, out):
+    import os
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        if which == "meander":
+            sc = scenarios.meander(n_target=6000, seed=11)
+        else:
+            sc = scenarios.channel(nx=40, ny=6, rstop=2e-4, stop_cr=1)
+        dp = partition.DistributedPart(sc.problem, sc.options, rank, world, dist, partition.GpuPartEngine)
+        dp.set_state(sc.h0, sc.u0, sc.v0)
+        st = dp.step(steps)
+        pm = fvt.build_mesh(sc.problem)
+        whole = fvt.Solver(pm, sc.options, keep=pm)
+        whole.set_state(sc.h0, sc.u0, sc.v0)
+        sw = whole.step(steps)
+        mine, ref = dp.owned_state(), whole.state()
+        c = mine["cells"]
+        ok = {k: bool(np.array_equal(mine[k].view(np.uint64), ref[k][c].view(np.uint64)))
+              for k in ("h", "u", "v", "rkh", "rku", "rkv")}
+        out.put((rank, ok, st["iter"], sw["iter"], bool(st["converged"]), bool(sw["converged"]),
+                 st["tmass"], sw["tmass"], dp.engine.solver.stage_path()))
+        dp.engine.close()
+        whole.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("which,steps", [("meander", 30), ("channel", 3000)])
+def test_one_part_per_process_gpu(which, steps, storm_lib):
+    """The multi-process decomposition with each part in the CUDA library (fused stage
+    kernel): two processes share this one GPU and exchange through the host over gloo
+    (no kernel waits on another process).  Owned cells are bit for bit those of the
+    undivided GPU run; both stop at the same iteration."""
+    import socket
+    import torch.multiprocessing as mp
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gpu_parts_rank, args=(r, 2, port, which, steps, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=600) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+    for rank, ok, it, it_ref, conv, conv_ref, tm, tm_ref, path in res:
+        assert all(ok.values()), (rank, ok)
+        assert it == it_ref and conv == conv_ref
+        assert tm == pytest.approx(tm_ref, rel=1e-13)
+        assert path == fvt.STAGE_FUSED

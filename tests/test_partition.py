@@ -262,6 +262,13 @@ def test_halo_exchange_over_two_gloo_ranks():
         assert total == pytest.approx(whole, rel=1e-13)
 
 
+def _oracle_engine(problem, options, bch_max):
+    from oracle.oracle import Oracle
+    o = Oracle(problem, options)
+    o.set_bch_max(bch_max)
+    return o
+
+
 def _parts_rank(rank, world, port, which, steps, out):
     """One rank of the one-part-per-process run: its part stepped through the oracle
     with the real exchanges over gloo, then its owned cells against an undivided
@@ -277,7 +284,7 @@ def _parts_rank(rank, world, port, which, steps, out):
             sc = scenarios.meander(n_target=6000, seed=11)        # unsteady, CFL dt, wet/dry, Manning
         else:
             sc = scenarios.channel(nx=40, ny=6, rstop=2e-4, stop_cr=1)  # steady, stop test, friction dt
-        dp = partition.DistributedPart(sc.problem, sc.options, rank, world, dist, lambda p, o: Oracle(p, o))
+        dp = partition.DistributedPart(sc.problem, sc.options, rank, world, dist, _oracle_engine)
         dp.set_state(sc.h0, sc.u0, sc.v0)
         st = dp.step(steps)
         whole = Oracle(sc.problem, sc.options)
