@@ -23,6 +23,7 @@
 // No float atomics: every sum is a fixed-order tree or a serial loop, so the results
 // are reproducible run to run.
 #include <cstdint>
+#include <mutex>
 
 #include "fvt_device.cuh"
 #include "storm_internal.h"
@@ -1839,6 +1840,12 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       }
       s_dhx[l] = gr.hx;
       s_dhy[l] = gr.hy;
+      // the last stage's depth gradient is what the output step's error estimate reads
+      // (error_est.f90 etype 2); the boundary cells' comes from their k_grad pass
+      if (s == d.K && !(d.forder[g] & kOrderHasBc)) {
+        G.delh_x[g] = gr.hx;
+        G.delh_y[g] = gr.hy;
+      }
     }
     const double h_c = s_h[l];
 #pragma unroll
@@ -1928,9 +1935,23 @@ int tile_blocks_per_sm(bool mixed, size_t smem) {
   return n;
 }
 
+// The dynamic shared-memory limit is a property of the kernel function (per device),
+// shared by every handle: it only ever grows, so a handle that needs less never
+// lowers it under another handle's launches.
+static int raise_smem_limit(int* per_dev, int bytes) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return bytes;
+  if (bytes > per_dev[dev]) per_dev[dev] = bytes;
+  return per_dev[dev];
+}
+
 void set_tile_smem_limit(int bytes) {
-  cudaFuncSetAttribute(k_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  static int lim[64] = {0};
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  const int b = raise_smem_limit(lim, bytes);
+  cudaFuncSetAttribute(k_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  cudaFuncSetAttribute(k_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
 // ---------------------------------------------------------------------------
@@ -2594,8 +2615,12 @@ void launch_rsavg(const Dev& d, int off, int cnt, cudaStream_t st) {
 }
 
 void set_bc_smem_limit(int bytes) {
-  cudaFuncSetAttribute(k_bc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_bc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  static int lim[64] = {0};
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  const int b = raise_smem_limit(lim, bytes);
+  cudaFuncSetAttribute(k_bc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  cudaFuncSetAttribute(k_bc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
 }  // namespace storm
