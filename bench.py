@@ -217,6 +217,7 @@ def run_batch(args, rank, world, local):
                    "cells": int(sum(sizes)), "scenarios": args.batch_n, "rstop": 1e-6, "istop": args.istop,
                    "limiter": {0: "first order (opt 0)", 1: "LSQ (opt 1)", 2: "LSQ + BJ (opt 2)"}[args.batch_limiter],
                    "block_sizes_rank0": tuned, "parallelism": f"scenario shards x{world}",
+                   "stage_path_rank0": {0: "phases", 1: "fused", 2: "fused-node-kernel"}[b.stage_path()],
                    "shard_imbalance": shard.imbalance(sizes, shard.lpt_shards(sizes, world))},
         "time_to_steady_rank0": {"converged": int(conv.sum()), "of": len(scs),
                                  "iterations_median": float(np.median(iters[conv])) if conv.any() else None,
@@ -598,8 +599,9 @@ def main():
     ap.add_argument("--kt-steps", type=int, default=5, help="iterations of the per-kernel timing pass")
     ap.add_argument("--parts", type=int, default=1,
                     help="run the mesh as this many linked parts on one GPU (domain decomposition)")
-    ap.add_argument("--stage-path", choices=["fused", "phases"], default="fused",
-                    help="stage kernels of the timed runs: the fused tile kernel (default) or the phase kernels")
+    ap.add_argument("--stage-path", choices=["phases", "fused", "fused-node-kernel"], default="phases",
+                    help="stage kernels of the timed runs: the phase kernels (the library's default), the fused "
+                         "tile kernel, or the fused kernel with the vertex depths by k_node")
     ap.add_argument("--ab-steps", type=int, default=200,
                     help="iterations of the other stage path, timed in the same run (0: skip)")
     ap.add_argument("--trajectory", action="store_true",
@@ -688,8 +690,8 @@ def main():
     K_rk = sc.options.rkorder
     t0 = time.perf_counter()
     solver = fvt.Solver(pm, sc.options, keep=pm)
-    if args.stage_path == "phases":
-        solver.set_stage_path(fvt.STAGE_PHASES)
+    solver.set_stage_path({"phases": fvt.STAGE_PHASES, "fused": fvt.STAGE_FUSED,
+                           "fused-node-kernel": fvt.STAGE_FUSED_NODE_KERNEL}[args.stage_path])
     path_used = {fvt.STAGE_PHASES: "phases", fvt.STAGE_FUSED: "fused",
                  fvt.STAGE_FUSED_NODE_KERNEL: "fused-node-kernel"}[solver.stage_path()]
     setup = {"mesh_build_s": mesh_ratios.build_s, "create_s": time.perf_counter() - t0,

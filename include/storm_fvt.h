@@ -343,10 +343,12 @@ STORM_FVT_API int storm_fvt_last_timing(const StormFvtHandle* hd, double* step_m
  * 1 and 3 time the boundary cells' gradient and update kernels only. */
 STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, int64_t* launches);
 
-/* Project autotuner: times `iters` iterations per candidate block size of the node,
- * gradient, edge-flux and cell kernels on this handle's meshes (per-kernel CUDA
- * events), keeps the fastest of each, re-captures the iteration graph and restores
- * the state it started from.  `chosen` (may be NULL) receives the four sizes. */
+/* Project autotuner: first times `iters` whole iterations of each stage path
+ * (storm_fvt_set_stage_path) and keeps the fastest, then times `iters` iterations per
+ * candidate block size of the node, gradient, edge-flux and cell kernels on this
+ * handle's meshes (per-kernel CUDA events) and keeps the fastest of each;
+ * re-captures the iteration graph and restores the state it started from.  `chosen`
+ * (may be NULL) receives the four sizes; storm_fvt_stage_path reports the path. */
 STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t* chosen);
 
 /* Stage kernels of the captured iteration.  No counterpart in the reference (it
@@ -354,9 +356,10 @@ STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t*
  * same either way):
  *   STORM_STAGE_PHASES  k_node, k_grad, k_eflux, k_flux per stage (gradients and edge
  *                       fluxes pass through device memory between the kernels);
+ *                       the default;
  *   STORM_STAGE_FUSED   one fused kernel per stage over Morton tiles of 256 cells
  *                       (vertex depths, gradients, edge fluxes and the RK update of a
- *                       tile in shared memory), the default wherever it applies;
+ *                       tile in shared memory);
  *   STORM_STAGE_FUSED_NODE_KERNEL  the same with the vertex depths computed by k_node
  *                       before it (for measurement).
  * The fused path does not apply to culverts, residual smoothing or linked partitions

@@ -84,7 +84,7 @@ struct StormFvtHandle {
   size_t tile_smem = 0;
   int tile_grid = 0;        // persistent grid of k_tile: resident CTAs on all SMs
   bool tiles_ok = false;    // plan built and within the shared-memory limit
-  bool want_tiles = true;   // storm_fvt_set_stage_path
+  bool want_tiles = false;  // storm_fvt_set_stage_path / storm_fvt_autotune (phase kernels by default)
   bool use_tiles = false;   // the captured iteration runs k_tile
   bool fuse_nodes = true;   // k_tile computes the vertex depths (else k_node runs before it)
   int32_t* bc_nodes = nullptr;  // vertices of the boundary cells (device, in tile_buf)
@@ -1233,6 +1233,40 @@ int storm_fvt_autotune(StormFvtHandle* h, int32_t iters, int32_t* chosen) {
     CK(cudaMemcpyAsync(snap + off, pc.p, pc.n, cudaMemcpyDeviceToDevice, h->stream));
     off += pc.n;
   }
+  // the stage path first: whole iterations (graph replays) of each path, from the same
+  // state, the fastest kept
+  auto restore = [&]() -> int {
+    size_t o2 = 0;
+    for (auto& pc : pieces) {
+      CK(cudaMemcpyAsync(pc.p, snap + o2, pc.n, cudaMemcpyDeviceToDevice, h->stream));
+      o2 += pc.n;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+  };
+  int rc = 0;
+  {
+    const bool want0 = h->want_tiles, nodes0 = h->fuse_nodes;
+    int best_path = -1;
+    double best_ms = 1e300;
+    const int paths[3] = {STORM_STAGE_PHASES, STORM_STAGE_FUSED, STORM_STAGE_FUSED_NODE_KERNEL};
+    for (int p : paths) {
+      if (p != STORM_STAGE_PHASES && !h->tiles_ok) continue;
+      if ((rc = storm_fvt_set_stage_path(h, p))) break;
+      if (p != STORM_STAGE_PHASES && storm_fvt_stage_path(h) != p) continue;  // not applicable here
+      if ((rc = restore()) || (rc = storm_fvt_step(h, iters, nullptr))) break;
+      if (h->last_step_ms < best_ms) {
+        best_ms = h->last_step_ms;
+        best_path = p;
+      }
+    }
+    if (!rc && (rc = restore())) {}
+    if (!rc) rc = storm_fvt_set_stage_path(h, best_path >= 0 ? best_path : (want0 ? (nodes0 ? 1 : 2) : 0));
+    if (rc) {
+      cudaFree(snap);
+      return rc;
+    }
+  }
   struct Knob {
     int* bs;
     int cls;
@@ -1243,7 +1277,6 @@ int storm_fvt_autotune(StormFvtHandle* h, int32_t iters, int32_t* chosen) {
                {&h->bs_flux, KT_FLUX, {32, 64, 128}}};
   const bool was_timing = h->timing;
   h->timing = true;
-  int rc = 0;
   for (auto& kb : knobs) {
     double best = 1e300;
     int best_bs = *kb.bs;

@@ -563,12 +563,14 @@ class GpuPartEngine:
     """A part on this process's GPU through the library's per-process entry points
     (storm_fvt_iter_*, storm_fvt_pack_halo / storm_fvt_unpack_halo)."""
 
-    def __init__(self, problem: abi.ProblemHolder, options: abi.Options, bch_max: float):
+    def __init__(self, problem: abi.ProblemHolder, options: abi.Options, bch_max: float, stage_path=None):
         import ctypes as C
         self._C = C
         self.pm = fvt.build_mesh(problem)
         self.pm.mesh.bch_max = bch_max
         self.solver = fvt.Solver(self.pm, options, keep=self.pm)
+        if stage_path is not None:
+            self.solver.set_stage_path(stage_path)
         self._h = self.solver._h
 
     def close(self):

@@ -139,7 +139,7 @@ def scenario_q_hbc(sc) -> tuple[float, float]:
 # ---- solver runs ---------------------------------------------------------------------
 
 def run_steady_batch(scs, states=None, istop: int = 40000, chunk: int = 64, precision=abi.PREC_MIXED,
-                     device: int = 0, autotune: bool = False, keep_states: bool = True, rstop=None):
+                     device: int = 0, autotune: bool = True, keep_states: bool = True, rstop=None):
     """Run scenarios together to their stop test (or istop).  `states` (optional) is a
     list of (h, u, v) initial states; default is each scenario's cold start.  Returns
     per-scenario iterations, convergence time (ms of device time from the start) and,
@@ -175,7 +175,7 @@ def run_steady_batch(scs, states=None, istop: int = 40000, chunk: int = 64, prec
     out = {"iters": np.array([st["iter"] for st in stats]), "converged": np.array([bool(st["converged"]) for st in stats]),
            "conv_ms": np.array([c if c is not None else np.nan for c in conv_ms]), "device_ms": t_ms, "wall_s": wall,
            "rmax": np.array([st["rmax"] for st in stats]), "block_sizes": tuned,
-           "launches": b.kernel_launches()}
+           "stage_path": b.stage_path(), "launches": b.kernel_launches()}
     if keep_states:
         out["states"] = [b.scenario_state(i) for i in range(len(scs))]
     b.close()
@@ -443,7 +443,8 @@ def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, dev
     dh_pred = dmax(warm_states)
 
     def summ(r):
-        return {"converged": int(r["converged"].sum()), "iters_mean": float(r["iters"].mean()),
+        return {"stage_path": {0: "phases", 1: "fused", 2: "fused-node-kernel"}.get(r.get("stage_path"), None),
+                "converged": int(r["converged"].sum()), "iters_mean": float(r["iters"].mean()),
                 "iters_median": float(np.median(r["iters"])), "iters_max": int(r["iters"].max()),
                 "device_s_batch": r["device_ms"] / 1e3, "device_ms_per_scenario": r["device_ms"] / len(ev),
                 "wall_s_batch": r["wall_s"]}

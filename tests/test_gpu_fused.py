@@ -1,9 +1,10 @@
 """The fused stage kernel (k_tile) against the phase kernels (k_grad, k_eflux,
-k_flux), through the C-ABI.  Both paths run the same device functions for the
+k_flux, the default path), through the C-ABI.  Both paths run the same device functions for the
 gradient, edge-flux and update arithmetic, so every state array, RK level, vertex
 depth and iteration statistic must agree to the last bit, in FP64 and in mixed
 precision, with and without open boundaries, for single meshes and batches.  The
-oracle comparisons of test_gpu_parity.py run on the fused path (the default)."""
+oracle comparisons of test_gpu_parity.py run on the phase kernels (the default),
+so the fused path equals the oracle through them."""
 import numpy as np
 import pytest
 
@@ -18,8 +19,7 @@ def _bits(a):
 
 def _run(pm, opts, sc, path, steps):
     g = fvt.Solver(pm, opts, keep=pm)
-    if path != fvt.STAGE_FUSED:
-        g.set_stage_path(path)
+    g.set_stage_path(path)
     assert g.stage_path() == path
     g.set_state(sc.h0, sc.u0, sc.v0)
     st = None
@@ -58,8 +58,7 @@ def test_fused_batch_equals_phases(storm_lib):
     outs = []
     for path in (fvt.STAGE_FUSED, fvt.STAGE_PHASES):
         b = fvt.BatchSolver(pms, scs[0].options, keep=pms)
-        if path == fvt.STAGE_PHASES:
-            b.set_stage_path(path)
+        b.set_stage_path(path)
         assert b.stage_path() == path
         for i, s in enumerate(scs):
             b.set_scenario_state(i, s.h0, s.u0, s.v0)
@@ -79,5 +78,26 @@ def test_fused_not_used_for_culverts_or_smoothing(storm_lib):
     sc.options.rsavg_order = 1
     pm = fvt.build_mesh(sc.problem)
     g = fvt.Solver(pm, sc.options, keep=pm)
-    assert g.stage_path() == fvt.STAGE_PHASES
+    assert g.stage_path() == fvt.STAGE_PHASES  # the default
+    g.set_stage_path(fvt.STAGE_FUSED)
+    assert g.stage_path() == fvt.STAGE_PHASES  # not applicable with residual smoothing
     g.close()
+
+
+def test_autotune_keeps_state_and_picks_a_path(storm_lib):
+    """storm_fvt_autotune times the stage paths and the block sizes from the same
+    state and restores it: the run afterwards is bitwise the untuned run."""
+    sc = scenarios.meander(n_target=30_000, seed=5)
+    pm = fvt.build_mesh(sc.problem)
+    outs = []
+    for tune in (False, True):
+        g = fvt.Solver(pm, sc.options, keep=pm)
+        g.set_state(sc.h0, sc.u0, sc.v0)
+        if tune:
+            g.autotune(iters=2)
+            assert g.stage_path() in (fvt.STAGE_PHASES, fvt.STAGE_FUSED, fvt.STAGE_FUSED_NODE_KERNEL)
+        g.step(20)
+        outs.append(g.state())
+        g.close()
+    for k in ("h", "u", "v", "hvtx"):
+        assert np.array_equal(_bits(outs[0][k]), _bits(outs[1][k])), k
