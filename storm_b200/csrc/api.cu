@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -798,6 +799,13 @@ int storm_fvt_create_batch(const StormFvtMesh* const* meshes, int32_t n, const S
     if (!rc) merge_layouts(h->parts, kRed, h->L, h->info);
   } catch (const std::bad_alloc&) {
     rc = set_error(STORM_ERR_NOMEM, "storm_fvt_create: host out of memory");
+  }
+  if (!rc) {
+    // the kernels index the [rows][T] columns (stencil, faces, RK levels) in 32 bits
+    const int64_t rows = std::max<int64_t>({(int64_t)h->L.kst, 3, (int64_t)opt->rkorder + 1});
+    if (rows * (int64_t)h->L.T >= (int64_t)INT32_MAX)
+      rc = set_error(STORM_ERR_UNSUPPORTED, "storm_fvt_create: " + std::to_string(h->L.T) +
+                                                " cell slots exceed the 32-bit indexing of one handle (split the batch)");
   }
   if (rc) {
     delete h;

@@ -592,7 +592,7 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
       R w[3], dx[3], dy[3], pz[3], pu[3], pv[3];
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        const size_t q = (size_t)k * T + c;
+        const int q = k * T + c;
         jj[k] = st(k);
         w[k] = G.st_w[q];
         dx[k] = G.st_dx[q];
@@ -616,7 +616,7 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
       k0 = 3;
     }
     for (int k = k0; k < n; k++) {
-      const size_t q = (size_t)k * T + c;
+      const int q = k * T + c;
       const int j = st(k);
       const R w = G.st_w[q], dx = G.st_dx[q], dy = G.st_dy[q];
       const R pz = (R)((nb.H(j) + nb.Z(j)) - zeta_c);
@@ -641,7 +641,7 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
     R rz[3], ru[3], rv[3];
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-      const size_t q = (size_t)j * T + c;
+      const int q = j * T + c;
       const int k = t3[j];
       const R rx = G.rc_x[q], ry = G.rc_y[q];
       if (rcx) {
@@ -720,9 +720,9 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
   const NbGlobal nb{hs, d.z, u_in, v_in, dry};
   int t3[3];
 #pragma unroll
-  for (int j = 0; j < 3; j++) t3[j] = d.t2t3[(size_t)j * T + c];
-  const GradOut<R> g = cell_gradients<R>(d, G, nb, c, c, t3, [&](int k) { return d.st_id[(size_t)k * T + c]; },
-                                         [&](int j) { return d.vwet[d.vert[(size_t)j * T + c]] != 0; },
+  for (int j = 0; j < 3; j++) t3[j] = d.t2t3[j * T + c];
+  const GradOut<R> g = cell_gradients<R>(d, G, nb, c, c, t3, [&](int k) { return d.st_id[k * T + c]; },
+                                         [&](int j) { return d.vwet[d.vert[j * T + c]] != 0; },
                                          (R*)nullptr, (R*)nullptr);
   if (g.fix) {
     rku_prev[c] = kZero;
@@ -761,7 +761,7 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
   // reconstructed edge states (the h/u/v + grad . rc of the boundary element)
   for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
     const int i = d.bce_cell[off + e], m = d.bce_slot[off + e];
-    const size_t q = (size_t)m * T + i;
+    const int q = m * T + i;
     d.bc_rec[off + e] = recon(hs[i], G.delh_x[i], G.rc_x[q], G.delh_y[i], G.rc_y[q]);
     d.bc_rec[NB + off + e] = recon(d.u_b[i], G.delu_x[i], G.rc_x[q], G.delu_y[i], G.rc_y[q]);
     d.bc_rec[2 * NB + off + e] = recon(d.v_b[i], G.delv_x[i], G.rc_x[q], G.delv_y[i], G.rc_y[q]);
@@ -1147,7 +1147,7 @@ struct EdgeState {
 template <class R>
 __device__ __forceinline__ EdgeState edge_state(const Dev& d, const Geo<R>& G, const double* __restrict__ hs, int x,
                                                 int m) {
-  const size_t q = (size_t)m * d.T + x;
+  const int q = m * d.T + x;
   const R rx = G.rc_x[q], ry = G.rc_y[q];
   EdgeState s;
   s.h = recon(hs[x], G.delh_x[x], rx, G.delh_y[x], ry);
@@ -1254,7 +1254,7 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<double>& G, i
   bool adjust = false;
 #pragma unroll
   for (int i = 0; i < 3; i++) {
-    const size_t q = (size_t)i * T + c;
+    const int q = i * T + c;
     hp[i] = h_c + dhx * d.vox[q] + dhy * d.voy[q];
     if (hp[i] < kZero) adjust = true;
   }
@@ -1263,7 +1263,7 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<double>& G, i
     double zp[3], x[3], y[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-      const int vid = d.vert[(size_t)i * T + c];
+      const int vid = d.vert[i * T + c];
       hp[i] = fmin2(kZero, hp[i]);
       zp[i] = d.zvtx[vid] + hp[i];
       x[i] = d.node_x[vid];
@@ -1289,7 +1289,7 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<float>& G, in
   bool adjust = false;
 #pragma unroll
   for (int i = 0; i < 3; i++) {
-    const size_t q = (size_t)i * T + c;
+    const int q = i * T + c;
     hp[i] = h_c + (double)(dhx * G.vox[q] + dhy * G.voy[q]);
     if (hp[i] < kZero) adjust = true;
   }
@@ -1297,7 +1297,7 @@ __device__ __forceinline__ void bed_source(const Dev& d, const Geo<float>& G, in
     double zp[3], x[3], y[3];
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-      const int vid = d.vert[(size_t)i * T + c];
+      const int vid = d.vert[i * T + c];
       zp[i] = d.zvtx[vid] + fmin2(kZero, hp[i]);
       x[i] = d.node_x[vid];
       y[i] = d.node_y[vid];
@@ -1324,7 +1324,7 @@ struct FacesGlobal {
   int c;
   // flux*length of the interior face in slot j, and whether the edge produced one
   __device__ __forceinline__ bool iface(int j, R* f) const {
-    const int e = d.fref[(size_t)j * d.T + c];
+    const int e = d.fref[j * d.T + c];
     f[0] = G.efx[e];
     f[1] = G.efx[d.ne + e];
     f[2] = G.efx[2 * d.ne + e];
@@ -1332,7 +1332,7 @@ struct FacesGlobal {
   }
   // the cell's own reconstructed state at face j (weslp2 walls)
   __device__ __forceinline__ EdgeState own(int j) const {
-    const size_t q = (size_t)j * d.T + c;
+    const int q = j * d.T + c;
     EdgeState s;
     s.h = recon(hs[c], G.delh_x[c], G.rc_x[q], G.delh_y[c], G.rc_y[q]);
     s.u = recon(d.u_b[c], G.delu_x[c], G.rc_x[q], G.delu_y[c], G.rc_y[q]);
@@ -1345,7 +1345,7 @@ struct FacesGlobal {
   }
   // vertex depths at the two ends (walledg1 order) of the wall face in slot j
   __device__ __forceinline__ void hwall(int j, double* h1, double* h2) const {
-    const int w = d.fref[(size_t)j * d.T + c];
+    const int w = d.fref[j * d.T + c];
     *h1 = d.hvtx[d.wall_p1[w]];
     *h2 = d.hvtx[d.wall_p2[w]];
   }
@@ -1368,7 +1368,7 @@ struct FacesTile {
   const int32_t* __restrict__ wall_p2;
   const int32_t* __restrict__ fref;
   __device__ __forceinline__ void hwall(int j, double* h1, double* h2) const {
-    const size_t q = (size_t)j * T + c;
+    const int q = j * T + c;
     if (shv) {
       const uint32_t w = lwall[q];
       *h1 = shv[w & 0xFFFF];
@@ -1380,7 +1380,7 @@ struct FacesTile {
     }
   }
   __device__ __forceinline__ bool iface(int j, R* f) const {
-    const int le = lfe[(size_t)j * T + c];
+    const int le = lfe[j * T + c];
     f[0] = sf[le];
     f[1] = sf[nem + le];
     f[2] = sf[2 * nem + le];
@@ -1417,7 +1417,7 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, cons
 #pragma unroll
   for (int t = 0; t < 3; t++) {
     fj[t] = (ord >> (2 * t)) & 3;
-    fkd[t] = d.fkind[(size_t)fj[t] * T + c] & 7;
+    fkd[t] = d.fkind[fj[t] * T + c] & 7;
   }
   bool fok[3];
   R fv[3][3];
@@ -1430,7 +1430,7 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, cons
 #pragma unroll
   for (int t = 0; t < 3; t++) {
     const int j = fj[t];
-    const size_t q = (size_t)j * T + c;
+    const int q = j * T + c;
     const int kind = fkd[t];
     if (kind == FACE_LEFT || kind == FACE_RIGHT) {
       if (fok[t]) {
@@ -1534,7 +1534,7 @@ __device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c
     // a zero coefficient (SSP-RK3 stage 3, level 1) adds a signed zero to a sum that
     // started at +0, which leaves its bits unchanged: skip the loads
     if (d.alpha[s][j] == kZero) continue;
-    const size_t q = (size_t)j * T + c;
+    const int q = j * T + c;
     rh = rh + d.alpha[s][j] * d.rkh[q];
     ru = ru + d.alpha[s][j] * d.rku[q];
     rv = rv + d.alpha[s][j] * d.rkv[q];
@@ -1559,7 +1559,7 @@ __device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c
   } else {
     ru = kZero; rv = kZero; un = kZero; vn = kZero;
   }
-  const size_t qs = (size_t)s * T + c;
+  const int qs = s * T + c;
   d.rkh[qs] = rh;
   d.rku[qs] = ru;
   d.rkv[qs] = rv;
@@ -1626,7 +1626,7 @@ __global__ void __launch_bounds__(256) k_rsavg(Dev d, int off, int cnt) {
   const int n = d.nst[c];
   for (int k = 0; k < 3; k++) {
     double p = d.rs_fac1 * d.phi0[k * T + c];
-    for (int m = 0; m < n; m++) p = p + d.rs_fac2 * d.phi[k * T + d.st_id[(size_t)m * T + c]];
+    for (int m = 0; m < n; m++) p = p + d.rs_fac2 * d.phi[k * T + d.st_id[m * T + c]];
     d.phi[k * T + c] = p;
   }
 }
@@ -1797,17 +1797,17 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     if (sid < 0 || d.sc[sid].converged) continue;
     int t3[3];
     const uint16_t *st, *vt;
-    size_t sst, svt;
+    int sst, svt;
     if (own) {
 #pragma unroll
       for (int j = 0; j < 3; j++) {
-        const uint16_t x = tp.lt3[(size_t)j * T + g];
+        const uint16_t x = tp.lt3[j * T + g];
         t3[j] = x == kNoLocal ? -1 : (int)x;
       }
       st = tp.lst + g;
-      sst = (size_t)T;
+      sst = T;
       vt = tp.lvt + g;
-      svt = (size_t)T;
+      svt = T;
     } else {
       const size_t r = (size_t)(h1off + l - nown);
 #pragma unroll
@@ -1822,14 +1822,14 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     }
     R rx[3], ry[3];
     const GradOut<R> gr = cell_gradients<R>(
-        d, G, nbs, g, l, t3, [&](int k) { return (int)st[(size_t)k * sst]; },
-        [&](int j) { return tp.nodes ? s_vw[vt[(size_t)j * svt]] != 0 : d.vwet[d.vert[(size_t)j * T + g]] != 0; },
+        d, G, nbs, g, l, t3, [&](int k) { return (int)st[k * sst]; },
+        [&](int j) { return tp.nodes ? s_vw[vt[j * svt]] != 0 : d.vwet[d.vert[j * T + g]] != 0; },
         rx, ry);
     if (d.lim != 2) {
 #pragma unroll
       for (int j = 0; j < 3; j++) {
-        rx[j] = G.rc_x[(size_t)j * T + g];
-        ry[j] = G.rc_y[(size_t)j * T + g];
+        rx[j] = G.rc_x[j * T + g];
+        ry[j] = G.rc_y[j * T + g];
       }
     }
     if (own) {
@@ -1971,7 +1971,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d, const double* __res
   if (d.sc[d.cell_sid[blockIdx.x * blockDim.x] < 0 ? 0 : d.cell_sid[blockIdx.x * blockDim.x]].converged) return;
   double st = kZero, sb = kZero, tm = kZero, rm = kZero, dtc = kVlarge;
   if (sid >= 0) {
-    const size_t qk = (size_t)K * T + c;
+    const int qk = K * T + c;
     const double h = d.rkh[qk];
     double u = u_src[c], v = v_src[c];
     double ru = d.rku[qk], rv = d.rkv[qk];
@@ -2024,7 +2024,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d, const double* __res
 #pragma unroll
       for (int j = 0; j < 3; j++)
         if (hm & (1u << j)) {
-          const size_t q = (size_t)j * T + c;
+          const int q = j * T + c;
           const double dot = u * d.fnx[q] + v * d.fny[q];
           if (dot < 0) zero = true;
         }
