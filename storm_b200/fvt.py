@@ -204,11 +204,12 @@ class Solver:
         _chk(lib().storm_fvt_step(self._h, int(n), C.byref(st)))
         return st.as_dict()
 
-    def state(self) -> dict:
-        out = {k: np.empty(self.T) for k in ("h", "u", "v", "rkh", "rku", "rkv")}
-        out["hvtx"] = np.empty(self.N)
-        _chk(lib().storm_fvt_get_state(self._h, *(abi.dptr(out[k]) for k in
-                                                 ("h", "u", "v", "rkh", "rku", "rkv", "hvtx"))))
+    def state(self, keys=("h", "u", "v", "rkh", "rku", "rkv", "hvtx")) -> dict:
+        """The state in element order; `keys` selects the arrays read back (the
+        others are not copied)."""
+        out = {k: np.empty(self.N if k == "hvtx" else self.T) for k in keys}
+        ptr = lambda k: abi.dptr(out[k]) if k in out else None  # noqa: E731
+        _chk(lib().storm_fvt_get_state(self._h, *(ptr(k) for k in ("h", "u", "v", "rkh", "rku", "rkv", "hvtx"))))
         return out
 
     def output_vertices(self, ob: "abi.OutputBoundaryHolder", in_loop: bool = True) -> dict:
