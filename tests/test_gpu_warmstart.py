@@ -40,3 +40,29 @@ def test_warm_start_needs_fewer_iterations(storm_lib):
     for a, b in zip(warm["states"], cold["states"]):
         # both runs stop at RMS dh < 1e-6, a few cm short of the steady state
         assert np.abs(a["h"] - b["h"]).max() < 0.25
+
+
+MODEL_20K = os.path.join(os.path.dirname(warmstart.__file__), "models", "warmstart_channels_20k-40k.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(MODEL_20K), reason="no 20k-40k model in the package")
+def test_warm_start_20k_40k_beats_cold_and_prior(storm_lib):
+    """The 20k-40k-cell model on four held-out members of that band (seeds disjoint
+    from its training data): fewer iterations to RMS dh < 1e-6 than the cold start
+    and than the analytic prior alone (zero network output, same mapping)."""
+    net, norm = warmstart.load_model(MODEL_20K)
+    scs = scenarios.batch_channels(4, 20_000, 40_000, seed=515_151, opt_limiter=0)
+    inps = []
+    for sc in scs:
+        pm = fvt.build_mesh(sc.problem)
+        q, hbc = warmstart.scenario_q_hbc(sc)
+        inps.append(warmstart.scenario_inputs(pm.numpy(), q, hbc, sc.options.h_dry))
+    preds = warmstart.predict(net, norm, inps, "cuda:0")
+    warm = [warmstart.state_from_prediction(i, p) for i, p in zip(inps, preds)]
+    prior = [warmstart.state_from_prediction(i, np.zeros((len(i.d0), 3), dtype=np.float32)) for i in inps]
+    runs = {name: warmstart.run_steady_batch(scs, states=st, istop=60000, precision=abi.PREC_MIXED,
+                                             keep_states=False)
+            for name, st in (("cold", None), ("prior", prior), ("warm", warm))}
+    assert all(r["converged"].all() for r in runs.values()), {k: r["iters"] for k, r in runs.items()}
+    assert runs["warm"]["iters"].mean() < 0.8 * runs["cold"]["iters"].mean(), runs["warm"]["iters"]
+    assert runs["warm"]["iters"].mean() < 0.8 * runs["prior"]["iters"].mean(), runs["prior"]["iters"]
