@@ -100,6 +100,20 @@ __device__ __forceinline__ bool dry_flag(double h, double u, double v, double h_
   return dry;
 }
 
+// Whether cell slot c (node n, edge e) belongs to a scenario that is still running.
+// A one-scenario handle answers from the slot number and one flag shared by every
+// thread, so a thread's own loads do not wait behind a per-cell scenario lookup; a
+// batch looks up the slot's scenario (-1: padding).
+__device__ __forceinline__ bool cell_live(const Dev& d, int c) {
+  if (d.nscen == 1) return c < d.t_real && !d.sc[0].converged;
+  const int sid = d.cell_sid[c];
+  return sid >= 0 && !d.sc[sid].converged;
+}
+__device__ __forceinline__ bool item_live(const Dev& d, const int32_t* __restrict__ sid_of, int i) {
+  if (d.nscen == 1) return !d.sc[0].converged;
+  return !d.sc[sid_of[i]].converged;
+}
+
 // Arithmetic type of the flux, gradient and source kernels: double reproduces the
 // reference bit for bit; float is the mixed-precision path (state, the eta - zb
 // reconstruction at the faces and the RK accumulation stay in double).
@@ -480,8 +494,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ 
     if (i >= d.N) return;
     n = i;
   }
-  const int sid = d.node_sid[n];
-  if (d.sc[sid].converged) return;
+  if (!item_live(d, d.node_sid, n)) return;
   double hv;
   bool wet;
   node_depth(d, n, d.n2t_off[n], d.n2t_off[n + 1],
@@ -523,6 +536,23 @@ __device__ __forceinline__ double limited_r(double q0, double qn, double g_x, do
     // When |num| > |delq| the exact quotient exceeds one, so the rounded one is
     // >= 1 and the limiter's min(r,1) is 1: the division is skipped, same bits.
     const double num = (delq < 0) ? (qmin - q0) : (qmax - q0);
+    rj = (fabs(num) > fabs(delq)) ? kOne : qdiv(num, delq);
+  }
+  const double a = fmin2(kOne * rj, kOne);
+  const double b = fmin2(rj, kOne);
+  return fmax2(a, b);
+}
+// The same from d = qn - q0 (a stencil difference already formed): min(q0,qn) - q0 is
+// qn - q0 = d when qn < q0 and q0 - q0 otherwise, and qn < q0 exactly when d < 0 (the
+// difference of two doubles rounds to zero only when they are equal); likewise for the
+// maximum, so the quotient and the result are bit for bit those of limited_r.
+__device__ __forceinline__ double limited_rd(double q0, double dq, double g_x, double g_y, double rx, double ry) {
+  const double qj = q0 + g_x * rx + g_y * ry;
+  const double delq = qj - q0;
+  double rj;
+  if (equals(delq, kZero)) rj = kOne;
+  else {
+    const double num = (delq < 0) ? ((dq < 0) ? dq : q0 - q0) : ((dq > 0) ? dq : q0 - q0);
     rj = (fabs(num) > fabs(delq)) ? kOne : qdiv(num, delq);
   }
   const double a = fmin2(kOne * rj, kOne);
@@ -583,6 +613,11 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
   const double u_c = nb.U(self), v_c = nb.V(self);
   const bool dry_c = nb.D(self);
   R hx = R(0), hy = R(0), ux = R(0), uy = R(0), vx = R(0), vy = R(0);
+  constexpr bool kF64 = sizeof(R) == 8;
+  // FP64: the differences to the first three stencil members, which the limiter reuses
+  // for the face neighbours among them (no second gather of their state)
+  double dzs[3] = {0, 0, 0}, dus[3] = {0, 0, 0}, dvs[3] = {0, 0, 0};
+  int kmap = 0xFF;
   if (d.lim == 1 || d.lim == 2) {
     R dz = R(0), ez = R(0), du = R(0), eu = R(0), dv = R(0), ev = R(0);
     const int n = d.nst[c];
@@ -603,7 +638,13 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
         pz[k] = (R)((nb.H(jj[k]) + nb.Z(jj[k])) - zeta_c);
         pu[k] = (R)(nb.U(jj[k]) - u_c);
         pv[k] = (R)(nb.V(jj[k]) - v_c);
+        if (kF64) {
+          dzs[k] = (double)pz[k];
+          dus[k] = (double)pu[k];
+          dvs[k] = (double)pv[k];
+        }
       }
+      if (kF64 && d.lim == 2) kmap = d.t3k[c];
 #pragma unroll
       for (int k = 0; k < 3; k++) {
         dz = dz + w[k] * pz[k] * dx[k];
@@ -648,12 +689,22 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
         rcx[j] = rx;
         rcy[j] = ry;
       }
-      const double qz = k < 0 ? zeta_c : nb.H(k) + nb.Z(k);
-      const double qu = k < 0 ? u_c : nb.U(k);
-      const double qv = k < 0 ? v_c : nb.V(k);
-      rz[j] = limited_r(zeta_c, qz, hx, hy, rx, ry);
-      ru[j] = limited_r(u_c, qu, ux, uy, rx, ry);
-      rv[j] = limited_r(v_c, qv, vx, vy, rx, ry);
+      const int ks = (kmap >> (2 * j)) & 3;
+      if (kF64 && ks < 3) {
+        const double ddz = ks == 0 ? dzs[0] : (ks == 1 ? dzs[1] : dzs[2]);
+        const double ddu = ks == 0 ? dus[0] : (ks == 1 ? dus[1] : dus[2]);
+        const double ddv = ks == 0 ? dvs[0] : (ks == 1 ? dvs[1] : dvs[2]);
+        rz[j] = (R)limited_rd(zeta_c, ddz, (double)hx, (double)hy, (double)rx, (double)ry);
+        ru[j] = (R)limited_rd(u_c, ddu, (double)ux, (double)uy, (double)rx, (double)ry);
+        rv[j] = (R)limited_rd(v_c, ddv, (double)vx, (double)vy, (double)rx, (double)ry);
+      } else {
+        const double qz = k < 0 ? zeta_c : nb.H(k) + nb.Z(k);
+        const double qu = k < 0 ? u_c : nb.U(k);
+        const double qv = k < 0 ? v_c : nb.V(k);
+        rz[j] = limited_r(zeta_c, qz, hx, hy, rx, ry);
+        ru[j] = limited_r(u_c, qu, ux, uy, rx, ry);
+        rv[j] = limited_r(v_c, qv, vx, vy, rx, ry);
+      }
     }
     const R pz = fmin2(fmin2(rz[0], rz[1]), rz[2]);
     const R pu = fmin2(fmin2(ru[0], ru[1]), ru[2]);
@@ -714,8 +765,7 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
     if (i >= d.T) return;
     c = i;
   }
-  const int sid = d.cell_sid[c];
-  if (sid < 0 || d.sc[sid].converged) return;
+  if (!cell_live(d, c)) return;
   const int T = d.T;
   const NbGlobal nb{hs, d.z, u_in, v_in, dry};
   int t3[3];
@@ -1224,8 +1274,7 @@ __global__ void __launch_bounds__(128, 8) k_eflux(Dev d, Geo<R> G, const double*
                                                const uint8_t* __restrict__ dry) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.ne) return;
-  const int sid = d.edge_sid[e];
-  if (d.sc[sid].converged) return;
+  if (!item_live(d, d.edge_sid, e)) return;
   const int L = d.eL[e], Rc = d.eR[e];
   const uint8_t sl = d.eslot[e];
   R f[3];
@@ -1239,7 +1288,7 @@ __global__ void __launch_bounds__(128, 8) k_eflux(Dev d, Geo<R> G, const double*
     G.efx[d.ne + e] = f[1] * len;
     G.efx[2 * d.ne + e] = f[2] * len;
   }
-  if (bad) atomicOr(&d.sc[sid].status, 2);
+  if (bad) atomicOr(&d.sc[d.edge_sid[e]].status, 2);
 }
 
 // bed_slope_STD.f90:23-70 with adjustZb.f90:41-70: the amounts g*h*gradzb*area that
@@ -1603,8 +1652,7 @@ __global__ void __launch_bounds__(128) k_flux_phi(Dev d, Geo<R> G, const double*
     c = i;
     if (d.forder[c] & kOrderHasBc) return;
   }
-  const int sid = d.cell_sid[c];
-  if (sid < 0 || d.sc[sid].converged) return;
+  if (!cell_live(d, c)) return;
   double p1, p2, p3;
   assemble_phi<R>(d, G, FacesGlobal<R>{d, G, hs, c}, c, hs[c], dry[c] != 0, &p1, &p2, &p3);
   const size_t T = d.T;
@@ -1620,8 +1668,7 @@ __global__ void __launch_bounds__(256) k_rsavg(Dev d, int off, int cnt) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= cnt) return;
   const int c = d.rs_cells[off + q];
-  const int sid = d.cell_sid[c];
-  if (sid < 0 || d.sc[sid].converged) return;
+  if (!cell_live(d, c)) return;
   const size_t T = d.T;
   const int n = d.nst[c];
   for (int k = 0; k < 3; k++) {
@@ -1635,8 +1682,7 @@ __global__ void __launch_bounds__(128) k_update(Dev d, int s, const double* __re
                                             const uint8_t* __restrict__ dry, uint8_t* __restrict__ dry_next) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.T) return;
-  const int sid = d.cell_sid[c];
-  if (sid < 0 || d.sc[sid].converged) return;
+  if (!cell_live(d, c)) return;
   const size_t T = d.T;
   rk_update(d, s, c, hs[c], dry[c] != 0, d.phi[c], d.phi[T + c], d.phi[2 * T + c], dry_next, d.u_a, d.v_a, d.u_a,
             d.v_a);
@@ -1650,8 +1696,7 @@ __global__ void __launch_bounds__(128, 10) k_flux(Dev d, Geo<R> G, int s, const 
                                               double* __restrict__ u_out, double* __restrict__ v_out) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.T) return;
-  const int sid = d.cell_sid[c];
-  if (sid < 0 || d.sc[sid].converged) return;
+  if (!cell_live(d, c)) return;
   if (d.forder[c] & kOrderHasBc) return;
   flux_cell<R>(d, G, s, c, hs, dry, dry_next, u_in, v_in, u_out, v_out);
 }
@@ -1665,7 +1710,7 @@ __global__ void __launch_bounds__(128) k_flux_bc(Dev d, Geo<R> G, int s, const d
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.nbc_cells) return;
   const int c = d.bc_cells[i];
-  if (d.sc[d.cell_sid[c]].converged) return;
+  if (!cell_live(d, c)) return;
   flux_cell<R>(d, G, s, c, hs, dry, dry_next, u_in, v_in, u_out, v_out);
 }
 
@@ -1765,7 +1810,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   if (tp.nodes) {
     for (int ln = threadIdx.x; ln < nn; ln += blockDim.x) {
       const int n = tp.tnode[noff + ln];
-      if (d.sc[d.node_sid[n]].converged) continue;
+      if (!item_live(d, d.node_sid, n)) continue;
       const int b0 = d.n2t_off[n], b1 = d.n2t_off[n + 1];
       const int base = tp.tn_start[noff + ln] - b0;  // tn_cells[base + q] for q in [b0, b1)
       double hv;
@@ -1793,8 +1838,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   for (int l = threadIdx.x; l < nG; l += blockDim.x) {
     const bool own = l < nown;
     const int g = own ? c0 + l : tp.halo[hoff + l - nown];
-    const int sid = d.cell_sid[g];
-    if (sid < 0 || d.sc[sid].converged) continue;
+    if (!cell_live(d, g)) continue;
     int t3[3];
     const uint16_t *st, *vt;
     int sst, svt;
@@ -1870,9 +1914,8 @@ __global__ void __launch_bounds__(kTileThreads, 3)
       e = tp.be[boff + le - nr];
       lo = tp.beloc[boff + le - nr];
     }
-    const int sid = d.edge_sid[e];
     bool ok = false;
-    if (!d.sc[sid].converged) {
+    if (item_live(d, d.edge_sid, e)) {
       const int a = lo & 0xFFFF, b = lo >> 16;
       const uint8_t sl = d.eslot[e];
       const int ml = sl & 3, mr = (sl >> 2) & 3;
@@ -1900,7 +1943,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
           G.efx[2 * d.ne + e] = f[2];
         }
       }
-      if (bad) atomicOr(&d.sc[sid].status, 2);
+      if (bad) atomicOr(&d.sc[d.edge_sid[e]].status, 2);
     }
     s_eok[le] = ok;
   }
@@ -1909,8 +1952,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   // D: ordered gather, sources and RK update of the owned cells
   for (int l = threadIdx.x; l < nown; l += blockDim.x) {
     const int c = c0 + l;
-    const int sid = d.cell_sid[c];
-    if (sid < 0 || d.sc[sid].converged) continue;
+    if (!cell_live(d, c)) continue;
     if (d.forder[c] & kOrderHasBc) continue;
     const double h_c = s_h[l];
     const bool dry_c = s_dry[l] != 0;

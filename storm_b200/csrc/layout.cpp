@@ -297,7 +297,7 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
   L.delz_x.resize(T); L.delz_y.resize(T); L.zmax.resize(T); L.cd.resize(T);
   if (m.wcoef1 && m.wcoef2) { L.wcoef1.resize(T); L.wcoef2.resize(T); }
   L.lsq_a.resize(T); L.lsq_b.resize(T); L.lsq_c.resize(T); L.lsq_det.resize(T);
-  L.nst.resize(T); L.forder.resize(T); L.hvmask.assign(T, 0);
+  L.nst.resize(T); L.forder.resize(T); L.hvmask.assign(T, 0); L.t3k.assign(T, 0xFF);
   L.vert.resize(3 * (size_t)T); L.t2t3.resize(3 * (size_t)T); L.fref.assign(3 * (size_t)T, 0);
   L.rc_x.resize(3 * (size_t)T); L.rc_y.resize(3 * (size_t)T);
   L.fnx.assign(3 * (size_t)T, 0.0); L.fny.assign(3 * (size_t)T, 0.0);
@@ -405,6 +405,23 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
       }
       L.fnx[q] = nx;
       L.fny[q] = ny;
+    }
+    // where each face neighbour sits among the first three stencil members (interior
+    // cells: the three face neighbours), so the limiter reuses the stencil differences
+    {
+      uint8_t mk = 0;
+      for (int j = 0; j < 3; j++) {
+        const int32_t nbj = L.t2t3[(size_t)j * T + c];
+        int k3 = 3;
+        if (nbj >= 0)
+          for (int k = 0; k < std::min<int>(n, 3); k++)
+            if (L.st_id[(size_t)k * T + c] == nbj) {
+              k3 = k;
+              break;
+            }
+        mk |= (uint8_t)(k3 << (2 * j));
+      }
+      L.t3k[c] = mk;
     }
     int ord[3] = {0, 1, 2};
     std::sort(ord, ord + 3, [&](int a, int b) { return key[a] < key[b]; });
@@ -537,6 +554,7 @@ void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& 
   M.z.assign(T, 0.0); M.delz_x.assign(T, 0.0); M.delz_y.assign(T, 0.0); M.zmax.assign(T, 0.0);
   M.cd.assign(T, 0.0); M.lsq_a.assign(T, 1.0); M.lsq_b.assign(T, 0.0); M.lsq_c.assign(T, 1.0);
   M.lsq_det.assign(T, 1.0); M.nst.assign(T, 0); M.forder.assign(T, 0); M.hvmask.assign(T, 0);
+  M.t3k.assign(T, 0xFF);
   M.vert.assign(T3, 0); M.t2t3.assign(T3, -1); M.fref.assign(T3, 0); M.fkind.assign(T3, FACE_NONE);
   M.rc_x.assign(T3, 0.0); M.rc_y.assign(T3, 0.0); M.fnx.assign(T3, 0.0); M.fny.assign(T3, 0.0);
   M.flen.assign(T3, 0.0); M.fz0.assign(T3, 0.0);
@@ -559,6 +577,7 @@ void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& 
       M.z[g] = P.z[c]; M.delz_x[g] = P.delz_x[c]; M.delz_y[g] = P.delz_y[c]; M.zmax[g] = P.zmax[c];
       M.cd[g] = P.cd[c]; M.lsq_a[g] = P.lsq_a[c]; M.lsq_b[g] = P.lsq_b[c]; M.lsq_c[g] = P.lsq_c[c];
       M.lsq_det[g] = P.lsq_det[c]; M.nst[g] = P.nst[c]; M.forder[g] = P.forder[c]; M.hvmask[g] = P.hvmask[c];
+      M.t3k[g] = P.t3k[c];
       if (!P.wcoef1.empty()) { M.wcoef1[g] = P.wcoef1[c]; M.wcoef2[g] = P.wcoef2[c]; }
       for (int j = 0; j < 3; j++) {
         const size_t q = (size_t)j * P.T + c, qg = (size_t)j * T + g;

@@ -50,6 +50,7 @@ struct HostLayout {
   std::vector<double> wcoef1, wcoef2;  // wind terms (empty: none)
   std::vector<double> lsq_a, lsq_b, lsq_c, lsq_det;
   std::vector<uint8_t> nst, forder, hvmask;
+  std::vector<uint8_t> t3k;  // 2 bits per face: the face neighbour's slot in the first three stencil entries (3: none)
   std::vector<int32_t> bc_cells;  // cells with an open-boundary face, increasing
   std::vector<int32_t> rs_cells, rs_off;  // cells by colour of the t2t stencil (new ids), CSR
   // [3][T]
