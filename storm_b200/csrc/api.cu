@@ -48,7 +48,7 @@ struct StormFvtHandle {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;       // boundary kernel, overlapped with k_flux
-  cudaEvent_t fork_ev[4] = {}, join_ev[4] = {};
+  cudaEvent_t fork_ev[4] = {}, join_ev[4] = {}, eflux_ev[4] = {};
   void* arena = nullptr;
   void* arena32 = nullptr;  // FP32 geometry copies (mixed precision only)
   Dev d{};
@@ -272,16 +272,19 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used, int only = -1
     if (done()) return STORM_ERR_CUDA;
     const int sF = rs ? STAGE_PHI : STAGE_FLUX, sFB = rs ? STAGE_PHI_BC : STAGE_FLUX_BC;
     if (d.nbdr > 0 && !timing) {
-      // k_bc on the side stream overlaps k_eflux and k_flux of the cells without
-      // boundary faces; the boundary cells are finished once both are done
+      // k_bc on the side stream overlaps k_eflux; the cells with an open-boundary face
+      // (k_flux_bc: their own values, the edge fluxes and k_bc's contributions) are
+      // then finished on the side stream beside k_flux of all the other cells
       CK(cudaEventRecord(h->fork_ev[s], h->stream));
       CK(cudaStreamWaitEvent(h->side, h->fork_ev[s], 0));
       launch(STAGE_BC, d.nbdr, 128, h->bc_smem, h->side, s, hs, dry, dry_next);
-      CK(cudaEventRecord(h->join_ev[s], h->side));
       if (gE > 0) launch(STAGE_EFLUX, gE, h->bs_eflux, 0, h->stream, s, hs, dry, dry_next);
+      CK(cudaEventRecord(h->eflux_ev[s], h->stream));
+      CK(cudaStreamWaitEvent(h->side, h->eflux_ev[s], 0));
+      if (gB > 0) launch(sFB, gB, kFluxThreads, 0, h->side, s, hs, dry, dry_next);
+      CK(cudaEventRecord(h->join_ev[s], h->side));
       launch(sF, gF, h->bs_flux, 0, h->stream, s, hs, dry, dry_next);
       CK(cudaStreamWaitEvent(h->stream, h->join_ev[s], 0));
-      if (gB > 0) launch(sFB, gB, kFluxThreads, 0, h->stream, s, hs, dry, dry_next);
     } else {
       if (d.nbdr > 0) {
         if (mark(KT_BC)) return STORM_ERR_CUDA;
@@ -357,6 +360,7 @@ void release(StormFvtHandle* h) {
   for (int i = 0; i < 4; i++) {
     if (h->fork_ev[i]) cudaEventDestroy(h->fork_ev[i]);
     if (h->join_ev[i]) cudaEventDestroy(h->join_ev[i]);
+    if (h->eflux_ev[i]) cudaEventDestroy(h->eflux_ev[i]);
   }
   if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -831,6 +835,7 @@ int storm_fvt_create_batch(const StormFvtMesh* const* meshes, int32_t n, const S
   for (int i = 0; i < 4 && e == cudaSuccess; i++) {
     e = cudaEventCreateWithFlags(&h->fork_ev[i], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->eflux_ev[i], cudaEventDisableTiming);
   }
   if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
