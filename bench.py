@@ -46,10 +46,11 @@ import numpy as np  # noqa: E402
 from storm_b200 import scenarios  # noqa: E402
 
 METRIC = "cell-stage updates/s (FVT time step, 2M-triangle meander)"
-# DRAM bytes (read + write) per cell-stage of one iteration's kernels, from ncu
-# captures of the same kernels on the 500k-cell meander (one kernel per capture);
-# traffic grows in proportion to the cells, so it is scaled to the workload's mesh.
-NCU_DRAM_BYTES_PER_CELL_STAGE = {("meander", "phases"): 714.6}
+# DRAM bytes (read + write) per cell-stage of one iteration's kernels (every stage
+# kernel, k_fric and k_final), from one ncu capture of three whole iterations on the
+# 500k-cell meander (dram__bytes_read.sum + dram__bytes_write.sum); traffic grows in
+# proportion to the cells, so it is scaled to the workload's mesh.
+NCU_DRAM_BYTES_PER_CELL_STAGE = {("meander", "phases"): 701.3}
 UNIT = "cell-stage updates/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 
@@ -848,8 +849,8 @@ def main():
         "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
         "kernel": f"one iteration (CUDA graph: {chain}, k_fric, k_final)",
         "algorithmic_bytes_per_launch": B * T * K_rk, "bytes_per_cell_stage": B, "peak_source": pk["source"],
-        "traffic_source": "ncu dram__bytes_read+write of the stage kernels on the 500k-cell meander, "
-                          "per cell-stage, scaled to this mesh" if traffic else None,
+        "traffic_source": "ncu dram__bytes_read+write of three iterations' kernels on the 500k-cell "
+                          "meander, per cell-stage, scaled to this mesh" if traffic else None,
         "achieved_serialised_stage_chain": achieved_serial,
         "kernel_ms_share": {k: round(v[0] / iter_ms, 4) for k, v in kt.items()},
         "stage_kernel_avg_ms": (kt["tile"][0] / max(1, kt["tile"][1]) if path_used != "phases"

@@ -487,7 +487,6 @@ int upload(StormFvtHandle* h) {
   size_t o_cvq = cpy(L.cv_q, ncvt), o_cvcc = cpy(L.cvc_cell, ncvc), o_cvco = cpy(L.cvc_code, ncvc);
   size_t o_cvsrc = A.take(sizeof(double) * ncv);
   size_t o_nst = cpy(L.nst, T), o_ford = cpy(L.forder, T), o_hvm = cpy(L.hvmask, T), o_fk = cpy(L.fkind, T3);
-  size_t o_t3k = cpy(L.t3k, T);
   size_t o_vert = cpy(L.vert, T3), o_t3 = cpy(L.t2t3, T3), o_fref = cpy(L.fref, T3), o_sid = cpy(L.st_id, TK);
   size_t o_rcx = cpy(L.rc_x, T3), o_rcy = cpy(L.rc_y, T3), o_fnx = cpy(L.fnx, T3), o_fny = cpy(L.fny, T3);
   size_t o_flen = cpy(L.flen, T3), o_fz0 = cpy(L.fz0, T3);
@@ -574,7 +573,6 @@ int upload(StormFvtHandle* h) {
   d.cv_q = at<double>(B, o_cvq); d.cvc_cell = at<int32_t>(B, o_cvcc); d.cvc_code = at<int32_t>(B, o_cvco);
   d.cvsrc = at<double>(B, o_cvsrc);
   d.nst = at<uint8_t>(B, o_nst); d.forder = at<uint8_t>(B, o_ford); d.hvmask = at<uint8_t>(B, o_hvm);
-  d.t3k = at<uint8_t>(B, o_t3k);
   d.fkind = at<uint8_t>(B, o_fk);
   d.vert = at<int32_t>(B, o_vert); d.t2t3 = at<int32_t>(B, o_t3); d.fref = at<int32_t>(B, o_fref);
   d.st_id = at<int32_t>(B, o_sid);
@@ -594,6 +592,7 @@ int upload(StormFvtHandle* h) {
   d.edge_sid = at<int32_t>(B, o_esid); d.bdr_sid = at<int32_t>(B, o_bsid);
   d.nscen = h->nscen;
   d.t_real = h->nscen == 1 ? h->info[0].cell_cnt : T;
+  d.lsq_derived = L.lsq_derived ? 1 : 0;
   d.rkh = at<double>(B, o_rkh); d.rku = at<double>(B, o_rku); d.rkv = at<double>(B, o_rkv);
   d.u_a = at<double>(B, o_ua); d.v_a = at<double>(B, o_va); d.u_b = at<double>(B, o_ub); d.v_b = at<double>(B, o_vb);
   h->u_a2 = at<double>(B, o_ua2); h->v_a2 = at<double>(B, o_va2);

@@ -46,6 +46,7 @@ struct Dev {
   int32_t steady, dt_op, lim, btype, hvalve, vclip, fric, stop_cr, flux;
   int32_t nscen;
   int32_t t_real;  // one-scenario handles: its cells are the slots below t_real
+  int32_t lsq_derived;  // FP64 gradients form lsq_a/b/c/det from the stencil (bit-equal)
   // scenario of each cell slot (-1: padding), node, interior edge and open boundary
   const int32_t *cell_sid, *node_sid, *edge_sid, *bdr_sid;
   double h_dry, h_wet, cfl, vceiling, visc, rstop;
@@ -67,7 +68,6 @@ struct Dev {
   double* cvsrc;
   const double *lsq_a, *lsq_b, *lsq_c, *lsq_det;
   const uint8_t *nst, *forder, *hvmask, *fkind;
-  const uint8_t* t3k;  // [T] 2 bits per face: its neighbour's slot among the first three stencil members (3: none)
   const int32_t *vert, *t2t3, *fref, *st_id;
   const double *rc_x, *rc_y, *fnx, *fny, *flen, *fz0, *st_w, *st_dx, *st_dy;
   const int32_t *wall_p1, *wall_p2;

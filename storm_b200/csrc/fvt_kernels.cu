@@ -542,23 +542,6 @@ __device__ __forceinline__ double limited_r(double q0, double qn, double g_x, do
   const double b = fmin2(rj, kOne);
   return fmax2(a, b);
 }
-// The same from d = qn - q0 (a stencil difference already formed): min(q0,qn) - q0 is
-// qn - q0 = d when qn < q0 and q0 - q0 otherwise, and qn < q0 exactly when d < 0 (the
-// difference of two doubles rounds to zero only when they are equal); likewise for the
-// maximum, so the quotient and the result are bit for bit those of limited_r.
-__device__ __forceinline__ double limited_rd(double q0, double dq, double g_x, double g_y, double rx, double ry) {
-  const double qj = q0 + g_x * rx + g_y * ry;
-  const double delq = qj - q0;
-  double rj;
-  if (equals(delq, kZero)) rj = kOne;
-  else {
-    const double num = (delq < 0) ? ((dq < 0) ? dq : q0 - q0) : ((dq > 0) ? dq : q0 - q0);
-    rj = (fabs(num) > fabs(delq)) ? kOne : qdiv(num, delq);
-  }
-  const double a = fmin2(kOne * rj, kOne);
-  const double b = fmin2(rj, kOne);
-  return fmax2(a, b);
-}
 __device__ __forceinline__ float limited_r(double q0, double qn, float g_x, float g_y, float rx, float ry) {
   const float dmin = (float)(fmin2(q0, qn) - q0), dmax = (float)(fmax2(q0, qn) - q0);
   const float delq = g_x * rx + g_y * ry;
@@ -613,13 +596,12 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
   const double u_c = nb.U(self), v_c = nb.V(self);
   const bool dry_c = nb.D(self);
   R hx = R(0), hy = R(0), ux = R(0), uy = R(0), vx = R(0), vy = R(0);
-  constexpr bool kF64 = sizeof(R) == 8;
-  // FP64: the differences to the first three stencil members, which the limiter reuses
-  // for the face neighbours among them (no second gather of their state)
-  double dzs[3] = {0, 0, 0}, dus[3] = {0, 0, 0}, dvs[3] = {0, 0, 0};
-  int kmap = 0xFF;
   if (d.lim == 1 || d.lim == 2) {
     R dz = R(0), ez = R(0), du = R(0), eu = R(0), dv = R(0), ev = R(0);
+    // FP64: lsq_setup's sums over the same stencil values, in its order (used when
+    // the layout found them bit-equal to lsq_a/b/c for every cell)
+    constexpr bool kF64 = sizeof(R) == 8;
+    double sa = 0.0, sb = 0.0, sc = 0.0;
     const int n = d.nst[c];
     int k0 = 0;
     if (n >= 3) {  // interior cells: the three face neighbours, all gathers issued together
@@ -638,13 +620,7 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
         pz[k] = (R)((nb.H(jj[k]) + nb.Z(jj[k])) - zeta_c);
         pu[k] = (R)(nb.U(jj[k]) - u_c);
         pv[k] = (R)(nb.V(jj[k]) - v_c);
-        if (kF64) {
-          dzs[k] = (double)pz[k];
-          dus[k] = (double)pu[k];
-          dvs[k] = (double)pv[k];
-        }
       }
-      if (kF64 && d.lim == 2) kmap = d.t3k[c];
 #pragma unroll
       for (int k = 0; k < 3; k++) {
         dz = dz + w[k] * pz[k] * dx[k];
@@ -653,6 +629,11 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
         eu = eu + w[k] * pu[k] * dy[k];
         dv = dv + w[k] * pv[k] * dx[k];
         ev = ev + w[k] * pv[k] * dy[k];
+        if (kF64) {
+          sa = sa + (double)w[k] * (double)dx[k] * (double)dx[k];
+          sb = sb + (double)w[k] * (double)dx[k] * (double)dy[k];
+          sc = sc + (double)w[k] * (double)dy[k] * (double)dy[k];
+        }
       }
       k0 = 3;
     }
@@ -669,8 +650,24 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
       eu = eu + w * pu * dy;
       dv = dv + w * pv * dx;
       ev = ev + w * pv * dy;
+      if (kF64) {
+        sa = sa + (double)w * (double)dx * (double)dx;
+        sb = sb + (double)w * (double)dx * (double)dy;
+        sc = sc + (double)w * (double)dy * (double)dy;
+      }
     }
-    const R ai = G.lsq_a[c], bi = G.lsq_b[c], ci = G.lsq_c[c], det = G.lsq_det[c];
+    R ai, bi, ci, det;
+    if (kF64 && d.lsq_derived) {
+      ai = (R)sa;
+      bi = (R)sb;
+      ci = (R)sc;
+      det = (R)(sa * sc - sb * sb);
+    } else {
+      ai = G.lsq_a[c];
+      bi = G.lsq_b[c];
+      ci = G.lsq_c[c];
+      det = G.lsq_det[c];
+    }
     hx = qdiv(ci * dz - bi * ez, det);
     hy = qdiv(ai * ez - dz * bi, det);
     ux = qdiv(ci * du - bi * eu, det);
@@ -689,22 +686,12 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
         rcx[j] = rx;
         rcy[j] = ry;
       }
-      const int ks = (kmap >> (2 * j)) & 3;
-      if (kF64 && ks < 3) {
-        const double ddz = ks == 0 ? dzs[0] : (ks == 1 ? dzs[1] : dzs[2]);
-        const double ddu = ks == 0 ? dus[0] : (ks == 1 ? dus[1] : dus[2]);
-        const double ddv = ks == 0 ? dvs[0] : (ks == 1 ? dvs[1] : dvs[2]);
-        rz[j] = (R)limited_rd(zeta_c, ddz, (double)hx, (double)hy, (double)rx, (double)ry);
-        ru[j] = (R)limited_rd(u_c, ddu, (double)ux, (double)uy, (double)rx, (double)ry);
-        rv[j] = (R)limited_rd(v_c, ddv, (double)vx, (double)vy, (double)rx, (double)ry);
-      } else {
-        const double qz = k < 0 ? zeta_c : nb.H(k) + nb.Z(k);
-        const double qu = k < 0 ? u_c : nb.U(k);
-        const double qv = k < 0 ? v_c : nb.V(k);
-        rz[j] = limited_r(zeta_c, qz, hx, hy, rx, ry);
-        ru[j] = limited_r(u_c, qu, ux, uy, rx, ry);
-        rv[j] = limited_r(v_c, qv, vx, vy, rx, ry);
-      }
+      const double qz = k < 0 ? zeta_c : nb.H(k) + nb.Z(k);
+      const double qu = k < 0 ? u_c : nb.U(k);
+      const double qv = k < 0 ? v_c : nb.V(k);
+      rz[j] = limited_r(zeta_c, qz, hx, hy, rx, ry);
+      ru[j] = limited_r(u_c, qu, ux, uy, rx, ry);
+      rv[j] = limited_r(v_c, qv, vx, vy, rx, ry);
     }
     const R pz = fmin2(fmin2(rz[0], rz[1]), rz[2]);
     const R pu = fmin2(fmin2(ru[0], ru[1]), ru[2]);

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <numeric>
 #include <string>
 #include <unordered_map>
@@ -56,6 +57,13 @@ std::vector<int32_t> morton_order(const std::vector<double>& x, const std::vecto
   std::iota(perm.begin(), perm.end(), 0);
   std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
   return perm;
+}
+
+bool same_bits(double a, double b) {
+  uint64_t x, y;
+  std::memcpy(&x, &a, 8);
+  std::memcpy(&y, &b, 8);
+  return x == y;
 }
 
 }  // namespace
@@ -297,7 +305,7 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
   L.delz_x.resize(T); L.delz_y.resize(T); L.zmax.resize(T); L.cd.resize(T);
   if (m.wcoef1 && m.wcoef2) { L.wcoef1.resize(T); L.wcoef2.resize(T); }
   L.lsq_a.resize(T); L.lsq_b.resize(T); L.lsq_c.resize(T); L.lsq_det.resize(T);
-  L.nst.resize(T); L.forder.resize(T); L.hvmask.assign(T, 0); L.t3k.assign(T, 0xFF);
+  L.nst.resize(T); L.forder.resize(T); L.hvmask.assign(T, 0);
   L.vert.resize(3 * (size_t)T); L.t2t3.resize(3 * (size_t)T); L.fref.assign(3 * (size_t)T, 0);
   L.rc_x.resize(3 * (size_t)T); L.rc_y.resize(3 * (size_t)T);
   L.fnx.assign(3 * (size_t)T, 0.0); L.fny.assign(3 * (size_t)T, 0.0);
@@ -311,6 +319,7 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
   L.st_dx.assign((size_t)L.kst * T, 0.0);
   L.st_dy.assign((size_t)L.kst * T, 0.0);
   const size_t lsq_ld = (size_t)T;
+  bool lsq_all = true;
   for (int32_t c = 0; c < T; c++) {
     const int32_t o = L.cell_old[c];  // 0-based old id
     const int32_t i1 = o + 1;         // 1-based old id
@@ -344,14 +353,25 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
     int32_t n = m.t2t[o];
     if (n < 0 || n > m.t2t_ncol - 1) return set_error(STORM_ERR_MESH, "storm_fvt_create: t2t count out of range");
     L.nst[c] = (uint8_t)n;
+    double sa = 0.0, sb = 0.0, sc = 0.0;
     for (int32_t k = 0; k < n; k++) {
       int32_t nb = m.t2t[(size_t)(k + 1) * T + o];
       if (nb < 1 || nb > T) return set_error(STORM_ERR_MESH, "storm_fvt_create: t2t entry out of range");
       L.st_id[(size_t)k * T + c] = CN(nb);
-      L.st_w[(size_t)k * T + c] = m.lsq_w[(size_t)k * lsq_ld + o];
-      L.st_dx[(size_t)k * T + c] = m.lsq_dx[(size_t)k * lsq_ld + o];
-      L.st_dy[(size_t)k * T + c] = m.lsq_dy[(size_t)k * lsq_ld + o];
+      const double w = m.lsq_w[(size_t)k * lsq_ld + o];
+      const double dx = m.lsq_dx[(size_t)k * lsq_ld + o];
+      const double dy = m.lsq_dy[(size_t)k * lsq_ld + o];
+      L.st_w[(size_t)k * T + c] = w;
+      L.st_dx[(size_t)k * T + c] = dx;
+      L.st_dy[(size_t)k * T + c] = dy;
+      sa = sa + w * dx * dx;  // lsq_setup.f90:92-145, in its order
+      sb = sb + w * dx * dy;
+      sc = sc + w * dy * dy;
     }
+    const double sd = sa * sc - sb * sb;
+    if (!same_bits(sa, L.lsq_a[c]) || !same_bits(sb, L.lsq_b[c]) || !same_bits(sc, L.lsq_c[c]) ||
+        !same_bits(sd, L.lsq_det[c]))
+      lsq_all = false;
     // per-slot data
     int64_t key[3];
     for (int j = 1; j <= 3; j++) {
@@ -406,23 +426,6 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
       L.fnx[q] = nx;
       L.fny[q] = ny;
     }
-    // where each face neighbour sits among the first three stencil members (interior
-    // cells: the three face neighbours), so the limiter reuses the stencil differences
-    {
-      uint8_t mk = 0;
-      for (int j = 0; j < 3; j++) {
-        const int32_t nbj = L.t2t3[(size_t)j * T + c];
-        int k3 = 3;
-        if (nbj >= 0)
-          for (int k = 0; k < std::min<int>(n, 3); k++)
-            if (L.st_id[(size_t)k * T + c] == nbj) {
-              k3 = k;
-              break;
-            }
-        mk |= (uint8_t)(k3 << (2 * j));
-      }
-      L.t3k[c] = mk;
-    }
     int ord[3] = {0, 1, 2};
     std::sort(ord, ord + 3, [&](int a, int b) { return key[a] < key[b]; });
     L.forder[c] = (uint8_t)(ord[0] | (ord[1] << 2) | (ord[2] << 4));
@@ -430,6 +433,7 @@ int build_layout(const StormFvtMesh& m, const StormFvtOptions& opt, HostLayout& 
       if (L.fkind[(size_t)j * T + c] == FACE_BC) L.forder[c] |= kOrderHasBc;
     if (L.forder[c] & kOrderHasBc) L.bc_cells.push_back(c);
   }
+  L.lsq_derived = lsq_all;
   // culverts (cvprep.f90 placed them; solverFVT.f90:227-233 adds their terms)
   if (m.n_culvert > 0) {
     const int32_t n = m.n_culvert, ld = m.cv_ld;
@@ -554,7 +558,9 @@ void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& 
   M.z.assign(T, 0.0); M.delz_x.assign(T, 0.0); M.delz_y.assign(T, 0.0); M.zmax.assign(T, 0.0);
   M.cd.assign(T, 0.0); M.lsq_a.assign(T, 1.0); M.lsq_b.assign(T, 0.0); M.lsq_c.assign(T, 1.0);
   M.lsq_det.assign(T, 1.0); M.nst.assign(T, 0); M.forder.assign(T, 0); M.hvmask.assign(T, 0);
-  M.t3k.assign(T, 0xFF);
+  // padding slots are never live, so only the scenarios' own cells decide
+  M.lsq_derived = true;
+  for (const HostLayout& P : parts) M.lsq_derived = M.lsq_derived && P.lsq_derived;
   M.vert.assign(T3, 0); M.t2t3.assign(T3, -1); M.fref.assign(T3, 0); M.fkind.assign(T3, FACE_NONE);
   M.rc_x.assign(T3, 0.0); M.rc_y.assign(T3, 0.0); M.fnx.assign(T3, 0.0); M.fny.assign(T3, 0.0);
   M.flen.assign(T3, 0.0); M.fz0.assign(T3, 0.0);
@@ -577,7 +583,6 @@ void merge_layouts(const std::vector<HostLayout>& parts, int block, HostLayout& 
       M.z[g] = P.z[c]; M.delz_x[g] = P.delz_x[c]; M.delz_y[g] = P.delz_y[c]; M.zmax[g] = P.zmax[c];
       M.cd[g] = P.cd[c]; M.lsq_a[g] = P.lsq_a[c]; M.lsq_b[g] = P.lsq_b[c]; M.lsq_c[g] = P.lsq_c[c];
       M.lsq_det[g] = P.lsq_det[c]; M.nst[g] = P.nst[c]; M.forder[g] = P.forder[c]; M.hvmask[g] = P.hvmask[c];
-      M.t3k[g] = P.t3k[c];
       if (!P.wcoef1.empty()) { M.wcoef1[g] = P.wcoef1[c]; M.wcoef2[g] = P.wcoef2[c]; }
       for (int j = 0; j < 3; j++) {
         const size_t q = (size_t)j * P.T + c, qg = (size_t)j * T + g;

@@ -49,8 +49,12 @@ struct HostLayout {
   std::vector<double> area, perim, xc, yc, z, delz_x, delz_y, zmax, cd;
   std::vector<double> wcoef1, wcoef2;  // wind terms (empty: none)
   std::vector<double> lsq_a, lsq_b, lsq_c, lsq_det;
+  // every cell's lsq_a/b/c/det equal, bit for bit, the sums lsq_setup forms from its
+  // stencil weights and offsets (a = sum w dx dx, b = sum w dx dy, c = sum w dy dy in
+  // stencil order, det = a c - b b), so the FP64 gradient kernel forms them again from
+  // the stencil values it loads instead of reading four more arrays
+  bool lsq_derived = false;
   std::vector<uint8_t> nst, forder, hvmask;
-  std::vector<uint8_t> t3k;  // 2 bits per face: the face neighbour's slot in the first three stencil entries (3: none)
   std::vector<int32_t> bc_cells;  // cells with an open-boundary face, increasing
   std::vector<int32_t> rs_cells, rs_off;  // cells by colour of the t2t stencil (new ids), CSR
   // [3][T]

@@ -208,3 +208,21 @@ def test_mixed_boundary_types(storm_lib, oracle_mod):
     o, g, so, sg = run_pair(sc, 50, oracle_mod, chunks=2)
     assert_bitwise(o, g)
     assert_stats_close(so, sg)
+
+
+def test_given_lsq_coefficients_are_read_when_not_derivable(storm_lib, oracle_mod):
+    """A caller's lsq_a that is not the sum lsq_setup forms (here one ulp above it in
+    every cell, as another compiler's rounding might leave it) is read, not formed
+    again: the GPU follows the oracle, which reads the same perturbed array."""
+    sc = _no_friction(scenarios.meander(n_target=20000, seed=5))
+    o = oracle_mod.Oracle(sc.problem, sc.options)
+    o.set_state(sc.h0, sc.u0, sc.v0)
+    m = o.mesh()
+    T = m.n_elems
+    a = np.ctypeslib.as_array(m.lsq_a, shape=(T,))
+    a[:] = np.nextafter(a, np.inf)  # writes through to the oracle's own array
+    g = fvt.Solver(o.mesh(), sc.options, keep=o)
+    g.set_state(sc.h0, sc.u0, sc.v0)
+    so, sg = o.step(20), g.step(20)
+    assert_bitwise(o, g)
+    assert_stats_close(so, sg)
