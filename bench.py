@@ -423,6 +423,8 @@ def warm_start_eval(args, local) -> dict:
         # depth errors against the steady state (FP64 run on from the cold result to 1e-10)
         "depth_err_vs_steady_max_m": {k: ev["depth_err_vs_steady_max_m"][k] for k in ("warm_mixed", "cold_fp64")},
         "within_1cm": ev["within_1cm"],
+        # each start against the plain FP64 cold run's own result at the same 1e-6 stop
+        "depth_diff_vs_cold_fp64_same_stop": ev["depth_diff_vs_cold_fp64_same_stop"],
         # the same tighter stop test from the network, the prior alone and the cold start
         "to_1e-8": {"warm_mixed": at("warm_mixed", 1e-8), "prior_mixed": at("prior_mixed", 1e-8),
                     "cold_mixed": at("cold_mixed", 1e-8)},

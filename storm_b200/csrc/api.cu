@@ -487,6 +487,16 @@ int upload(StormFvtHandle* h) {
   size_t o_cvq = cpy(L.cv_q, ncvt), o_cvcc = cpy(L.cvc_cell, ncvc), o_cvco = cpy(L.cvc_code, ncvc);
   size_t o_cvsrc = A.take(sizeof(double) * ncv);
   size_t o_nst = cpy(L.nst, T), o_ford = cpy(L.forder, T), o_hvm = cpy(L.hvmask, T), o_fk = cpy(L.fkind, T3);
+  // face kinds and references in summation order (static; see Dev::fko)
+  std::vector<uint16_t> fko(T, 0);
+  std::vector<int32_t> frefo(T3, 0);
+  for (size_t c = 0; c < (size_t)T; c++)
+    for (int t = 0; t < 3; t++) {
+      const int j = (L.forder[c] >> (2 * t)) & 3;
+      fko[c] |= (uint16_t)((L.fkind[(size_t)j * T + c] & 7) << (3 * t));
+      frefo[(size_t)t * T + c] = L.fref[(size_t)j * T + c];
+    }
+  size_t o_fko = cpy(fko, T), o_frefo = cpy(frefo, T3);
   size_t o_vert = cpy(L.vert, T3), o_t3 = cpy(L.t2t3, T3), o_fref = cpy(L.fref, T3), o_sid = cpy(L.st_id, TK);
   size_t o_rcx = cpy(L.rc_x, T3), o_rcy = cpy(L.rc_y, T3), o_fnx = cpy(L.fnx, T3), o_fny = cpy(L.fny, T3);
   size_t o_flen = cpy(L.flen, T3), o_fz0 = cpy(L.fz0, T3);
@@ -575,6 +585,7 @@ int upload(StormFvtHandle* h) {
   d.nst = at<uint8_t>(B, o_nst); d.forder = at<uint8_t>(B, o_ford); d.hvmask = at<uint8_t>(B, o_hvm);
   d.fkind = at<uint8_t>(B, o_fk);
   d.vert = at<int32_t>(B, o_vert); d.t2t3 = at<int32_t>(B, o_t3); d.fref = at<int32_t>(B, o_fref);
+  d.fko = at<uint16_t>(B, o_fko); d.frefo = at<int32_t>(B, o_frefo);
   d.st_id = at<int32_t>(B, o_sid);
   d.rc_x = at<double>(B, o_rcx); d.rc_y = at<double>(B, o_rcy); d.fnx = at<double>(B, o_fnx);
   d.fny = at<double>(B, o_fny); d.flen = at<double>(B, o_flen); d.fz0 = at<double>(B, o_fz0);

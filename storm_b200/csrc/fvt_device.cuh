@@ -69,6 +69,10 @@ struct Dev {
   const double *lsq_a, *lsq_b, *lsq_c, *lsq_det;
   const uint8_t *nst, *forder, *hvmask, *fkind;
   const int32_t *vert, *t2t3, *fref, *st_id;
+  // the faces of each cell in the order their terms are added (forder): kinds, 3 bits
+  // each, and references ([3][T]) of the t-th face added
+  const uint16_t* fko;
+  const int32_t* frefo;
   const double *rc_x, *rc_y, *fnx, *fny, *flen, *fz0, *st_w, *st_dx, *st_dy;
   const int32_t *wall_p1, *wall_p2;
   // interior edges

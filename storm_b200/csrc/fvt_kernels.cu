@@ -109,6 +109,8 @@ __device__ __forceinline__ bool cell_live(const Dev& d, int c) {
   const int sid = d.cell_sid[c];
   return sid >= 0 && !d.sc[sid].converged;
 }
+// Scenario of a live cell (one-scenario handles: 0, without the lookup).
+__device__ __forceinline__ int cell_scenario(const Dev& d, int c) { return d.nscen == 1 ? 0 : d.cell_sid[c]; }
 __device__ __forceinline__ bool item_live(const Dev& d, const int32_t* __restrict__ sid_of, int i) {
   if (d.nscen == 1) return !d.sc[0].converged;
   return !d.sc[sid_of[i]].converged;
@@ -1358,9 +1360,21 @@ struct FacesGlobal {
   const Geo<R>& G;
   const double* __restrict__ hs;
   int c;
-  // flux*length of the interior face in slot j, and whether the edge produced one
-  __device__ __forceinline__ bool iface(int j, R* f) const {
-    const int e = d.fref[j * d.T + c];
+  // the faces in the order their terms are added (slots, kinds, references), read
+  // from the per-cell arrays kept in that order so that none waits on forder
+  __device__ __forceinline__ uint8_t order(int (&fj)[3], int (&fkd)[3], int (&fe)[3]) const {
+    const uint8_t ord = d.forder[c];
+    const unsigned ko = d.fko[c];
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      fj[t] = (ord >> (2 * t)) & 3;
+      fkd[t] = (ko >> (3 * t)) & 7;
+      fe[t] = d.frefo[t * d.T + c];
+    }
+    return ord;
+  }
+  // flux*length of the interior face in slot j (edge e), and whether the edge produced one
+  __device__ __forceinline__ bool iface(int j, int e, R* f) const {
     f[0] = G.efx[e];
     f[1] = G.efx[d.ne + e];
     f[2] = G.efx[2 * d.ne + e];
@@ -1379,9 +1393,8 @@ struct FacesGlobal {
     *x = G.delh_x[c];
     *y = G.delh_y[c];
   }
-  // vertex depths at the two ends (walledg1 order) of the wall face in slot j
-  __device__ __forceinline__ void hwall(int j, double* h1, double* h2) const {
-    const int w = d.fref[j * d.T + c];
+  // vertex depths at the two ends (walledg1 order) of the wall face in slot j (wall w)
+  __device__ __forceinline__ void hwall(int j, int w, double* h1, double* h2) const {
     *h1 = d.hvtx[d.wall_p1[w]];
     *h2 = d.hvtx[d.wall_p2[w]];
   }
@@ -1403,19 +1416,29 @@ struct FacesTile {
   const int32_t* __restrict__ wall_p1;
   const int32_t* __restrict__ wall_p2;
   const int32_t* __restrict__ fref;
-  __device__ __forceinline__ void hwall(int j, double* h1, double* h2) const {
-    const int q = j * T + c;
+  const uint8_t* __restrict__ forder;
+  const uint8_t* __restrict__ fkind;
+  __device__ __forceinline__ uint8_t order(int (&fj)[3], int (&fkd)[3], int (&fe)[3]) const {
+    const uint8_t ord = forder[c];
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      fj[t] = (ord >> (2 * t)) & 3;
+      fkd[t] = fkind[fj[t] * T + c] & 7;
+      fe[t] = fref[fj[t] * T + c];
+    }
+    return ord;
+  }
+  __device__ __forceinline__ void hwall(int j, int w, double* h1, double* h2) const {
     if (shv) {
-      const uint32_t w = lwall[q];
-      *h1 = shv[w & 0xFFFF];
-      *h2 = shv[w >> 16];
+      const uint32_t lw = lwall[j * T + c];
+      *h1 = shv[lw & 0xFFFF];
+      *h2 = shv[lw >> 16];
     } else {
-      const int w = fref[q];
       *h1 = hvtx[wall_p1[w]];
       *h2 = hvtx[wall_p2[w]];
     }
   }
-  __device__ __forceinline__ bool iface(int j, R* f) const {
+  __device__ __forceinline__ bool iface(int j, int, R* f) const {
     const int le = lfe[j * T + c];
     f[0] = sf[le];
     f[1] = sf[nem + le];
@@ -1445,23 +1468,18 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, cons
                                              bool dry_c, double* p1o, double* p2o, double* p3o) {
   const int T = d.T;
   double p1 = kZero, p2 = kZero, p3 = kZero;
-  const uint8_t ord = d.forder[c];
   // Issue the loads of all three faces before the (ordered) accumulation: face
   // descriptors first, then the fluxes of the interior faces, so the gathers overlap
   // instead of forming one dependent chain per face.
-  int fj[3], fkd[3];
-#pragma unroll
-  for (int t = 0; t < 3; t++) {
-    fj[t] = (ord >> (2 * t)) & 3;
-    fkd[t] = d.fkind[fj[t] * T + c] & 7;
-  }
+  int fj[3], fkd[3], fe[3];
+  const uint8_t ord = fs.order(fj, fkd, fe);
   bool fok[3];
   R fv[3][3];
 #pragma unroll
   for (int t = 0; t < 3; t++) {
     fok[t] = false;
     fv[t][0] = fv[t][1] = fv[t][2] = R(0);
-    if (fkd[t] == FACE_LEFT || fkd[t] == FACE_RIGHT) fok[t] = fs.iface(fj[t], fv[t]);
+    if (fkd[t] == FACE_LEFT || fkd[t] == FACE_RIGHT) fok[t] = fs.iface(fj[t], fe[t], fv[t]);
   }
 #pragma unroll
   for (int t = 0; t < 3; t++) {
@@ -1486,7 +1504,7 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, cons
       const double nx = d.fnx[q], ny = d.fny[q], len = d.flen[q];
       if (d.btype == 0) {  // wenslp3_fluxes.f90:34-67
         double h1, h2;
-        fs.hwall(j, &h1, &h2);
+        fs.hwall(j, fe[t], &h1, &h2);
         double hedge = qsqrt((h1 * h1 + h1 * h2 + h2 * h2) * kOneThird);
         if (hedge < kZero) hedge = kZero;
         if (hedge < d.h_dry) continue;
@@ -1509,7 +1527,7 @@ __device__ __forceinline__ void assemble_phi(const Dev& d, const Geo<R>& G, cons
         p3 = p3 - (f3 + dh * ny) * len;
       }
     } else if (kind == FACE_BC) {
-      const int e = d.fref[q];
+      const int e = fe[t];
       p1 = p1 - d.bc_c[e];
       p2 = p2 - d.bc_c[d.nbce + e];
       p3 = p3 - d.bc_c[2 * d.nbce + e];
@@ -1560,9 +1578,10 @@ __device__ __forceinline__ void rk_update(const Dev& d, int s, int c, double h_c
     delt = um + wc;
     if (delt < SMALL_F) delt = 1.044;
     delt = d.cfl * d.area[c] / (delt * d.perim[c]);
-    if (s == d.K && c == d.sc[d.cell_sid[c]].last_cell) d.sc[d.cell_sid[c]].delt_fric = delt;
+    Scalars& sc = d.sc[cell_scenario(d, c)];
+    if (s == d.K && c == sc.last_cell) sc.delt_fric = delt;
   } else {
-    delt = d.sc[d.cell_sid[c]].delt;
+    delt = d.sc[cell_scenario(d, c)].delt;
   }
   const double dt = delt / d.area[c];
   double rh = kZero, ru = kZero, rv = kZero;
@@ -1944,7 +1963,8 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     const double h_c = s_h[l];
     const bool dry_c = s_dry[l] != 0;
     const FacesTile<R> fs{tp.lfe, T, c, l, ngm, nem, s_f, s_eok, s_fh, s_fu, s_fv, s_dhx, s_dhy,
-                          tp.lwall, tp.nodes ? s_hv : nullptr, d.hvtx, d.wall_p1, d.wall_p2, d.fref};
+                          tp.lwall, tp.nodes ? s_hv : nullptr, d.hvtx, d.wall_p1, d.wall_p2, d.fref,
+                          d.forder, d.fkind};
     double p1, p2, p3;
     assemble_phi<R>(d, G, fs, c, h_c, dry_c, &p1, &p2, &p3);
     rk_update(d, s, c, h_c, dry_c, p1, p2, p3, dry_next, u_in, v_in, u_out, v_out);

@@ -478,6 +478,16 @@ def evaluate(net, norm, eval_n=64, lo=2000, hi=8000, istop=40000, limiter=0, dev
             out[f"{name}_rstop_{rs:g}"] = dict(summ(w), depth_err_vs_steady_median_m=float(np.median(dw)),
                                                 depth_err_vs_steady_max_m=max(dw),
                                                 within_1cm=int(sum(x <= 0.01 for x in dw)))
+    # the other reading of the depth bar: each start against the FP64 cold run's own
+    # result at the same stop test (the plain solver's answer, not the steady state)
+    def dvs64(states):
+        return [float(np.max(np.abs((a["h"] if isinstance(a, dict) else a[0]) - b["h"])))
+                for a, b in zip(states, cold64["states"])]
+    out["depth_diff_vs_cold_fp64_same_stop"] = {}
+    for name, r in (("warm_mixed", warm_mx), ("prior_mixed", prior_mx), ("cold_mixed", cold_mx)):
+        dv = dvs64(r["states"])
+        out["depth_diff_vs_cold_fp64_same_stop"][name] = {
+            "max_m": max(dv), "median_m": float(np.median(dv)), "within_1cm": int(sum(x <= 0.01 for x in dv))}
     out["within_1cm"] = {"warm_mixed": int(sum(x <= 0.01 for x in dh_warm)),
                          "prior_mixed": int(sum(x <= 0.01 for x in dh_prior)),
                          "cold_fp64": int(sum(x <= 0.01 for x in dh_cold64)), "of": len(ev)}
