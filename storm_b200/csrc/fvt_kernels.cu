@@ -60,14 +60,11 @@ __device__ __forceinline__ double qdiv(double a, double b) {
     r = a / b;
   return r;
 }
-__device__ __forceinline__ float qdiv(float a, float b) {
-  float r;
-  if (a == 0.0f && b != 0.0f && b == b)
-    r = __int_as_float((__float_as_int(a) ^ __float_as_int(b)) & (int)0x80000000u);
-  else
-    r = a / b;
-  return r;
-}
+// The mixed path's FP32 quotients: the approximate reciprocal-multiply division
+// (__fdividef, within 2 ulp for |b| in [2^-126, 2^126]; the denominators here are
+// determinants, celerities, wave-speed spans and limiter increments of ordinary
+// magnitude), whose error is far below the FP32 rounding the path already accepts.
+__device__ __forceinline__ float qdiv(float a, float b) { return __fdividef(a, b); }
 
 // sqrt with a zero argument answered directly (sqrt(+-0) = +-0 under IEEE), for the
 // same reason as qdiv: still water and dry sides make zero arguments common.
