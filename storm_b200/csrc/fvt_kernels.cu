@@ -393,8 +393,19 @@ __device__ void time_bcs(const Dev& d, int sid, double time) {
 
 }  // namespace
 
+// The FP32 (mixed-precision) instantiations of the stage and output kernels live in
+// fvt_kernels_f32.cu, a second compilation of this file with FMA contraction allowed:
+// the FP64 path keeps every operation rounded as written, the mixed path needs no
+// such order.  These are its entry points.
+int tile_blocks_per_sm_f32(size_t smem);
+void set_tile_smem_attr_f32(int bytes);
+void set_bc_smem_attr_f32(int bytes);
+void launch_stage_f32(const StageLaunch& L, const Dev& d, const Geo<float>& G);
+void launch_out_cell_f32(const Dev& d, const Geo<float>& G, const OutputArgs& a, int grid, cudaStream_t st);
+
 constexpr int kRedThreads = 256;
 
+#ifndef STORM_FVT_F32_TU
 // ---------------------------------------------------------------------------
 // Initial state: rk(:,0) = (h, h*u, h*v) (solverFVT.f90:122-126 then :138-142),
 // first-stage dry flags and the CFL dt partials of the initial state.
@@ -447,6 +458,7 @@ __global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int sid) {
     else sc->delt = (d.dt_op == 0) ? d.cfl : dtmin;
   }
 }
+#endif  // !STORM_FVT_F32_TU
 
 // ---------------------------------------------------------------------------
 // Vertex water surface and depth of one stage (to_vertices.f90:26-41: ctr2vtxWSE type
@@ -480,6 +492,7 @@ __device__ __forceinline__ void node_depth(const Dev& d, int n, int b0, int b1, 
   *hv_out = hv;
 }
 
+#ifndef STORM_FVT_F32_TU
 // Every node, or the listed nodes (the vertices of the cells with an open-boundary
 // face, ahead of their gradients on the side stream of the fused path).
 __global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ hs, const uint8_t* __restrict__ dry,
@@ -507,6 +520,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const double* __restrict__ 
   d.vwet[n] = wet;
   d.hvtx[n] = hv;
 }
+#endif  // !STORM_FVT_F32_TU
 
 // The face value of a cell field, x + grad . rc (invisc_fluxes.f90:58-64): in double as
 // the reference writes it; on the mixed path the FP32 correction is added to the FP64
@@ -1667,6 +1681,7 @@ __global__ void __launch_bounds__(128) k_flux_phi(Dev d, Geo<R> G, const double*
   d.phi0[2 * T + c] = p3;
 }
 
+#ifndef STORM_FVT_F32_TU
 __global__ void __launch_bounds__(256) k_rsavg(Dev d, int off, int cnt) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= cnt) return;
@@ -1690,6 +1705,7 @@ __global__ void __launch_bounds__(128) k_update(Dev d, int s, const double* __re
   rk_update(d, s, c, hs[c], dry[c] != 0, d.phi[c], d.phi[T + c], d.phi[2 * T + c], dry_next, d.u_a, d.v_a, d.u_a,
             d.v_a);
 }
+#endif  // !STORM_FVT_F32_TU
 
 // All cells without an open-boundary face (those wait for k_bc in k_flux_bc).
 template <class R>
@@ -1970,13 +1986,14 @@ __global__ void __launch_bounds__(kTileThreads, 3)
   }
 }
 
+#ifndef STORM_FVT_F32_TU
 size_t tile_smem_bytes(const TileDev& t, bool mixed) {
   return tile_smem_layout(t.ns_max, t.ng_max, t.ne_max, t.tc, mixed ? 4 : 8, t.nodes ? t.nn_max : 0).total;
 }
 
 int tile_blocks_per_sm(bool mixed, size_t smem) {
   int n = 0;
-  if (mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile<float>, kTileThreads, smem);
+  if (mixed) n = tile_blocks_per_sm_f32(smem);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile<double>, kTileThreads, smem);
   return n;
 }
@@ -1997,8 +2014,9 @@ void set_tile_smem_limit(int bytes) {
   std::lock_guard<std::mutex> lock(mu);
   const int b = raise_smem_limit(lim, bytes);
   cudaFuncSetAttribute(k_tile<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  cudaFuncSetAttribute(k_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  set_tile_smem_attr_f32(b);
 }
+#endif  // !STORM_FVT_F32_TU
 
 // ---------------------------------------------------------------------------
 // After the RK stages: find_dry_cells, fric_terms_impl, hvalve, rk level copy and the
@@ -2102,6 +2120,7 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d, const double* __res
   block_reduce5<kRedThreads>(st, sb, tm, rm, dtc, sm, d.part + 8 * blockIdx.x);
 }
 
+#ifndef STORM_FVT_F32_TU
 __global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
   __shared__ double sm[5 * (kRedThreads / 32)];
   __shared__ double red[5];
@@ -2166,6 +2185,7 @@ __global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
     }
   }
 }
+#endif  // !STORM_FVT_F32_TU
 
 // ---------------------------------------------------------------------------
 // The output pass of solverFVT.f90:389-405 (to_vertices.f90:26-65, ctr2vtx.f90:69-80,
@@ -2174,6 +2194,7 @@ __global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
 // is the only assignment of zeta) and the dry flags of the find_dry_cells call before
 // the friction step (:335), as in the reference.
 
+#ifndef STORM_FVT_F32_TU
 // to_vertices.f90:26-41: ctr2vtxWSE type 3, cap, positivity_vtx
 __global__ void __launch_bounds__(256) k_out_depth(Dev d, OutputArgs a) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2202,6 +2223,7 @@ __global__ void __launch_bounds__(256) k_out_depth(Dev d, OutputArgs a) {
   if (hv < kZero) hv = kZero;
   a.hv[n] = hv;
 }
+#endif  // !STORM_FVT_F32_TU
 
 // to_vertices.f90:44-55 on the solution (and the next stage's dry flag of a cell whose
 // velocity it zeroes), error_est.f90 etype 2
@@ -2237,6 +2259,7 @@ __global__ void __launch_bounds__(256) k_out_cell(Dev d, Geo<R> G, OutputArgs a)
   }
 }
 
+#ifndef STORM_FVT_F32_TU
 // ctr2vtx type 3 of u, v and cd with the normalised weights (c2v_setup.f90:113-117),
 // wetdryvfix (btype 0), the dry-vertex zeroing of to_vertices.f90:58-61
 __global__ void __launch_bounds__(256) k_out_vel(Dev d, OutputArgs a) {
@@ -2315,10 +2338,11 @@ __global__ void __launch_bounds__(256) k_out_drynodes(Dev d, OutputArgs a) {
     a.vv[n] = kZero;
   }
 }
+#endif  // !STORM_FVT_F32_TU
 
 // enforce_bcs.f90:124-169 with vbc_by_h.f90 for one inflow string, serial in node order
 // as the reference (the sums of vbc_by_h keep their order)
-__device__ void out_inflow_string(const Dev& d, const OutputArgs& a, int b) {
+static __device__ void out_inflow_string(const Dev& d, const OutputArgs& a, int b) {
   const int o = a.in_off[b], n = a.in_off[b + 1] - o;
   const int vt = a.in_type[b];
   const double qin = a.qin[b];
@@ -2360,6 +2384,7 @@ __device__ void out_inflow_string(const Dev& d, const OutputArgs& a, int b) {
     }
   }
 }
+#ifndef STORM_FVT_F32_TU
 __global__ void k_out_inflow(Dev d, OutputArgs a) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   for (int b = 0; b < a.n_in; b++) out_inflow_string(d, a, b);
@@ -2395,7 +2420,7 @@ void launch_output(const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bo
                    cudaStream_t st) {
   const int gN = (d.N + 255) / 256, gT = (d.T + 255) / 256;
   k_out_depth<<<gN, 256, 0, st>>>(d, a);
-  if (mixed) k_out_cell<float><<<gT, 256, 0, st>>>(d, Gf, a);
+  if (mixed) launch_out_cell_f32(d, Gf, a, gT, st);
   else k_out_cell<double><<<gT, 256, 0, st>>>(d, Gd, a);
   k_out_vel<<<gN, 256, 0, st>>>(d, a);
   if (a.n_out > 0) k_out_outflow<<<1, 32, 0, st>>>(d, a);
@@ -2407,6 +2432,7 @@ void launch_output(const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bo
     k_out_dtfinal<<<d.nscen, kRedThreads, 0, st>>>(d);
   }
 }
+#endif  // !STORM_FVT_F32_TU
 
 // Discharge of every culvert (cvdisch.f90:19-49), one thread per culvert, after the
 // stage's gradients: the headwater at the inlet is the stage reconstructed from the
@@ -2448,6 +2474,7 @@ __global__ void k_culvert(Dev d, Geo<R> G, const double* __restrict__ hs, const 
 // Linked partitions of one mesh (storm_fvt_link_partitions).  The scenarios share
 // one clock, so the first one's stop flag stands for all.
 
+#ifndef STORM_FVT_F32_TU
 // Every halo cell takes its owner's values of one RK level, the velocities and up to
 // two flag arrays.
 __global__ void __launch_bounds__(256) k_halo(Dev d, int level, uint8_t* f1, uint8_t* f2) {
@@ -2507,12 +2534,14 @@ __global__ void k_link(Dev d) {
     if (!d.steady && d.dt_op != 0) sc->delt = dmin;
   }
 }
+#endif  // !STORM_FVT_F32_TU
 
 // ---------------------------------------------------------------------------
 // One part of a mesh per process (storm_fvt_iter_*): the caller moves the halo values
 // between the processes and reduces dt and the sums; these kernels set the agreed
 // scalars and pack / unpack the exchanged cells.
 
+#ifndef STORM_FVT_F32_TU
 // which 0: the iteration's dt; 1: the steady friction dt (element n_elems of the mesh)
 __global__ void k_part_scalar(Dev d, int which, double v) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -2600,6 +2629,7 @@ void launch_fric(const Dev& d, const double* u_src, const double* v_src, cudaStr
 }
 void launch_link_dt(const Dev& d, cudaStream_t st) { k_link_dt<<<1, 32, 0, st>>>(d); }
 void launch_link(const Dev& d, cudaStream_t st) { k_link<<<1, 32, 0, st>>>(d); }
+#endif  // !STORM_FVT_F32_TU
 
 // ---------------------------------------------------------------------------
 // Host launchers of the templated stage kernels (api.cu is not templated).
@@ -2632,9 +2662,6 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
     case STAGE_PHI_BC:
       k_flux_phi<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, 1);
       break;
-    case STAGE_UPDATE:
-      k_update<<<L.grid, L.block, 0, L.stream>>>(d, L.s, L.hs, L.dry, L.dry_next);
-      break;
     case STAGE_CULVERT:
       k_culvert<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry);
       break;
@@ -2645,8 +2672,13 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
   }
 }
 
+#ifndef STORM_FVT_F32_TU
 void launch_stage(const StageLaunch& L, const Dev& d, const Geo<double>& Gd, const Geo<float>& Gf, bool mixed) {
-  if (mixed) launch_stage_t<float>(L, d, Gf);
+  if (L.which == STAGE_UPDATE) {  // not templated: the same kernel on both paths
+    k_update<<<L.grid, L.block, 0, L.stream>>>(d, L.s, L.hs, L.dry, L.dry_next);
+    return;
+  }
+  if (mixed) launch_stage_f32(L, d, Gf);
   else launch_stage_t<double>(L, d, Gd);
 }
 
@@ -2666,7 +2698,26 @@ void set_bc_smem_limit(int bytes) {
   std::lock_guard<std::mutex> lock(mu);
   const int b = raise_smem_limit(lim, bytes);
   cudaFuncSetAttribute(k_bc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  cudaFuncSetAttribute(k_bc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  set_bc_smem_attr_f32(b);
 }
+#endif  // !STORM_FVT_F32_TU
+
+#ifdef STORM_FVT_F32_TU
+int tile_blocks_per_sm_f32(size_t smem) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile<float>, kTileThreads, smem);
+  return n;
+}
+void set_tile_smem_attr_f32(int bytes) {
+  cudaFuncSetAttribute(k_tile<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+void set_bc_smem_attr_f32(int bytes) {
+  cudaFuncSetAttribute(k_bc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+void launch_stage_f32(const StageLaunch& L, const Dev& d, const Geo<float>& G) { launch_stage_t<float>(L, d, G); }
+void launch_out_cell_f32(const Dev& d, const Geo<float>& G, const OutputArgs& a, int grid, cudaStream_t st) {
+  k_out_cell<float><<<grid, 256, 0, st>>>(d, G, a);
+}
+#endif  // STORM_FVT_F32_TU
 
 }  // namespace storm
