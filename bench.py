@@ -50,7 +50,7 @@ METRIC = "cell-stage updates/s (FVT time step, 2M-triangle meander)"
 # kernel, k_fric and k_final), from one ncu capture of three whole iterations on the
 # 500k-cell meander (dram__bytes_read.sum + dram__bytes_write.sum); traffic grows in
 # proportion to the cells, so it is scaled to the workload's mesh.
-NCU_DRAM_BYTES_PER_CELL_STAGE = {("meander", "phases"): 701.3}
+NCU_DRAM_BYTES_PER_CELL_STAGE = {("meander", "phases"): 648.3}
 UNIT = "cell-stage updates/s"
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 

@@ -101,6 +101,7 @@ namespace {
 
 constexpr int kFluxThreads = 128;
 constexpr int kRed = 256;
+constexpr int kFinalThreadsHost = 512;  // k_final's block (kFinalThreads in fvt_kernels.cu)
 
 #define CK(call)                                                                                     \
   do {                                                                                               \
@@ -323,7 +324,7 @@ int enqueue_step(StormFvtHandle* h, bool timing, size_t* fev_used, int only = -1
   if (done()) return STORM_ERR_CUDA;
   if (linked && d.nhalo > 0) launch_halo(d, 0, d.dry_a, d.dry_out, h->stream);
   if (mark(KT_FINAL)) return STORM_ERR_CUDA;
-  k_final<<<d.nscen, kRed, 0, h->stream>>>(d);
+  k_final<<<d.nscen, kFinalThreadsHost, 0, h->stream>>>(d);
   if (done()) return STORM_ERR_CUDA;
   if (linked) launch_link(d, h->stream);
   CK(cudaGetLastError());

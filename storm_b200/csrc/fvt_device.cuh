@@ -107,7 +107,7 @@ struct Dev {
   int32_t bc_cache;         // k_bc keeps the inflow fixed point's invariants in shared memory
   double* bc_c;             // [3][nbce] boundary contributions to phi
   double* bc_rec;           // [3][nbce] reconstructed boundary-edge h, u, v
-  double* part;             // [nblk][8] reduction partials (blocks never span scenarios)
+  double* part;             // [5][nblk] reduction partials, field-major (blocks never span scenarios)
   int32_t nbc_cells;        // cells with an open-boundary face (finished after k_bc)
   const int32_t* bc_cells;
   int32_t nblk_red;

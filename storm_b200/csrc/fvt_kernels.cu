@@ -318,7 +318,7 @@ __device__ __forceinline__ double block_min(double x, double* sm) {
 // block_sum / block_max / block_min (so the same bits), with one barrier.
 template <int NT>
 __device__ __forceinline__ void block_reduce5(double st, double sb, double tm, double rm, double dt, double* sm,
-                                              double* out) {
+                                              double* out, size_t os = 1) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     st = st + __shfl_xor_sync(0xffffffffu, st, o);
@@ -348,10 +348,10 @@ __device__ __forceinline__ void block_reduce5(double st, double sb, double tm, d
       n = fmin2(n, sm[4 * NW + i]);
     }
     out[0] = a;
-    out[1] = b;
-    out[2] = c;
-    out[3] = m;
-    out[4] = n;
+    out[os] = b;
+    out[2 * os] = c;
+    out[3 * os] = m;
+    out[4 * os] = n;
   }
 }
 
@@ -404,6 +404,7 @@ void launch_stage_f32(const StageLaunch& L, const Dev& d, const Geo<float>& G);
 void launch_out_cell_f32(const Dev& d, const Geo<float>& G, const OutputArgs& a, int grid, cudaStream_t st);
 
 constexpr int kRedThreads = 256;
+constexpr int kFinalThreads = 512;  // k_final: one CTA per scenario over its block partials
 
 #ifndef STORM_FVT_F32_TU
 // ---------------------------------------------------------------------------
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(kRedThreads) k_init(Dev d, int c0) {
     dtc = d.cfl * d.area[c] / (dl * d.perim[c]);
   }
   double r = block_min<kRedThreads>(dtc, sm);
-  if (threadIdx.x == 0) d.part[8 * (c0 / kRedThreads + blockIdx.x) + 4] = r;
+  if (threadIdx.x == 0) d.part[4 * (size_t)d.nblk_red + c0 / kRedThreads + blockIdx.x] = r;
 }
 
 // One block per listed scenario: initial scalars and the first dt.
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(kRedThreads) k_init_final(Dev d, int sid) {
   __shared__ double sm[kRedThreads / 32];
   Scalars* sc = &d.sc[sid];
   double m = kVlarge;
-  for (int b = threadIdx.x; b < sc->blk_cnt; b += blockDim.x) m = fmin2(m, d.part[8 * (sc->blk_off + b) + 4]);
+  for (int b = threadIdx.x; b < sc->blk_cnt; b += blockDim.x) m = fmin2(m, d.part[4 * (size_t)d.nblk_red + sc->blk_off + b]);
   double dtmin = block_min<kRedThreads>(m, sm);
   if (threadIdx.x == 0) {
     sc->iter = 0;
@@ -2117,30 +2118,33 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d, const double* __res
       atomicOr(&d.sc[sid].status, 1);
     }
   }
-  block_reduce5<kRedThreads>(st, sb, tm, rm, dtc, sm, d.part + 8 * blockIdx.x);
+  block_reduce5<kRedThreads>(st, sb, tm, rm, dtc, sm, d.part + blockIdx.x, d.nblk_red);
 }
 
 #ifndef STORM_FVT_F32_TU
-__global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
-  __shared__ double sm[5 * (kRedThreads / 32)];
+__global__ void __launch_bounds__(kFinalThreads) k_final(Dev d) {
+  __shared__ double sm[5 * (kFinalThreads / 32)];
   __shared__ double red[5];
   const int sid = blockIdx.x;
   Scalars* sc = &d.sc[sid];
   if (sc->converged) return;
   double a0 = kZero, a1 = kZero, a2 = kZero, a3 = kZero, a4 = kVlarge;
   const int cnt = sc->blk_cnt;
-  const double* p0 = d.part + 8 * (size_t)sc->blk_off;
+  // field-major partials ([5][nblk_red]): a warp's loads of one field are coalesced
+  const size_t fs = d.nblk_red;
+  const double* p0 = d.part + sc->blk_off;
   int b = threadIdx.x;
-  // four partial records in flight per thread; each thread still adds its records in
-  // increasing order, so the sums round as in a one-at-a-time loop
-  for (; b + 3 * kRedThreads < cnt; b += 4 * kRedThreads) {
-    double r[4][5];
+  // eight partial records in flight per thread (the 2M meander's 7,813 records take
+  // two rounds); each thread still adds its records in increasing order, so the sums
+  // round as in a one-at-a-time loop over the same records
+  for (; b + 7 * kFinalThreads < cnt; b += 8 * kFinalThreads) {
+    double r[8][5];
 #pragma unroll
-    for (int k = 0; k < 4; k++)
+    for (int k = 0; k < 8; k++)
 #pragma unroll
-      for (int j = 0; j < 5; j++) r[k][j] = p0[8 * (size_t)(b + k * kRedThreads) + j];
+      for (int j = 0; j < 5; j++) r[k][j] = p0[j * fs + b + k * kFinalThreads];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < 8; k++) {
       a0 = a0 + r[k][0];
       a1 = a1 + r[k][1];
       a2 = a2 + r[k][2];
@@ -2148,15 +2152,15 @@ __global__ void __launch_bounds__(kRedThreads) k_final(Dev d) {
       a4 = fmin2(a4, r[k][4]);
     }
   }
-  for (; b < cnt; b += kRedThreads) {
-    const double* pb = p0 + 8 * (size_t)b;
+  for (; b < cnt; b += kFinalThreads) {
+    const double* pb = p0 + b;
     a0 = a0 + pb[0];
-    a1 = a1 + pb[1];
-    a2 = a2 + pb[2];
-    a3 = fmax2(a3, pb[3]);
-    a4 = fmin2(a4, pb[4]);
+    a1 = a1 + pb[fs];
+    a2 = a2 + pb[2 * fs];
+    a3 = fmax2(a3, pb[3 * fs]);
+    a4 = fmin2(a4, pb[4 * fs]);
   }
-  block_reduce5<kRedThreads>(a0, a1, a2, a3, a4, sm, red);
+  block_reduce5<kFinalThreads>(a0, a1, a2, a3, a4, sm, red);
   const double sumtop = red[0], sumbot = red[1], tmass = red[2], rmax_phi = red[3], dtmin = red[4];
   if (threadIdx.x == 0) {
     sc->sumtop = sumtop;
@@ -2405,13 +2409,13 @@ __global__ void __launch_bounds__(kRedThreads) k_out_dt(Dev d) {
     dtc = d.cfl * d.area[c] / ((um1 + wc1 + SMALL_F) * d.perim[c]);
   }
   const double r = block_min<kRedThreads>(dtc, sm);
-  if (threadIdx.x == 0) d.part[8 * blockIdx.x + 4] = r;
+  if (threadIdx.x == 0) d.part[4 * (size_t)d.nblk_red + blockIdx.x] = r;
 }
 __global__ void __launch_bounds__(kRedThreads) k_out_dtfinal(Dev d) {
   __shared__ double sm[kRedThreads / 32];
   Scalars* sc = &d.sc[blockIdx.x];
   double a4 = kVlarge;
-  for (int b = threadIdx.x; b < sc->blk_cnt; b += blockDim.x) a4 = fmin2(a4, d.part[8 * (sc->blk_off + b) + 4]);
+  for (int b = threadIdx.x; b < sc->blk_cnt; b += blockDim.x) a4 = fmin2(a4, d.part[4 * (size_t)d.nblk_red + sc->blk_off + b]);
   const double dtmin = block_min<kRedThreads>(a4, sm);
   if (threadIdx.x == 0) sc->delt = dtmin;
 }
