@@ -608,6 +608,8 @@ def main():
     ap.add_argument("--cells", type=int, default=2_000_000)
     ap.add_argument("--cpu-steps", type=int, default=3, help="oracle iterations timed for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="run the library's autotuner (stage kernels, block sizes) before timing")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="arithmetic of the headline run")
     ap.add_argument("--no-mixed", action="store_true", help="skip the secondary mixed-precision run")
@@ -711,6 +713,10 @@ def main():
     solver = fvt.Solver(pm, sc.options, keep=pm)
     solver.set_stage_path({"phases": fvt.STAGE_PHASES, "fused": fvt.STAGE_FUSED,
                            "fused-node-kernel": fvt.STAGE_FUSED_NODE_KERNEL}[args.stage_path])
+    tuned = None
+    if args.autotune:  # stage path and block sizes by timing (state restored; outside the timed region)
+        solver.set_state(sc.h0, sc.u0, sc.v0)
+        tuned = solver.autotune(iters=3)
     path_used = {fvt.STAGE_PHASES: "phases", fvt.STAGE_FUSED: "fused",
                  fvt.STAGE_FUSED_NODE_KERNEL: "fused-node-kernel"}[solver.stage_path()]
     setup = {"mesh_build_s": mesh_ratios.build_s, "create_s": time.perf_counter() - t0,
@@ -870,6 +876,7 @@ def main():
                 "steps": e2e_steps},
         "gpu_launches": gpu_launches,
         "stage_kernels": path_used,
+        "block_sizes": tuned if tuned is not None else "defaults (node 256, grad 256, eflux 128, flux 128)",
         "setup": setup,
         "roofline": roofline,
         "clocks": clk.summary(),

@@ -2133,32 +2133,26 @@ __global__ void __launch_bounds__(kFinalThreads) k_final(Dev d) {
   // field-major partials ([5][nblk_red]): a warp's loads of one field are coalesced
   const size_t fs = d.nblk_red;
   const double* p0 = d.part + sc->blk_off;
-  int b = threadIdx.x;
-  // eight partial records in flight per thread (the 2M meander's 7,813 records take
-  // two rounds); each thread still adds its records in increasing order, so the sums
+  // rounds of eight partial records in flight per thread (the 2M meander's 7,813
+  // records take two); each thread adds its records in increasing order, so the sums
   // round as in a one-at-a-time loop over the same records
-  for (; b + 7 * kFinalThreads < cnt; b += 8 * kFinalThreads) {
+  for (int b = threadIdx.x; b < cnt; b += 8 * kFinalThreads) {
     double r[8][5];
 #pragma unroll
-    for (int k = 0; k < 8; k++)
+    for (int k = 0; k < 8; k++) {
+      const int q = b + k * kFinalThreads;
 #pragma unroll
-      for (int j = 0; j < 5; j++) r[k][j] = p0[j * fs + b + k * kFinalThreads];
+      for (int j = 0; j < 5; j++) r[k][j] = q < cnt ? p0[j * fs + q] : kZero;
+    }
 #pragma unroll
     for (int k = 0; k < 8; k++) {
+      if (b + k * kFinalThreads >= cnt) break;
       a0 = a0 + r[k][0];
       a1 = a1 + r[k][1];
       a2 = a2 + r[k][2];
       a3 = fmax2(a3, r[k][3]);
       a4 = fmin2(a4, r[k][4]);
     }
-  }
-  for (; b < cnt; b += kFinalThreads) {
-    const double* pb = p0 + b;
-    a0 = a0 + pb[0];
-    a1 = a1 + pb[fs];
-    a2 = a2 + pb[2 * fs];
-    a3 = fmax2(a3, pb[3 * fs]);
-    a4 = fmin2(a4, pb[4 * fs]);
   }
   block_reduce5<kFinalThreads>(a0, a1, a2, a3, a4, sm, red);
   const double sumtop = red[0], sumbot = red[1], tmass = red[2], rmax_phi = red[3], dtmin = red[4];

@@ -246,8 +246,9 @@ class Solver:
         return dict(zip(("node", "grad", "eflux", "flux"), ch.tolist()))
 
     def set_stage_path(self, path: int):
-        """STAGE_FUSED (one tile kernel per stage, the default where it applies) or
-        STAGE_PHASES (k_grad, k_eflux, k_flux); re-captures the iteration graph."""
+        """STAGE_PHASES (k_node, k_grad, k_eflux, k_flux: the default) or STAGE_FUSED /
+        STAGE_FUSED_NODE_KERNEL (one tile kernel per stage); results are bitwise the
+        same in FP64; re-captures the iteration graph."""
         _chk(lib().storm_fvt_set_stage_path(self._h, int(path)))
 
     def stage_path(self) -> int:
