@@ -876,7 +876,7 @@ def main():
                 "steps": e2e_steps},
         "gpu_launches": gpu_launches,
         "stage_kernels": path_used,
-        "block_sizes": tuned if tuned is not None else "defaults (node 256, grad 256, eflux 128, flux 128)",
+        "block_sizes": tuned if tuned is not None else "library defaults (node 128, grad 64, eflux 64 FP64 / 128 mixed, flux 64)",
         "setup": setup,
         "roofline": roofline,
         "clocks": clk.summary(),

@@ -71,7 +71,9 @@ struct StormFvtHandle {
   double kt_ms[8] = {0};         // per-class totals of the last timed call
   int64_t kt_n[8] = {0};
   // block sizes of the stage kernels (storm_fvt_autotune picks them)
-  int bs_node = 256, bs_grad = 256, bs_eflux = 128, bs_flux = 128;
+  // block sizes of the node, gradient, edge-flux and cell kernels: the autotuner's
+  // choice on the 2M meander (FP64; the mixed path takes 128 for the edge fluxes)
+  int bs_node = 128, bs_grad = 64, bs_eflux = 64, bs_flux = 64;
   // output pass (storm_fvt_output_vertices): device buffers, allocated at first use
   void* out_buf = nullptr;
   size_t out_bytes = 0;
@@ -535,8 +537,8 @@ int upload(StormFvtHandle* h) {
   // state
   const size_t TL = (size_t)(K + 1) * T;
   size_t o_rkh = A.take(8 * TL), o_rku = A.take(8 * TL), o_rkv = A.take(8 * TL);
-  size_t o_ua = A.take(8 * (size_t)T), o_va = A.take(8 * (size_t)T), o_ub = A.take(8 * (size_t)T),
-         o_vb = A.take(8 * (size_t)T);
+  size_t o_ua = A.take(8 * (size_t)T), o_va = A.take(8 * (size_t)T), o_vz = A.take((size_t)T);
+  size_t o_ub = h->mixed ? A.take(8 * (size_t)T) : 0, o_vb = h->mixed ? A.take(8 * (size_t)T) : 0;
   size_t o_ua2 = A.take(8 * (size_t)T), o_va2 = A.take(8 * (size_t)T);
   size_t o_g[6];
   for (int i = 0; i < 6; i++) o_g[i] = A.take(8 * (size_t)T);
@@ -606,7 +608,9 @@ int upload(StormFvtHandle* h) {
   d.t_real = h->nscen == 1 ? h->info[0].cell_cnt : T;
   d.lsq_derived = L.lsq_derived ? 1 : 0;
   d.rkh = at<double>(B, o_rkh); d.rku = at<double>(B, o_rku); d.rkv = at<double>(B, o_rkv);
-  d.u_a = at<double>(B, o_ua); d.v_a = at<double>(B, o_va); d.u_b = at<double>(B, o_ub); d.v_b = at<double>(B, o_vb);
+  d.u_a = at<double>(B, o_ua); d.v_a = at<double>(B, o_va); d.vzero = at<uint8_t>(B, o_vz);
+  d.u_b = h->mixed ? at<double>(B, o_ub) : nullptr;
+  d.v_b = h->mixed ? at<double>(B, o_vb) : nullptr;
   h->u_a2 = at<double>(B, o_ua2); h->v_a2 = at<double>(B, o_va2);
   d.vox = at<double>(B, o_vox); d.voy = at<double>(B, o_voy);
   d.delh_x = at<double>(B, o_g[0]); d.delh_y = at<double>(B, o_g[1]); d.delu_x = at<double>(B, o_g[2]);
@@ -810,6 +814,7 @@ int storm_fvt_create_batch(const StormFvtMesh* const* meshes, int32_t n, const S
   h->opt = *opt;
   h->device = opt->device;
   h->mixed = opt->precision == STORM_PREC_MIXED;
+  if (h->mixed) h->bs_eflux = 128;
   h->nscen = n;
   try {
     h->parts.resize(n);

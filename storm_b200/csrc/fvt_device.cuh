@@ -93,7 +93,11 @@ struct Dev {
   // state
   double *rkh, *rku, *rkv;  // [K+1][T]
   double *u_a, *v_a;        // stage-input velocities (find_dry_cells, LSQ)
-  double *u_b, *v_b;        // velocities after hgradfix2 / to_vertices zeroing (fluxes)
+  // the velocities this stage's fluxes use (after hgradfix2 / to_vertices zeroing):
+  // FP64 path, a flag per cell (1: zero, else the stage-input u, v); mixed path, the
+  // values themselves (read by the lighter FP32 edge kernel while still in L2)
+  uint8_t* vzero;
+  double *u_b, *v_b;
   double *delh_x, *delh_y, *delu_x, *delu_y, *delv_x, *delv_y;
   uint8_t *dry_a, *dry_b;   // stage dry flags (ping-pong)
   uint8_t* dry_out;         // find_dry_cells before the friction step (the output pass)

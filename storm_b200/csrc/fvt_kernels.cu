@@ -600,7 +600,18 @@ struct GradOut {
   R hx, hy, ux, uy, vx, vy;
   double ub, vb;
   bool fix;  // hgradfix2 set the gradient: the previous RK level's momentum is zeroed
+  bool vz;   // ub, vb are the zeros hgradfix2 / to_vertices set (else the cell's u, v)
 };
+
+// The velocity the flux kernels use for cell x this stage (k_grad's ub, vb): FP64,
+// the zero hgradfix2 / to_vertices set or the stage-input value, from a flag; mixed,
+// the stored value (stored is the velocity array k_grad wrote, d.u_b or d.v_b).
+template <class R>
+__device__ __forceinline__ double post_fix(const Dev& d, const double* __restrict__ vel,
+                                           const double* __restrict__ stored, int x) {
+  if (sizeof(R) == 8) return d.vzero[x] ? kZero : vel[x];
+  return stored[x];
+}
 
 template <class R, class NB, class ST, class VW>
 __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>& G, const NB& nb, int c, int self,
@@ -717,7 +728,7 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
   hx = hx - G.delz_x[c];
   hy = hy - G.delz_y[c];
   double ub = u_c, vb = v_c;
-  bool fix = false;
+  bool fix = false, vz = false;
   if (!dry_c) {
     // hgradfix2.f90:48-98
     bool setgrad = zeta_c < d.zmax[c];
@@ -733,6 +744,7 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
       ub = kZero;
       vb = kZero;
       fix = true;
+      vz = true;
       ux = R(0); uy = R(0); vx = R(0); vy = R(0);
     }
     // to_vertices.f90:44-55
@@ -742,11 +754,12 @@ __device__ __forceinline__ GradOut<R> cell_gradients(const Dev& d, const Geo<R>&
     if (!flag) {
       ub = kZero;
       vb = kZero;
+      vz = true;
     }
   }
   GradOut<R> o;
   o.hx = hx; o.hy = hy; o.ux = ux; o.uy = uy; o.vx = vx; o.vy = vy;
-  o.ub = ub; o.vb = vb; o.fix = fix;
+  o.ub = ub; o.vb = vb; o.fix = fix; o.vz = vz;
   return o;
 }
 
@@ -782,8 +795,12 @@ __global__ void __launch_bounds__(256, 5) k_grad(Dev d, Geo<R> G, const double* 
   G.delh_x[c] = g.hx; G.delh_y[c] = g.hy;
   G.delu_x[c] = g.ux; G.delu_y[c] = g.uy;
   G.delv_x[c] = g.vx; G.delv_y[c] = g.vy;
-  d.u_b[c] = g.ub;
-  d.v_b[c] = g.vb;
+  if (sizeof(R) == 8) {
+    d.vzero[c] = g.vz;
+  } else {
+    d.u_b[c] = g.ub;
+    d.v_b[c] = g.vb;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -795,7 +812,8 @@ constexpr int kBcThreads = 128;
 
 template <class R>
 __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double* __restrict__ hs,
-                                                   const uint8_t* __restrict__ dry) {
+                                                   const uint8_t* __restrict__ dry, const double* __restrict__ u_in,
+                                                   const double* __restrict__ v_in) {
   const int b = blockIdx.x;
   Scalars* const sc = &d.sc[d.bdr_sid[b]];
   if (sc->converged) return;
@@ -814,8 +832,8 @@ __global__ void __launch_bounds__(kBcThreads) k_bc(Dev d, Geo<R> G, const double
     const int i = d.bce_cell[off + e], m = d.bce_slot[off + e];
     const int q = m * T + i;
     d.bc_rec[off + e] = recon(hs[i], G.delh_x[i], G.rc_x[q], G.delh_y[i], G.rc_y[q]);
-    d.bc_rec[NB + off + e] = recon(d.u_b[i], G.delu_x[i], G.rc_x[q], G.delu_y[i], G.rc_y[q]);
-    d.bc_rec[2 * NB + off + e] = recon(d.v_b[i], G.delv_x[i], G.rc_x[q], G.delv_y[i], G.rc_y[q]);
+    d.bc_rec[NB + off + e] = recon(post_fix<R>(d, u_in, d.u_b, i), G.delu_x[i], G.rc_x[q], G.delu_y[i], G.rc_y[q]);
+    d.bc_rec[2 * NB + off + e] = recon(post_fix<R>(d, v_in, d.v_b, i), G.delv_x[i], G.rc_x[q], G.delv_y[i], G.rc_y[q]);
   }
   __syncthreads();
   auto put = [&](int e, double c1, double c2, double c3) {
@@ -1196,15 +1214,16 @@ struct EdgeState {
 };
 
 template <class R>
-__device__ __forceinline__ EdgeState edge_state(const Dev& d, const Geo<R>& G, const double* __restrict__ hs, int x,
-                                                int m) {
+__device__ __forceinline__ EdgeState edge_state(const Dev& d, const Geo<R>& G, const double* __restrict__ hs,
+                                                const double* __restrict__ u_in, const double* __restrict__ v_in,
+                                                int x, int m) {
   const int q = m * d.T + x;
   const R rx = G.rc_x[q], ry = G.rc_y[q];
   EdgeState s;
   s.h = recon(hs[x], G.delh_x[x], rx, G.delh_y[x], ry);
   if (s.h < kZero) s.h = kZero;
-  s.u = recon(d.u_b[x], G.delu_x[x], rx, G.delu_y[x], ry);
-  s.v = recon(d.v_b[x], G.delv_x[x], rx, G.delv_y[x], ry);
+  s.u = recon(post_fix<R>(d, u_in, d.u_b, x), G.delu_x[x], rx, G.delu_y[x], ry);
+  s.v = recon(post_fix<R>(d, v_in, d.v_b, x), G.delv_x[x], rx, G.delv_y[x], ry);
   return s;
 }
 
@@ -1256,13 +1275,14 @@ __device__ __forceinline__ bool edge_flux(const Dev& d, bool dl, bool dr, const 
 // states reconstructed from the stored gradients.
 template <class R>
 __device__ __forceinline__ bool interior_flux(const Dev& d, const Geo<R>& G, const double* __restrict__ hs,
-                                              const uint8_t* __restrict__ dry, int L, int ml, int Rc, int mr, R nx,
+                                              const uint8_t* __restrict__ dry, const double* __restrict__ u_in,
+                                              const double* __restrict__ v_in, int L, int ml, int Rc, int mr, R nx,
                                               R ny, double z0e, R* f, bool* bad) {
   const bool dl = dry[L], dr = dry[Rc];
   if (dl && dr) return false;
   EdgeState sl{kZero, kZero, kZero}, sr{kZero, kZero, kZero};
-  if (!dl) sl = edge_state(d, G, hs, L, ml);
-  if (!dr) sr = edge_state(d, G, hs, Rc, mr);
+  if (!dl) sl = edge_state(d, G, hs, u_in, v_in, L, ml);
+  if (!dr) sr = edge_state(d, G, hs, u_in, v_in, Rc, mr);
   return edge_flux<R>(d, dl, dr, sl, sr, d.z[L], d.z[Rc], hs[L], hs[Rc], nx, ny, z0e, f, bad);
 }
 
@@ -1272,7 +1292,8 @@ __device__ __forceinline__ bool interior_flux(const Dev& d, const Geo<R>& G, con
 // phi(e(1),:) and adds to phi(e(2),:).
 template <class R>
 __global__ void __launch_bounds__(128, 8) k_eflux(Dev d, Geo<R> G, const double* __restrict__ hs,
-                                               const uint8_t* __restrict__ dry) {
+                                               const uint8_t* __restrict__ dry, const double* __restrict__ u_in,
+                                               const double* __restrict__ v_in) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.ne) return;
   if (!item_live(d, d.edge_sid, e)) return;
@@ -1280,7 +1301,7 @@ __global__ void __launch_bounds__(128, 8) k_eflux(Dev d, Geo<R> G, const double*
   const uint8_t sl = d.eslot[e];
   R f[3];
   bool bad = false;
-  const bool ok = interior_flux<R>(d, G, hs, dry, L, sl & 3, Rc, (sl >> 2) & 3, G.enx[e], G.eny[e],
+  const bool ok = interior_flux<R>(d, G, hs, dry, u_in, v_in, L, sl & 3, Rc, (sl >> 2) & 3, G.enx[e], G.eny[e],
                                    (dry[L] || dry[Rc]) ? d.ez0[e] : kZero, f, &bad);
   d.eok[e] = ok;
   if (ok) {
@@ -1372,6 +1393,8 @@ struct FacesGlobal {
   const Geo<R>& G;
   const double* __restrict__ hs;
   int c;
+  const double* __restrict__ u_in;  // stage-input velocities (the cell's own, for weslp2 walls)
+  const double* __restrict__ v_in;
   // the faces in the order their terms are added (slots, kinds, references), read
   // from the per-cell arrays kept in that order so that none waits on forder
   __device__ __forceinline__ uint8_t order(int (&fj)[3], int (&fkd)[3], int (&fe)[3]) const {
@@ -1397,8 +1420,8 @@ struct FacesGlobal {
     const int q = j * d.T + c;
     EdgeState s;
     s.h = recon(hs[c], G.delh_x[c], G.rc_x[q], G.delh_y[c], G.rc_y[q]);
-    s.u = recon(d.u_b[c], G.delu_x[c], G.rc_x[q], G.delu_y[c], G.rc_y[q]);
-    s.v = recon(d.v_b[c], G.delv_x[c], G.rc_x[q], G.delv_y[c], G.rc_y[q]);
+    s.u = recon(post_fix<R>(d, u_in, d.u_b, c), G.delu_x[c], G.rc_x[q], G.delu_y[c], G.rc_y[q]);
+    s.v = recon(post_fix<R>(d, v_in, d.v_b, c), G.delv_x[c], G.rc_x[q], G.delv_y[c], G.rc_y[q]);
     return s;
   }
   __device__ __forceinline__ void dh(R* x, R* y) const {
@@ -1648,7 +1671,7 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
   double p1, p2, p3;
   const double h_c = hs[c];
   const bool dry_c = dry[c] != 0;
-  assemble_phi<R>(d, G, FacesGlobal<R>{d, G, hs, c}, c, h_c, dry_c, &p1, &p2, &p3);
+  assemble_phi<R>(d, G, FacesGlobal<R>{d, G, hs, c, u_in, v_in}, c, h_c, dry_c, &p1, &p2, &p3);
   rk_update(d, s, c, h_c, dry_c, p1, p2, p3, dry_next, u_in, v_in, u_out, v_out);
 }
 
@@ -1659,7 +1682,8 @@ __device__ __forceinline__ void flux_cell(const Dev& d, const Geo<R>& G, int s, 
 // in colour order does), then every cell is updated.
 template <class R>
 __global__ void __launch_bounds__(128) k_flux_phi(Dev d, Geo<R> G, const double* __restrict__ hs,
-                                              const uint8_t* __restrict__ dry, int bc_cells) {
+                                              const uint8_t* __restrict__ dry, const double* __restrict__ u_in,
+                                              const double* __restrict__ v_in, int bc_cells) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   int c;
   if (bc_cells) {
@@ -1672,7 +1696,7 @@ __global__ void __launch_bounds__(128) k_flux_phi(Dev d, Geo<R> G, const double*
   }
   if (!cell_live(d, c)) return;
   double p1, p2, p3;
-  assemble_phi<R>(d, G, FacesGlobal<R>{d, G, hs, c}, c, hs[c], dry[c] != 0, &p1, &p2, &p3);
+  assemble_phi<R>(d, G, FacesGlobal<R>{d, G, hs, c, u_in, v_in}, c, hs[c], dry[c] != 0, &p1, &p2, &p3);
   const size_t T = d.T;
   d.phi[c] = p1;
   d.phi[T + c] = p2;
@@ -2641,10 +2665,10 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
       k_grad<R, true><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.rku_prev, L.rkv_prev, L.u_in, L.v_in);
       break;
     case STAGE_BC:
-      k_bc<R><<<L.grid, L.block, L.smem, L.stream>>>(d, G, L.hs, L.dry);
+      k_bc<R><<<L.grid, L.block, L.smem, L.stream>>>(d, G, L.hs, L.dry, L.u_in, L.v_in);
       break;
     case STAGE_EFLUX:
-      k_eflux<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry);
+      k_eflux<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.u_in, L.v_in);
       break;
     case STAGE_FLUX:
       k_flux<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.s, L.hs, L.dry, L.dry_next, L.u_in, L.v_in, L.u_out,
@@ -2655,10 +2679,10 @@ static void launch_stage_t(const StageLaunch& L, const Dev& d, const Geo<R>& G) 
                                                       L.v_out);
       break;
     case STAGE_PHI:
-      k_flux_phi<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, 0);
+      k_flux_phi<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.u_in, L.v_in, 0);
       break;
     case STAGE_PHI_BC:
-      k_flux_phi<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, 1);
+      k_flux_phi<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry, L.u_in, L.v_in, 1);
       break;
     case STAGE_CULVERT:
       k_culvert<R><<<L.grid, L.block, 0, L.stream>>>(d, G, L.hs, L.dry);
