@@ -352,8 +352,9 @@ STORM_FVT_API int storm_fvt_kernel_times(const StormFvtHandle* hd, double* ms, i
 STORM_FVT_API int storm_fvt_autotune(StormFvtHandle* hd, int32_t iters, int32_t* chosen);
 
 /* Stage kernels of the captured iteration.  No counterpart in the reference (it
- * selects how this library schedules the same arithmetic; results are bitwise the
- * same either way):
+ * selects how this library schedules the same arithmetic; FP64 results are bitwise
+ * the same either way, mixed-precision ones agree to within that path's own error,
+ * its FP32 kernels being compiled with FMA contraction):
  *   STORM_STAGE_PHASES  k_node, k_grad, k_eflux, k_flux per stage (gradients and edge
  *                       fluxes pass through device memory between the kernels);
  *                       the default;
