@@ -160,3 +160,33 @@ def test_host_checks_of_the_newer_entry_points(storm_lib):
         with pytest.raises(fvt.StormError) as e:
             fvt.Solver(pm, fvt.default_options(**kw))
         assert e.value.code == abi.STORM_ERR_ARG, kw
+
+
+@pytest.mark.parametrize("make", [lambda: scenarios.meander(n_target=20000, seed=5),
+                                  lambda: scenarios.dambreak(n_target=20000, seed=4),
+                                  lambda: scenarios.channel(nx=60, ny=8)])
+def test_lsq_coefficients_are_the_stencil_sums(make, storm_lib):
+    """lsq_a/b/c/det of a prepared mesh are, bit for bit, the sums lsq_setup.f90:92-145
+    forms from the stencil weights and offsets in stencil order (a = sum w dx dx, ...,
+    det = a c - b b), which the FP64 gradient kernel relies on to form them itself
+    (numpy float64 rounds each operation as the FMA-free device code does)."""
+    sc = make()
+    pm = fvt.PreparedMesh(sc.problem)
+    try:
+        m = pm.numpy()
+        ncol = pm.mesh.t2t_ncol
+        T = m["t2t"].size // ncol
+        cnt = m["t2t"].reshape(ncol, T)[0]
+        kl = max(ncol - 1, 1)
+        w, dx, dy = (m[k].reshape(kl, T) for k in ("lsq_w", "lsq_dx", "lsq_dy"))
+        a, b, c = np.zeros(T), np.zeros(T), np.zeros(T)
+        for k in range(kl):
+            on = cnt > k
+            a = np.where(on, a + w[k] * dx[k] * dx[k], a)
+            b = np.where(on, b + w[k] * dx[k] * dy[k], b)
+            c = np.where(on, c + w[k] * dy[k] * dy[k], c)
+        det = a * c - b * b
+        for got, key in ((a, "lsq_a"), (b, "lsq_b"), (c, "lsq_c"), (det, "lsq_det")):
+            assert np.array_equal(got.view(np.uint64), m[key].view(np.uint64)), key
+    finally:
+        pm.close()
