@@ -2055,9 +2055,13 @@ __global__ void __launch_bounds__(kRedThreads) k_fric(Dev d, const double* __res
   __shared__ double sm[5 * (kRedThreads / 32)];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int T = d.T, K = d.K;
-  const int sid = c < T ? d.cell_sid[c] : -1;
+  // one-scenario handles: scenario 0 for the cells below t_real, padding above, with
+  // no per-cell scenario id read
+  const bool one = d.nscen == 1;
+  const int sid = one ? (c < d.t_real ? 0 : -1) : (c < T ? d.cell_sid[c] : -1);
   // a block never spans two scenarios, so this test is uniform over the block
-  if (d.sc[d.cell_sid[blockIdx.x * blockDim.x] < 0 ? 0 : d.cell_sid[blockIdx.x * blockDim.x]].converged) return;
+  const int bsid = one ? 0 : d.cell_sid[blockIdx.x * blockDim.x];
+  if (d.sc[bsid < 0 ? 0 : bsid].converged) return;
   double st = kZero, sb = kZero, tm = kZero, rm = kZero, dtc = kVlarge;
   if (sid >= 0) {
     const int qk = K * T + c;
